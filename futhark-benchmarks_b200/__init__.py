@@ -1,0 +1,299 @@
+"""B200-native engine for the finpar LocVolCalib benchmark (diku-dk/futhark-benchmarks).
+
+The product is the C-ABI library ``liblvc.so`` (declared in
+``include/LocVolCalib.h``): the Futhark-generated C API of
+finpar/LocVolCalib.fut's entry point ``main`` plus batched and serving forms,
+all running hand-written sm_100a kernels.  This module is the Python host
+mirror of that API (ctypes), with the same names, argument meaning and error
+behaviour as the generated library:
+
+    ctx = Context()                       # futhark_context_config_new + futhark_context_new
+    prices = ctx.main(16, 32, 256, 256, 0.03, 5.0, 0.2, 0.6, 0.5)        # f32, futhark_entry_main
+    prices = ctx.main_f64(16, 32, 256, 256, 0.03, 5.0, 0.2, 0.6, 0.5)    # f64 twin
+    plan = ctx.plan([Calibration(...), ...], precision=F64)              # batched form
+    plan.run(); plan.prices()
+
+A failing call raises ``FutharkError`` carrying futhark_context_get_error's
+message and the non-zero return code.  There is no CPU fallback: if the
+library is missing the import of this module fails loudly.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass, astuple
+from typing import Iterable, List, Sequence
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "liblvc.so")
+
+FUTHARK_SUCCESS = 0
+FUTHARK_PROGRAM_ERROR = 2
+FUTHARK_OUT_OF_MEMORY = 3
+F64 = 0
+F32_STATE = 1
+
+_lib = None
+
+
+class FutharkError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+        self.msg = msg
+
+
+class _Calib(ctypes.Structure):
+    _fields_ = [("outer", ctypes.c_int32), ("numX", ctypes.c_int32), ("numY", ctypes.c_int32),
+                ("numT", ctypes.c_int32), ("s0", ctypes.c_double), ("t", ctypes.c_double),
+                ("alpha", ctypes.c_double), ("nu", ctypes.c_double), ("beta", ctypes.c_double)]
+
+
+@dataclass(frozen=True)
+class Calibration:
+    """The nine scalar inputs of `main` (finpar/LocVolCalib.fut:238-246)."""
+    outer: int
+    numX: int
+    numY: int
+    numT: int
+    s0: float
+    t: float
+    alpha: float
+    nu: float
+    beta: float
+
+    def work(self) -> int:
+        """Option-cell-steps: outer * numX * numY * (numT - 1)."""
+        return self.outer * self.numX * self.numY * max(self.numT - 1, 0)
+
+
+def load_library(path: str = LIB_PATH):
+    """Load liblvc.so and declare its C signatures."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(f"{path} is missing; build it with `python futhark-benchmarks_b200/build.py`")
+    L = ctypes.CDLL(path)
+    vp, i32, i64, f32, f64 = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_float, ctypes.c_double
+    sig = {
+        "futhark_context_config_new": (vp, []),
+        "futhark_context_config_free": (None, [vp]),
+        "futhark_context_config_set_device": (None, [vp, ctypes.c_char_p]),
+        "futhark_context_config_set_debugging": (None, [vp, ctypes.c_int]),
+        "futhark_context_config_set_profiling": (None, [vp, ctypes.c_int]),
+        "futhark_context_config_set_logging": (None, [vp, ctypes.c_int]),
+        "futhark_context_config_set_cache_file": (None, [vp, ctypes.c_char_p]),
+        "futhark_context_new": (vp, [vp]),
+        "futhark_context_free": (None, [vp]),
+        "futhark_context_sync": (ctypes.c_int, [vp]),
+        "futhark_context_get_error": (ctypes.POINTER(ctypes.c_char), [vp]),
+        "futhark_context_clear_caches": (ctypes.c_int, [vp]),
+        "futhark_new_f32_1d": (vp, [vp, vp, i64]),
+        "futhark_new_f64_1d": (vp, [vp, vp, i64]),
+        "futhark_free_f32_1d": (ctypes.c_int, [vp, vp]),
+        "futhark_free_f64_1d": (ctypes.c_int, [vp, vp]),
+        "futhark_values_f32_1d": (ctypes.c_int, [vp, vp, vp]),
+        "futhark_values_f64_1d": (ctypes.c_int, [vp, vp, vp]),
+        "futhark_shape_f32_1d": (ctypes.POINTER(i64), [vp, vp]),
+        "futhark_shape_f64_1d": (ctypes.POINTER(i64), [vp, vp]),
+        "futhark_entry_main": (ctypes.c_int, [vp, ctypes.POINTER(vp), i32, i32, i32, i32, f32, f32, f32, f32, f32]),
+        "futhark_entry_main_f64": (ctypes.c_int, [vp, ctypes.POINTER(vp), i32, i32, i32, i32, f64, f64, f64, f64, f64]),
+        "lvc_plan_new": (ctypes.c_int, [vp, ctypes.POINTER(_Calib), i32, i32, ctypes.POINTER(vp)]),
+        "lvc_plan_free": (ctypes.c_int, [vp, vp]),
+        "lvc_plan_num_prices": (i64, [vp]),
+        "lvc_plan_set_params": (ctypes.c_int, [vp, vp, ctypes.POINTER(_Calib), i32]),
+        "lvc_plan_run": (ctypes.c_int, [vp, vp]),
+        "lvc_plan_copy_prices": (ctypes.c_int, [vp, vp, vp]),
+        "lvc_plan_device_prices": (vp, [vp]),
+        "lvc_plan_time": (ctypes.c_int, [vp, vp, i32, ctypes.POINTER(f64)]),
+        "lvc_plan_rollback_ms": (f64, [vp]),
+        "lvc_plan_num_launches": (i32, [vp]),
+        "lvc_batch": (ctypes.c_int, [vp, ctypes.POINTER(_Calib), i32, i32, vp]),
+        "lvc_context_stream": (vp, [vp]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    libc = ctypes.CDLL(None)
+    libc.free.argtypes = [vp]
+    L._libc_free = libc.free
+    _lib = L
+    return L
+
+
+def _calib_array(calibs: Sequence[Calibration]):
+    arr = (_Calib * max(1, len(calibs)))()
+    for i, c in enumerate(calibs):
+        arr[i] = _Calib(*astuple(c))
+    return arr
+
+
+class Context:
+    """A futhark_context on one CUDA device ("#N" or a device-name substring)."""
+
+    def __init__(self, device: str | None = None):
+        self.lib = load_library()
+        self._cfg = self.lib.futhark_context_config_new()
+        if device is not None:
+            self.lib.futhark_context_config_set_device(self._cfg, device.encode())
+        self._ctx = self.lib.futhark_context_new(self._cfg)
+        if not self._ctx:
+            raise FutharkError(FUTHARK_OUT_OF_MEMORY, "futhark_context_new failed")
+        err = self._take_error()
+        if err:
+            self.close()
+            raise FutharkError(FUTHARK_PROGRAM_ERROR, err)
+
+    # -- plumbing -----------------------------------------------------------
+    def _take_error(self) -> str:
+        p = self.lib.futhark_context_get_error(self._ctx)
+        if not p:
+            return ""
+        msg = ctypes.cast(p, ctypes.c_char_p).value.decode(errors="replace")
+        self.lib._libc_free(ctypes.cast(p, ctypes.c_void_p))
+        return msg
+
+    def _check(self, rc: int):
+        if rc != 0:
+            raise FutharkError(rc, self._take_error() or "unknown error")
+
+    def close(self):
+        if getattr(self, "_ctx", None):
+            self.lib.futhark_context_free(self._ctx)
+            self._ctx = None
+        if getattr(self, "_cfg", None):
+            self.lib.futhark_context_config_free(self._cfg)
+            self._cfg = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def sync(self):
+        self._check(self.lib.futhark_context_sync(self._ctx))
+
+    @property
+    def stream(self) -> int:
+        return self.lib.lvc_context_stream(self._ctx) or 0
+
+    # -- the entry points ---------------------------------------------------
+    def _array_values(self, arr, kind: str) -> np.ndarray:
+        shape = getattr(self.lib, f"futhark_shape_{kind}_1d")(self._ctx, arr)
+        n = int(shape[0])
+        out = np.empty(n, dtype=np.float32 if kind == "f32" else np.float64)
+        self._check(getattr(self.lib, f"futhark_values_{kind}_1d")(self._ctx, arr, out.ctypes.data))
+        return out
+
+    def main(self, outer, numX, numY, numT, s0, t, alpha, nu, beta) -> np.ndarray:
+        """futhark_entry_main: f32 inputs, f32 prices (computed in f64)."""
+        arr = ctypes.c_void_p()
+        self._check(self.lib.futhark_entry_main(self._ctx, ctypes.byref(arr), outer, numX, numY, numT,
+                                                s0, t, alpha, nu, beta))
+        try:
+            return self._array_values(arr, "f32")
+        finally:
+            self.lib.futhark_free_f32_1d(self._ctx, arr)
+
+    def main_f64(self, outer, numX, numY, numT, s0, t, alpha, nu, beta) -> np.ndarray:
+        """futhark_entry_main_f64: the f64 instantiation of `main`."""
+        arr = ctypes.c_void_p()
+        self._check(self.lib.futhark_entry_main_f64(self._ctx, ctypes.byref(arr), outer, numX, numY,
+                                                    numT, s0, t, alpha, nu, beta))
+        try:
+            return self._array_values(arr, "f64")
+        finally:
+            self.lib.futhark_free_f64_1d(self._ctx, arr)
+
+    # -- batched form -------------------------------------------------------
+    def plan(self, calibs: Sequence[Calibration], precision: int = F64) -> "Plan":
+        return Plan(self, calibs, precision)
+
+    def batch(self, calibs: Sequence[Calibration], precision: int = F64) -> np.ndarray:
+        """lvc_batch: one-shot batched call from host memory; prices concatenated."""
+        arr = _calib_array(calibs)
+        n = sum(c.outer for c in calibs)
+        out = np.empty(max(n, 1), dtype=np.float64)
+        self._check(self.lib.lvc_batch(self._ctx, arr, len(calibs), precision, out.ctypes.data))
+        return out[:n]
+
+
+class Plan:
+    """lvc_plan: device tables, work lists and the captured graph of a batch."""
+
+    def __init__(self, ctx: Context, calibs: Sequence[Calibration], precision: int = F64):
+        self.ctx = ctx
+        self.calibs = list(calibs)
+        self.precision = precision
+        self._p = ctypes.c_void_p()
+        ctx._check(ctx.lib.lvc_plan_new(ctx._ctx, _calib_array(self.calibs), len(self.calibs),
+                                        precision, ctypes.byref(self._p)))
+        self.num_prices = int(ctx.lib.lvc_plan_num_prices(self._p))
+        self.offsets = np.concatenate([[0], np.cumsum([c.outer for c in self.calibs])]).astype(np.int64)
+
+    def run(self):
+        self.ctx._check(self.ctx.lib.lvc_plan_run(self.ctx._ctx, self._p))
+
+    def set_params(self, calibs: Sequence[Calibration]):
+        self.ctx._check(self.ctx.lib.lvc_plan_set_params(self.ctx._ctx, self._p, _calib_array(calibs),
+                                                         len(calibs)))
+        self.calibs = list(calibs)
+
+    def prices(self) -> np.ndarray:
+        out = np.empty(max(self.num_prices, 1), dtype=np.float64)
+        self.ctx._check(self.ctx.lib.lvc_plan_copy_prices(self.ctx._ctx, self._p, out.ctypes.data))
+        return out[: self.num_prices]
+
+    def split(self, prices: np.ndarray) -> List[np.ndarray]:
+        return [prices[self.offsets[i]:self.offsets[i + 1]] for i in range(len(self.calibs))]
+
+    def time(self, iters: int = 3) -> float:
+        """Mean milliseconds per run over `iters` graph launches (CUDA events)."""
+        ms = ctypes.c_double()
+        self.ctx._check(self.ctx.lib.lvc_plan_time(self.ctx._ctx, self._p, iters, ctypes.byref(ms)))
+        return ms.value
+
+    @property
+    def rollback_ms(self) -> float:
+        return float(self.ctx.lib.lvc_plan_rollback_ms(self._p))
+
+    @property
+    def num_launches(self) -> int:
+        return int(self.ctx.lib.lvc_plan_num_launches(self._p))
+
+    @property
+    def device_prices(self) -> int:
+        return int(self.ctx.lib.lvc_plan_device_prices(self._p) or 0)
+
+    def free(self):
+        if self._p:
+            self.ctx.lib.lvc_plan_free(self.ctx._ctx, self._p)
+            self._p = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            if self._p and self.ctx._ctx:
+                self.free()
+        except Exception:
+            pass
+
+
+def run_dataset(ctx: Context, path: str, f64: bool = False) -> np.ndarray:
+    """Run `main` on a reference dataset file (finpar/LocVolCalib-data/*.in)."""
+    from . import futhark_data
+    vals = futhark_data.read_file(path)
+    if len(vals) != 9:
+        raise ValueError(f"{path}: expected the 9 inputs of main, got {len(vals)} values")
+    args = [int(v) for v in vals[:4]] + [float(v) for v in vals[4:]]
+    return ctx.main_f64(*args) if f64 else ctx.main(*args)

@@ -1,0 +1,60 @@
+"""The workloads of the LocVolCalib path: the reference's three datasets and
+seeded synthetic calibration mixes.
+
+* `SMALL`, `MEDIUM`, `LARGE`: the inputs of finpar/LocVolCalib-data/{small,
+  medium,large}.in (16x32x256x256, 128x256x32x64, 256x256x256x64; s0=0.03,
+  t=5, alpha=0.2, nu=0.6, beta=0.5).
+* `uneven_mix(n, seed)`: n calibrations with numX, numY uniform on
+  {32, 64, 128, 256}, numT uniform on [32, 256], s0 ~ U[0.02, 0.05],
+  alpha ~ U[0.1, 0.3], nu ~ U[0.4, 0.8], beta ~ U[0.3, 0.7], t ~ U[1, 10],
+  outer uniform on [8, 64] (strikes 0.001*i as in `main`).  The reference
+  suite has no such dataset; this seeded generator stands in for it with the
+  value ranges of the reference's own inputs around them.
+* `poisson_arrivals(rate, n, seed)`: arrival times of a Poisson request stream.
+"""
+from __future__ import annotations
+
+from typing import List
+
+import numpy as np
+
+from . import Calibration
+
+REF = dict(s0=0.03, t=5.0, alpha=0.2, nu=0.6, beta=0.5)
+SMALL = Calibration(16, 32, 256, 256, **REF)
+MEDIUM = Calibration(128, 256, 32, 64, **REF)
+LARGE = Calibration(256, 256, 256, 64, **REF)
+DATASETS = {"small": SMALL, "medium": MEDIUM, "large": LARGE}
+
+GRID_SIZES = (32, 64, 128, 256)
+
+
+def uneven_mix(n: int = 512, seed: int = 0, sizes=GRID_SIZES, numT=(32, 256),
+               outer=(8, 64)) -> List[Calibration]:
+    rng = np.random.default_rng(seed)
+    X = rng.choice(np.asarray(sizes), size=n)
+    Y = rng.choice(np.asarray(sizes), size=n)
+    T = rng.integers(numT[0], numT[1] + 1, size=n)
+    s0 = rng.uniform(0.02, 0.05, size=n)
+    alpha = rng.uniform(0.1, 0.3, size=n)
+    nu = rng.uniform(0.4, 0.8, size=n)
+    beta = rng.uniform(0.3, 0.7, size=n)
+    t = rng.uniform(1.0, 10.0, size=n)
+    O = rng.integers(outer[0], outer[1] + 1, size=n)
+    return [Calibration(int(O[i]), int(X[i]), int(Y[i]), int(T[i]), float(s0[i]), float(t[i]),
+                        float(alpha[i]), float(nu[i]), float(beta[i])) for i in range(n)]
+
+
+def total_options(calibs) -> int:
+    return int(sum(c.outer for c in calibs))
+
+
+def total_work(calibs) -> int:
+    """Option-cell-steps: sum of outer * numX * numY * (numT - 1)."""
+    return int(sum(c.work() for c in calibs))
+
+
+def poisson_arrivals(rate: float, n: int, seed: int = 0) -> np.ndarray:
+    """Arrival times (seconds) of n requests of a Poisson process of `rate` per second."""
+    rng = np.random.default_rng(seed)
+    return np.cumsum(rng.exponential(1.0 / rate, size=n))

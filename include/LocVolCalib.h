@@ -1,0 +1,163 @@
+/*
+ * LocVolCalib.h -- C API of the B200 LocVolCalib engine (liblvc.so).
+ *
+ * Part 1 is the header that `futhark cuda --library finpar/LocVolCalib.fut`
+ * would generate for the reference program: the same context/config life
+ * cycle, the same `futhark_entry_main` signature (outputs first, then the nine
+ * scalar inputs of `main`, finpar/LocVolCalib.fut:238-246) and the same array
+ * accessors.  A C host written against the generated library links against
+ * liblvc.so instead, unchanged.  The shape of that API is witnessed in the
+ * reference by its in-repo consumer, the lys front-end (cited per function).
+ *
+ * Part 2 adds the f64 twin of the entry point and the engine's batched and
+ * serving forms, which have no counterpart in the generated API.
+ *
+ * Conventions (as in the generated API): functions returning int return 0 on
+ * success and a non-zero error code on failure, with a message available from
+ * futhark_context_get_error.  Invalid sizes are reported as errors, never by
+ * aborting the process.
+ */
+#ifndef LOCVOLCALIB_B200_H
+#define LOCVOLCALIB_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define LVC_API __attribute__((visibility("default")))
+#else
+#define LVC_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Error codes of the generated API. */
+#define FUTHARK_SUCCESS 0
+#define FUTHARK_PROGRAM_ERROR 2
+#define FUTHARK_OUT_OF_MEMORY 3
+
+/* ---------------- Part 1: the generated-library API ---------------- */
+
+struct futhark_context_config;
+struct futhark_context;
+struct futhark_f32_1d;
+struct futhark_f64_1d;
+
+/* lys/shared.c:20 */
+LVC_API struct futhark_context_config *futhark_context_config_new(void);
+/* lys/sdl/main.c:272 */
+LVC_API void futhark_context_config_free(struct futhark_context_config *cfg);
+/* lys/shared.c:25 -- "#N" selects CUDA device N, otherwise the first device
+ * whose name contains the string. */
+LVC_API void futhark_context_config_set_device(struct futhark_context_config *cfg, const char *s);
+LVC_API void futhark_context_config_set_debugging(struct futhark_context_config *cfg, int flag);
+LVC_API void futhark_context_config_set_profiling(struct futhark_context_config *cfg, int flag);
+LVC_API void futhark_context_config_set_logging(struct futhark_context_config *cfg, int flag);
+/* lys/shared.c:44 -- accepted for compatibility; the engine has no kernel
+ * cache file (its kernels are compiled ahead of time for sm_100a). */
+LVC_API void futhark_context_config_set_cache_file(struct futhark_context_config *cfg, const char *f);
+
+/* lys/shared.c:47 -- returns NULL only on allocation failure; a context whose
+ * device could not be initialised reports that from futhark_context_get_error. */
+LVC_API struct futhark_context *futhark_context_new(struct futhark_context_config *cfg);
+/* lys/sdl/main.c:271 */
+LVC_API void futhark_context_free(struct futhark_context *ctx);
+/* lys/sdl/main.c:109,134 -- waits for all work of the context. */
+LVC_API int futhark_context_sync(struct futhark_context *ctx);
+/* lys/shared.h:21-26 -- the last error message, malloc'd (caller frees), or
+ * NULL if there was none; retrieving it clears it. */
+LVC_API char *futhark_context_get_error(struct futhark_context *ctx);
+/* Releases cached device memory of the context. */
+LVC_API int futhark_context_clear_caches(struct futhark_context *ctx);
+
+LVC_API struct futhark_f32_1d *futhark_new_f32_1d(struct futhark_context *ctx, const float *data,
+                                          int64_t dim0);
+LVC_API struct futhark_f64_1d *futhark_new_f64_1d(struct futhark_context *ctx, const double *data,
+                                          int64_t dim0);
+/* lys/sdl/main.c:131 */
+LVC_API int futhark_free_f32_1d(struct futhark_context *ctx, struct futhark_f32_1d *arr);
+LVC_API int futhark_free_f64_1d(struct futhark_context *ctx, struct futhark_f64_1d *arr);
+/* lys/sdl/liblys.c:151 -- copies the array to host memory (synchronous). */
+LVC_API int futhark_values_f32_1d(struct futhark_context *ctx, struct futhark_f32_1d *arr, float *data);
+LVC_API int futhark_values_f64_1d(struct futhark_context *ctx, struct futhark_f64_1d *arr, double *data);
+/* lys/shared.c:79 */
+LVC_API const int64_t *futhark_shape_f32_1d(struct futhark_context *ctx, struct futhark_f32_1d *arr);
+LVC_API const int64_t *futhark_shape_f64_1d(struct futhark_context *ctx, struct futhark_f64_1d *arr);
+
+/*
+ * The entry point `main` (finpar/LocVolCalib.fut:238-252; calling convention
+ * of lys/sdl/main.c:108,124,130).  Prices of the strikes 0.001*i,
+ * i < outer_loop_count.  The engine computes in f64 and rounds each price to
+ * f32 once.  Errors: numX < 3, numY < 3, numT < 1, outer_loop_count < 0,
+ * numX > 512, or an initGrid spot index outside [0, numX) (the cases where the
+ * reference program fails an index or size check).
+ */
+LVC_API int futhark_entry_main(struct futhark_context *ctx, struct futhark_f32_1d **out0,
+                       const int32_t outer_loop_count, const int32_t numX, const int32_t numY,
+                       const int32_t numT, const float s0, const float t, const float alpha,
+                       const float nu, const float beta);
+
+/* ---------------- Part 2: engine extensions ---------------- */
+
+/* `main` instantiated at f64 (what the generated library of an f64 build of
+ * finpar/LocVolCalib.fut would export); same errors as futhark_entry_main. */
+LVC_API int futhark_entry_main_f64(struct futhark_context *ctx, struct futhark_f64_1d **out0,
+                           const int32_t outer_loop_count, const int32_t numX,
+                           const int32_t numY, const int32_t numT, const double s0,
+                           const double t, const double alpha, const double nu,
+                           const double beta);
+
+/* One calibration: the nine scalar inputs of `main`. */
+struct lvc_calibration {
+  int32_t outer, numX, numY, numT;
+  double s0, t, alpha, nu, beta;
+};
+
+/* State precision of the rollback.  LVC_F64: every operation in f64.
+ * LVC_F32_STATE: grid state and stencils in f32; the tridiagonal pivot
+ * divisions and the payoff stay in f64. */
+enum { LVC_F64 = 0, LVC_F32_STATE = 1 };
+
+/* A batch plan: the device tables, work lists and captured CUDA graph for a
+ * fixed list of calibrations.  Prices of calibration c are at offset
+ * sum_{c' < c} outer[c'] of the price vector. */
+struct lvc_plan;
+
+LVC_API int lvc_plan_new(struct futhark_context *ctx, const struct lvc_calibration *calibs, int32_t n,
+                 int32_t precision, struct lvc_plan **plan);
+LVC_API int lvc_plan_free(struct futhark_context *ctx, struct lvc_plan *plan);
+LVC_API int64_t lvc_plan_num_prices(const struct lvc_plan *plan);
+/* Re-uploads the scalar inputs of a plan (sizes must be unchanged). */
+LVC_API int lvc_plan_set_params(struct futhark_context *ctx, struct lvc_plan *plan,
+                        const struct lvc_calibration *calibs, int32_t n);
+/* Runs the whole batch (setup, pivot and rollback kernels, one graph launch)
+ * asynchronously on the context's stream; prices stay in device memory. */
+LVC_API int lvc_plan_run(struct futhark_context *ctx, struct lvc_plan *plan);
+/* Synchronises and copies the prices to host memory (n = lvc_plan_num_prices). */
+LVC_API int lvc_plan_copy_prices(struct futhark_context *ctx, struct lvc_plan *plan, double *prices);
+/* Device address of the plan's price vector (valid until lvc_plan_free). */
+LVC_API const double *lvc_plan_device_prices(const struct lvc_plan *plan);
+/* Times `iters` back-to-back runs with CUDA events on the context stream;
+ * writes the mean milliseconds per run. */
+LVC_API int lvc_plan_time(struct futhark_context *ctx, struct lvc_plan *plan, int32_t iters,
+                  double *ms_per_run);
+/* Per-launch device time of the rollback kernel(s) of the last lvc_plan_time
+ * (milliseconds, summed over the plan's rollback launches, mean per run). */
+LVC_API double lvc_plan_rollback_ms(const struct lvc_plan *plan);
+/* Number of kernel launches one lvc_plan_run performs. */
+LVC_API int32_t lvc_plan_num_launches(const struct lvc_plan *plan);
+
+/* One-shot batched call from host memory: plan, run, copy back, free. */
+LVC_API int lvc_batch(struct futhark_context *ctx, const struct lvc_calibration *calibs, int32_t n,
+              int32_t precision, double *prices);
+
+/* The cudaStream_t the context launches on (as void*). */
+LVC_API void *lvc_context_stream(struct futhark_context *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LOCVOLCALIB_B200_H */

@@ -1,0 +1,104 @@
+"""ctypes binding of the CPU oracle (liblvc_oracle.so) -- TEST INFRASTRUCTURE ONLY.
+
+Importers: tests/, __graft_entry__.smoke() and bench.py's CPU-baseline and
+reference legs.  The engine never imports this module.
+
+The oracle restates finpar/LocVolCalib.fut line by line (see lvc_oracle.cpp);
+`main_f32`/`main_f64` are the reference `main` at f32 (the reference's own
+precision) and at f64.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from typing import Sequence
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liblvc_oracle.so")
+_lib = None
+
+
+def load():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB):
+        subprocess.run(["make", "-C", HERE, "--no-print-directory"], check=True)
+    L = ctypes.CDLL(LIB)
+    i32, i64, f32, f64, vp = ctypes.c_int32, ctypes.c_int64, ctypes.c_float, ctypes.c_double, ctypes.c_void_p
+    L.lvc_oracle_main_f32.argtypes = [i32] * 4 + [f32] * 5 + [vp, ctypes.c_int, ctypes.c_int]
+    L.lvc_oracle_main_f32.restype = ctypes.c_int
+    L.lvc_oracle_main_f64.argtypes = [i32] * 4 + [f64] * 5 + [vp, ctypes.c_int, ctypes.c_int]
+    L.lvc_oracle_main_f64.restype = ctypes.c_int
+    L.lvc_oracle_value_f64.argtypes = [i32] * 3 + [f64] * 6 + [ctypes.c_int]
+    L.lvc_oracle_value_f64.restype = f64
+    L.lvc_oracle_value_f32.argtypes = [i32] * 3 + [f32] * 6 + [ctypes.c_int]
+    L.lvc_oracle_value_f32.restype = f32
+    L.lvc_oracle_xindex_f64.argtypes = [i32, f64, f64, f64]
+    L.lvc_oracle_xindex_f64.restype = ctypes.c_int
+    L.lvc_oracle_batch_f64.argtypes = [i32] + [vp] * 9 + [vp, vp, ctypes.c_int]
+    L.lvc_oracle_batch_f64.restype = ctypes.c_int
+    for name in ("lvc_oracle_tridag_par_f32", "lvc_oracle_tridag_par_f64",
+                 "lvc_oracle_tridag_seq_f32", "lvc_oracle_tridag_seq_f64"):
+        fn = getattr(L, name)
+        fn.argtypes = [i64, i64] + [vp] * 5
+        fn.restype = None
+    L.lvc_oracle_max_threads.restype = ctypes.c_int
+    _lib = L
+    return L
+
+
+def max_threads() -> int:
+    return int(load().lvc_oracle_max_threads())
+
+
+def main_f32(outer, numX, numY, numT, s0, t, alpha, nu, beta, threads=0, seq=False) -> np.ndarray:
+    out = np.zeros(max(outer, 1), dtype=np.float32)
+    rc = load().lvc_oracle_main_f32(outer, numX, numY, numT, s0, t, alpha, nu, beta,
+                                    out.ctypes.data, threads, int(seq))
+    if rc:
+        raise ValueError("oracle: invalid inputs")
+    return out[:outer]
+
+
+def main_f64(outer, numX, numY, numT, s0, t, alpha, nu, beta, threads=0, seq=False) -> np.ndarray:
+    out = np.zeros(max(outer, 1), dtype=np.float64)
+    rc = load().lvc_oracle_main_f64(outer, numX, numY, numT, s0, t, alpha, nu, beta,
+                                    out.ctypes.data, threads, int(seq))
+    if rc:
+        raise ValueError("oracle: invalid inputs")
+    return out[:outer]
+
+
+def value_f64(numX, numY, numT, s0, strike, t, alpha, nu, beta, seq=False) -> float:
+    return float(load().lvc_oracle_value_f64(numX, numY, numT, s0, strike, t, alpha, nu, beta, int(seq)))
+
+
+def batch_f64(calibs: Sequence, threads=0) -> np.ndarray:
+    """Prices of many calibrations (objects with the nine fields of `main`), concatenated."""
+    n = len(calibs)
+    cols = {k: np.array([getattr(c, k) for c in calibs], dtype=np.int32 if k in ("outer", "numX", "numY", "numT") else np.float64)
+            for k in ("outer", "numX", "numY", "numT", "s0", "t", "alpha", "nu", "beta")}
+    offsets = np.concatenate([[0], np.cumsum(cols["outer"])]).astype(np.int64)
+    out = np.zeros(max(int(offsets[-1]), 1), dtype=np.float64)
+    rc = load().lvc_oracle_batch_f64(n, *[cols[k].ctypes.data for k in
+                                          ("outer", "numX", "numY", "numT", "s0", "t", "alpha", "nu", "beta")],
+                                     offsets.ctypes.data, out.ctypes.data, threads)
+    if rc:
+        raise ValueError("oracle: invalid inputs")
+    return out[:offsets[-1]]
+
+
+def tridag(a, b, c, y, form="par") -> np.ndarray:
+    a = np.ascontiguousarray(a)
+    dt = a.dtype
+    b, c, y = (np.ascontiguousarray(v, dtype=dt) for v in (b, c, y))
+    rows, n = a.shape
+    out = np.zeros_like(a)
+    name = f"lvc_oracle_tridag_{form}_{'f32' if dt == np.float32 else 'f64'}"
+    getattr(load(), name)(rows, n, a.ctypes.data, b.ctypes.data, c.ctypes.data, y.ctypes.data,
+                          out.ctypes.data)
+    return out

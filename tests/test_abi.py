@@ -1,0 +1,60 @@
+"""The C-ABI library without a GPU: it loads, exports every function that
+include/*.h declares, and a context on a machine without a usable device
+reports an error instead of crashing."""
+import ctypes
+import glob
+import os
+import re
+
+import pytest
+
+from conftest import REPO
+
+HEADERS = sorted(glob.glob(os.path.join(REPO, "include", "*.h")))
+DECL = re.compile(r"^LVC_API\s+[^(]*?\b([a-z_][a-z_0-9]*)\s*\(", re.M)
+
+
+def declared_functions():
+    names = []
+    for h in HEADERS:
+        with open(h) as f:
+            names += DECL.findall(f.read())
+    return names
+
+
+def test_headers_declare_the_generated_api():
+    names = set(declared_functions())
+    for required in ("futhark_context_config_new", "futhark_context_new", "futhark_entry_main",
+                     "futhark_values_f32_1d", "futhark_shape_f32_1d", "futhark_free_f32_1d",
+                     "futhark_context_sync", "futhark_context_get_error", "futhark_context_free",
+                     "futhark_context_config_free", "futhark_context_config_set_device"):
+        assert required in names
+
+
+def test_library_exports_every_declared_symbol(pkg):
+    lib = ctypes.CDLL(pkg.LIB_PATH)
+    missing = [n for n in declared_functions() if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_python_mirror_binds_every_symbol(pkg):
+    pkg.load_library()  # raises if a signature names a missing symbol
+
+
+def test_context_without_gpu_reports_error(pkg):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(pkg.FutharkError) as ei:
+        pkg.Context()
+    assert ei.value.code == pkg.FUTHARK_PROGRAM_ERROR
+
+
+def test_config_api_is_callable_without_gpu(pkg):
+    lib = pkg.load_library()
+    cfg = lib.futhark_context_config_new()
+    assert cfg
+    lib.futhark_context_config_set_device(cfg, b"#0")
+    lib.futhark_context_config_set_debugging(cfg, 1)
+    lib.futhark_context_config_set_cache_file(cfg, b"/nonexistent")
+    lib.futhark_context_config_free(cfg)

@@ -1,0 +1,112 @@
+"""The CPU oracle pinned against the reference's own golden data (no GPU).
+
+* finpar/LocVolCalib-data/{small,medium,large}.out: prices of the reference's
+  f32 program.  Those files are f32 results printed to 6 significant digits
+  (large: 6 decimals), and they differ from the f64 solution by up to
+  2.8e-6 absolute; the restated f32 and f64 oracles must both land within
+  5e-6 absolute of every golden price.
+* misc/ocean-sim/data/tridiag32-small.{in,out}: the sequential Thomas solver
+  restated from misc/ocean-sim/tridiag.fut:81-95 reproduces the golden file
+  bit for bit.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, dataset_args
+
+GOLDEN_ABS_TOL = 5e-6
+
+
+@pytest.mark.parametrize("name", ["small", "medium"])
+def test_oracle_f32_matches_reference_outputs(oracle, golden, name):
+    e = golden[name]
+    got = oracle.main_f32(*dataset_args(e)).astype(np.float64)
+    exp = np.asarray(e["expected_f32"], dtype=np.float64)
+    assert got.shape == exp.shape
+    assert np.max(np.abs(got - exp)) <= GOLDEN_ABS_TOL
+
+
+@pytest.mark.parametrize("name", ["small", "medium"])
+def test_oracle_f64_matches_reference_outputs(oracle, golden, name):
+    e = golden[name]
+    got = oracle.main_f64(*dataset_args(e))
+    exp = np.asarray(e["expected_f32"], dtype=np.float64)
+    assert np.max(np.abs(got - exp)) <= GOLDEN_ABS_TOL
+
+
+@pytest.mark.slow
+def test_oracle_large_matches_reference_outputs(oracle, golden):
+    e = golden["large"]
+    exp = np.asarray(e["expected_f32"], dtype=np.float64)
+    got32 = oracle.main_f32(*dataset_args(e)).astype(np.float64)
+    assert np.max(np.abs(got32 - exp)) <= GOLDEN_ABS_TOL
+    got64 = oracle.main_f64(*dataset_args(e))
+    assert np.max(np.abs(got64 - exp)) <= GOLDEN_ABS_TOL
+
+
+def test_tridag_seq_reproduces_golden_bit_exact(oracle):
+    z = np.load(os.path.join(GOLDEN, "tridiag32_small.npz"))
+    x = oracle.tridag(z["a"], z["b"], z["c"], z["y"], form="seq")
+    assert x.dtype == np.float32
+    assert np.array_equal(x, z["x"])
+
+
+def test_tridag_scan_form_agrees_with_thomas_f64(oracle):
+    z = np.load(os.path.join(GOLDEN, "tridiag32_small.npz"))
+    a, b, c, y = (z[k].astype(np.float64) for k in "abcy")
+    xp = oracle.tridag(a, b, c, y, form="par")
+    xs = oracle.tridag(a, b, c, y, form="seq")
+    # the fixture's systems are not diagonally dominant; the two f64 forms
+    # still agree to ~1e-9 of the solution's scale, row by row
+    scale = np.max(np.abs(xs), axis=1, keepdims=True)
+    assert np.max(np.abs(xp - xs) / scale) < 1e-8
+
+
+def test_tridag_diagonally_dominant_forms_agree(oracle):
+    rng = np.random.default_rng(7)
+    rows, n = 64, 200
+    a = rng.uniform(-1, 1, (rows, n))
+    c = rng.uniform(-1, 1, (rows, n))
+    b = np.abs(a) + np.abs(c) + rng.uniform(0.5, 2, (rows, n))
+    y = rng.uniform(-1, 1, (rows, n))
+    xp = oracle.tridag(a, b, c, y, form="par")
+    xs = oracle.tridag(a, b, c, y, form="seq")
+    assert np.max(np.abs(xp - xs)) < 1e-13
+    # and both solve the system
+    r = b * xs + np.pad(a[:, 1:] * xs[:, :-1], ((0, 0), (1, 0))) + np.pad(c[:, :-1] * xs[:, 1:], ((0, 0), (0, 1)))
+    assert np.max(np.abs(r - y)) < 1e-12
+
+
+def test_value_scan_vs_thomas_f64(oracle):
+    # the whole rollback with the two tridiagonal formulations
+    args = (24, 20, 30, 0.03, 0.004, 5.0, 0.2, 0.6, 0.5)
+    v_par = oracle.value_f64(*args, seq=False)
+    v_seq = oracle.value_f64(*args, seq=True)
+    assert abs(v_par - v_seq) <= 1e-13 * abs(v_seq)
+
+
+def test_numT_one_is_the_payoff(oracle):
+    # no time step: res[myYindex, myXindex] of setPayoff, i.e. max(s0 - strike, 0)
+    out = oracle.main_f64(5, 16, 16, 1, 0.03, 5.0, 0.2, 0.6, 0.5)
+    strikes = 0.001 * np.arange(5)
+    assert np.allclose(out, np.maximum(0.03 - strikes, 0.0), rtol=0, atol=1e-16)
+
+
+def test_invalid_sizes_rejected(oracle):
+    with pytest.raises(ValueError):
+        oracle.main_f64(4, 2, 16, 8, 0.03, 5.0, 0.2, 0.6, 0.5)
+    with pytest.raises(ValueError):
+        oracle.main_f64(4, 16, 16, 0, 0.03, 5.0, 0.2, 0.6, 0.5)
+
+
+def test_batch_equals_per_calibration(oracle, pkg):
+    from importlib import import_module
+    wl = import_module("futhark-benchmarks_b200.workloads")
+    calibs = wl.uneven_mix(4, seed=3, sizes=(16, 24), numT=(4, 9), outer=(1, 4))
+    got = oracle.batch_f64(calibs)
+    exp = np.concatenate([oracle.main_f64(*[getattr(c, k) for k in
+                                           ("outer", "numX", "numY", "numT", "s0", "t", "alpha", "nu", "beta")])
+                          for c in calibs])
+    assert np.array_equal(got, exp)
