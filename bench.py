@@ -1,0 +1,361 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 LocVolCalib engine (finpar/LocVolCalib.fut).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload uneven|small|medium|large] [--precision f64|f32state]
+
+One step = one pass of the hot path over one batch: the whole batched run of
+the workload (setup kernel + pivot kernel + persistent rollback kernels, one
+CUDA-graph launch).  Default workload: the uneven calibration mix (512
+calibrations from seed 0: numX, numY in {32,64,128,256}, numT in [32,256],
+outer in [8,64]), f64.  `value` is options/s over all ranks with the
+calibration parameters resident on the device; `e2e` is the same through the
+C ABI with host buffers (parameters uploaded, prices read back every step).
+The plain per-call form (futhark_entry_main_f64 once per calibration) is timed
+on the same workload beside it.
+
+Under torchrun each rank runs its own mix (seed + rank; weak scaling, no
+collective on the data path); times are the max over ranks.
+`--impl reference` times the reference algorithm's CPU restatement (the
+reference's own Futhark build cannot be compiled here) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+if REPO not in sys.path:
+    sys.path.insert(0, REPO)
+
+METRIC = "options/sec, batched uneven LocVolCalib mix on one B200 (f64, <=1e-9 rel vs FP64 oracle)"
+UNIT = "options/s"
+# Algorithmic FP64 flops per option-cell-step, counted from the reference
+# formulas with the provably-zero drift terms removed (plus 1 exp + 1 log,
+# not counted): VarX 4, explicit X 11, combine 3, explicit Y 11, combine 1,
+# implicit-X coefficients 12, tridiagonal X 10, combine 3, implicit-Y
+# coefficients 12, tridiagonal Y 10.
+F_ALG = 77
+CALIB_DEV_BYTES = 96  # sizeof(lvc::CalibDev), uploaded per calibration per step
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="uneven", choices=["uneven", "small", "medium", "large"])
+    ap.add_argument("--calibs", type=int, default=512)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--precision", default="f64", choices=["f64", "f32state"])
+    ap.add_argument("--plain-calibs", type=int, default=0,
+                    help="time the plain per-call form on the first N calibrations (0 = all)")
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0,
+                    help="target CPU time of the bounded CPU-baseline sample")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def workload(args, rank):
+    wl = importlib.import_module("futhark-benchmarks_b200.workloads")
+    if args.workload == "uneven":
+        calibs = wl.uneven_mix(args.calibs, seed=args.seed + rank)
+        desc = {"workload": f"uneven LocVolCalib mix: {args.calibs} calibrations, seed {args.seed}+rank, "
+                            "numX,numY in {32,64,128,256}, numT in [32,256], outer in [8,64]"}
+    else:
+        calibs = [wl.DATASETS[args.workload]]
+        c = calibs[0]
+        desc = {"workload": f"LocVolCalib {args.workload}.in: outer={c.outer} numX={c.numX} "
+                            f"numY={c.numY} numT={c.numT}"}
+    return calibs, desc
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap,utilization.gpu")
+
+    def __init__(self, device: int):
+        self.rows = []
+        self.proc = None
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(device)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.3)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+        rows = self.rows
+        loaded = [r for r in rows if (num(r[8]) or 0) > 50] or rows
+        sm = [num(r[0]) for r in loaded if num(r[0]) is not None]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in loaded:
+            for n, v in zip(names, r[4:8]):
+                if v.strip().lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": num(rows[0][1]) if rows else None,
+                "power_w_max": max((num(r[2]) or 0) for r in rows) if rows else None,
+                "samples": len(rows), "samples_under_load": len(loaded),
+                "reasons": sorted(reasons)}
+
+
+def pick_sample(calibs, target_s):
+    """Leading calibrations of the workload worth about target_s of oracle time
+    on all host threads (the mix is in random order, so this is a fair sample)."""
+    from oracle import oracle
+    threads = oracle.max_threads()
+    p = calibs[0]
+    probe = type(p)(threads, p.numX, p.numY, min(p.numT, 9), p.s0, p.t, p.alpha, p.nu, p.beta)
+    t0 = time.perf_counter()
+    oracle.batch_f64([probe], threads=threads)
+    rate = probe.work() / max(time.perf_counter() - t0, 1e-6)  # option-cell-steps/s
+    budget = target_s * rate
+    sample, work = [], 0
+    for c in calibs:
+        if sample and work + c.work() > budget:
+            break
+        sample.append(c)
+        work += c.work()
+    return sample, threads
+
+
+def cpu_baseline(calibs, target_s):
+    """Time the oracle (CPU restatement of the reference) on a bounded sample."""
+    from oracle import oracle
+    sample, threads = pick_sample(calibs, target_s)
+    t0 = time.perf_counter()
+    oracle.batch_f64(sample, threads=threads)
+    dt = time.perf_counter() - t0
+    opts = sum(c.outer for c in sample)
+    work = sum(c.work() for c in sample)
+    return {"value": opts / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"first {len(sample)} calibrations of the workload ({opts} options, "
+                      f"{work:.3e} option-cell-steps), f64 oracle, {dt:.1f} s"}
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    calibs, desc = workload(args, 0)
+    from oracle import oracle
+    per_step = max(2.0, args.cpu_seconds * 8.0 / max(1, args.steps + args.warmup))
+    sample, threads = pick_sample(calibs, per_step)
+    opts = sum(c.outer for c in sample)
+    work = sum(c.work() for c in sample)
+    for _ in range(args.warmup):
+        oracle.batch_f64(sample[: max(1, len(sample) // 4)], threads=threads)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        oracle.batch_f64(sample, threads=threads)
+        times.append(time.perf_counter() - t0)
+    total = sum(times)
+    value = opts * args.steps / total
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "config": desc, "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"each step: first {len(sample)} calibrations of the workload "
+                                       f"({opts} options, {work:.3e} option-cell-steps)"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "the reference's Futhark multicore build cannot be compiled on this image (no "
+                    "futhark compiler); this arm times the line-by-line C++ restatement of "
+                    "finpar/LocVolCalib.fut on all host threads"}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+    rank, world, local = dist_env()
+    pkg = importlib.import_module("futhark-benchmarks_b200")
+    wl = importlib.import_module("futhark-benchmarks_b200.workloads")
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier(device_ids=[local])
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        import torch.distributed as dist
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        import torch.distributed as dist
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        return float(t.item())
+
+    calibs, desc = workload(args, rank)
+    precision = pkg.F64 if args.precision == "f64" else pkg.F32_STATE
+    ctx = pkg.Context(f"#{local}")
+    fp64_peak, smem_peak = ctx.probe_peaks()
+    plan = ctx.plan(calibs, precision=precision)
+    ext = torch.cuda.ExternalStream(ctx.stream, device=f"cuda:{local}")
+    n_opts = wl.total_options(calibs)
+    work = wl.total_work(calibs)
+
+    # ---- device-resident timing (value) ----
+    for _ in range(args.warmup):
+        plan.run()
+    ctx.sync()
+    barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(ext)
+    for _ in range(args.steps):
+        plan.run()
+    ev1.record(ext)
+    ctx.sync()
+    torch.cuda.synchronize()
+    barrier()
+    ms = ev0.elapsed_time(ev1)
+    clk = clocks.stop()
+    ms_max = max_over_ranks(ms)
+    value = sum_over_ranks(n_opts) * args.steps / (ms_max * 1e-3)
+
+    # ---- the rollback kernel alone (events around each rollback launch) ----
+    plan.time(max(1, args.steps))
+    roll_ms = plan.rollback_ms
+    achieved = F_ALG * work / (roll_ms * 1e-3) / 1e12
+
+    # ---- end to end through the C ABI with host buffers ----
+    for _ in range(1):
+        plan.set_params(calibs)
+        plan.run()
+        plan.prices()
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        plan.set_params(calibs)  # host -> device: the calibration parameters
+        plan.run()
+        prices = plan.prices()   # device -> host: the price vector
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    e2e = sum_over_ranks(n_opts) * args.steps / e2e_s
+    # one-shot batched call (plan build + run + copy + free), once
+    t0 = time.perf_counter()
+    ctx.batch(calibs, precision=precision)
+    oneshot = n_opts / (time.perf_counter() - t0)
+
+    # ---- plain per-call form on the same workload ----
+    plain = None
+    if not args.no_plain:
+        sub = calibs if args.plain_calibs <= 0 else calibs[: args.plain_calibs]
+        c0 = sub[0]
+        ctx.main_f64(c0.outer, c0.numX, c0.numY, c0.numT, c0.s0, c0.t, c0.alpha, c0.nu, c0.beta)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for c in sub:
+            ctx.main_f64(c.outer, c.numX, c.numY, c.numT, c.s0, c.t, c.alpha, c.nu, c.beta)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        plain = {"value": sum(c.outer for c in sub) / dt, "unit": UNIT,
+                 "calls": len(sub), "form": "futhark_entry_main_f64 once per calibration"}
+
+    cpu = None
+    if rank == 0 and world == 1:
+        cpu = cpu_baseline(calibs, args.cpu_seconds)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if precision == pkg.F64 else "f32-state (f64 pivots)",
+            "data": "synthetic (seeded calibration parameters; no dataset)",
+            "config": dict(desc, precision=args.precision, options_per_rank=n_opts,
+                           option_cell_steps_per_rank=work,
+                           l2="inputs larger than L2: the per-step pivot tables of the mix exceed 126 MB"),
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": CALIB_DEV_BYTES * len(calibs),
+                    "d2h_bytes_per_step": 8 * n_opts, "oneshot_value": oneshot,
+                    "path": "lvc_plan_set_params + lvc_plan_run + lvc_plan_copy_prices"},
+            "gpu_launches": args.steps * plan.num_launches,
+            "roofline": {"bound": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
+                         "frac": achieved / fp64_peak, "traffic": None,
+                         "kernel": "lvc_rollback_kernel (sum of its launches)",
+                         "flops_per_unit": F_ALG, "unit_of_work": "option-cell-step",
+                         "units_per_step": work, "kernel_ms_per_step": roll_ms,
+                         "peak_source": "measured live: lvc_probe_dfma_kernel on this GPU "
+                                        "(MEASURED_PEAKS.json has no FP64 figure)",
+                         "smem_peak_gbs": smem_peak},
+            "plain_per_call": plain,
+            "batched_vs_plain": (value / plain["value"]) if plain else None,
+            "cpu_baseline": cpu,
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    plan.free()
+    ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

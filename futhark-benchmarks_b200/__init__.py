@@ -113,6 +113,7 @@ def load_library(path: str = LIB_PATH):
         "lvc_plan_num_launches": (i32, [vp]),
         "lvc_batch": (ctypes.c_int, [vp, ctypes.POINTER(_Calib), i32, i32, vp]),
         "lvc_context_stream": (vp, [vp]),
+        "lvc_probe_peaks": (ctypes.c_int, [vp, ctypes.POINTER(f64), ctypes.POINTER(f64)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -187,6 +188,12 @@ class Context:
     @property
     def stream(self) -> int:
         return self.lib.lvc_context_stream(self._ctx) or 0
+
+    def probe_peaks(self):
+        """(FP64 TFLOP/s, shared-memory GB/s) measured on this context's device."""
+        f, s = ctypes.c_double(), ctypes.c_double()
+        self._check(self.lib.lvc_probe_peaks(self._ctx, ctypes.byref(f), ctypes.byref(s)))
+        return f.value, s.value
 
     # -- the entry points ---------------------------------------------------
     def _array_values(self, arr, kind: str) -> np.ndarray:

@@ -46,7 +46,8 @@ __global__ void __launch_bounds__(256) lvc_setup_kernel(const CalibDev* __restri
                                                         double* __restrict__ tabs) {
   const CalibDev c = calibs[blockIdx.x];
   const int X = c.numX, Y = c.numY, T = c.numT, Xp = c.Xp;
-  const TabLayout L = tab_layout(X, Y, T, Xp);
+  const bool line = c.kind == kKindLine;
+  const TabLayout L = tab_layout(X, Y, T, Xp, c.kind);
   double* tab = tabs + c.tab;
   const int tid = threadIdx.x, nt = blockDim.x;
 
@@ -82,6 +83,12 @@ __global__ void __launch_bounds__(256) lvc_setup_kernel(const CalibDev* __restri
     cc[2] = h1;
     cc[3] = h2;
     tab[L.x + i] = xv;
+    // line family: W_k = 0.25 * eX_i * Dxx_i[k], so that 0.5 * (0.5 * VarX * Dxx[k]) = e_j * W_k
+    if (line && i < L.xa) {
+      tab[L.wcol + i] = 0.5 * (e * h0);
+      tab[L.wcol + L.xa + i] = 0.5 * (e * h1);
+      tab[L.wcol + 2 * L.xa + i] = 0.5 * (e * h2);
+    }
   }
   // Row tables: 0.5 * nu^2 * Dyy_j[k]
   for (int j = tid; j < Y; j += nt) {
@@ -112,8 +119,11 @@ __global__ void __launch_bounds__(256) lvc_setup_kernel(const CalibDev* __restri
     const int k = (int)(e / Y), j = (int)(e % Y);
     const double tn = __ddiv_rn(__dmul_rn(c.t, (double)k), tden);
     const double yj = grid_pt(j, dy, yidx, logAlpha);
-    tab[L.eyt + (int64_t)k * L.eyt_ld + j] =
-        exp(__dmul_rn(2.0, __dsub_rn(yj, __dmul_rn(half_nu_nu, tn))));
+    const double ev = exp(__dmul_rn(2.0, __dsub_rn(yj, __dmul_rn(half_nu_nu, tn))));
+    if (line)
+      tab[L.stab + ((int64_t)k * Y + j) * 8] = ev;
+    else
+      tab[L.eyt + (int64_t)k * L.eyt_ld + j] = ev;
   }
   __syncthreads();  // row tables and dtInv are visible to the whole CTA
 
@@ -122,7 +132,8 @@ __global__ void __launch_bounds__(256) lvc_setup_kernel(const CalibDev* __restri
   for (int k = tid; k < steps; k += nt) {
     const double dt = tab[L.dtinv + k];
     double rb_prev = 0.0, c_prev = 0.0;
-    double* yc = tab + L.yco + 4LL * k * Y;
+    double* yc = line ? tab + L.stab + 8LL * k * Y : tab + L.yco + 4LL * k * Y;
+    const int w = line ? 8 : 4, o = line ? 1 : 0;
     for (int j = 0; j < Y; j++) {
       const double* rc = tab + L.rowc + 4LL * j;
       const double a = -(0.5 * rc[0]);
@@ -130,12 +141,36 @@ __global__ void __launch_bounds__(256) lvc_setup_kernel(const CalibDev* __restri
       const double cc = -(0.5 * rc[2]);
       const double bp = (j == 0) ? b : b - a * c_prev * rb_prev;
       const double rb = 1.0 / bp;
-      yc[4 * j + 0] = (j == 0) ? 0.0 : -a * rb_prev;  // forward multiplier -a_j / b'_{j-1}
-      yc[4 * j + 1] = (j == Y - 1) ? 0.0 : -cc * rb;  // backward multiplier -c_j / b'_j
-      yc[4 * j + 2] = rb;
-      yc[4 * j + 3] = 0.0;
+      yc[w * j + o + 0] = (j == 0) ? 0.0 : -a * rb_prev;  // forward multiplier -a_j / b'_{j-1}
+      yc[w * j + o + 1] = (j == Y - 1) ? 0.0 : -cc * rb;  // backward multiplier -c_j / b'_j
+      yc[w * j + o + 2] = rb;
+      if (!line) yc[w * j + 3] = 0.0;
       rb_prev = rb;
       c_prev = cc;
+    }
+    if (line) {
+      // products of the multipliers inside each kLineK-row chunk of each
+      // CTA's row block: cp_j = prod_{chunk start..j} mY, cq_j = prod_{j..chunk end} nY
+      for (int r0 = 0; r0 < Y; r0 += c.Ycs) {
+        const int r1 = min(Y, r0 + c.Ycs);
+        for (int jb = r0; jb < r1; jb += kLineK) {
+          const int je = min(r1, jb + kLineK);
+          double pr = 1.0;
+          for (int j = jb; j < je; j++) {
+            pr = pr * yc[8 * j + 1];
+            yc[8 * j + 4] = pr;
+          }
+          pr = 1.0;
+          for (int j = je - 1; j >= jb; j--) {
+            pr = pr * yc[8 * j + 2];
+            yc[8 * j + 5] = pr;
+          }
+          for (int j = jb; j < je; j++) {
+            yc[8 * j + 6] = 0.0;
+            yc[8 * j + 7] = 0.0;
+          }
+        }
+      }
     }
   }
 }
@@ -159,14 +194,36 @@ __global__ void __launch_bounds__(128) lvc_pivot_kernel(const CalibDev* __restri
     }
     const CalibDev c = calibs[lo];
     const int X = c.numX, Y = c.numY, Xp = c.Xp;
-    const TabLayout L = tab_layout(X, Y, c.numT, Xp);
+    const TabLayout L = tab_layout(X, Y, c.numT, Xp, c.kind);
     const int64_t local = r - row_start[lo];
     const int k = (int)(local / Y), j = (int)(local % Y);
     const double* tab = tabs + c.tab;
-    const double e = tab[L.eyt + (int64_t)k * L.eyt_ld + j];
     const double dt = tab[L.dtinv + k];
-    PV* o = piv + c.piv + ((int64_t)k * Y + j) * Xp;
     double rb_prev = 0.0, c_prev = 0.0;
+    if (c.kind == kKindLine) {
+      // b'_i = (dt - e W1_i) - (e W0_i)(e W2_{i-1}) / b'_{i-1}, stored as rows of
+      // stride LD (the line kernel's shared-memory image)
+      const double e = tab[L.stab + ((int64_t)k * Y + j) * 8];
+      const int LDl = line_ld(X);
+      PV* o = piv + c.piv + ((int64_t)k * round4(Y) + j) * LDl;
+      if (LDl > X) o[X] = (PV)0;
+      const double* W0 = tab + L.wcol;
+      const double* W1 = W0 + L.xa;
+      const double* W2 = W1 + L.xa;
+      for (int i = 0; i < X; i++) {
+        const double a = -(e * W0[i]);
+        const double b = dt - e * W1[i];
+        const double cc = -(e * W2[i]);
+        const double bp = (i == 0) ? b : b - a * c_prev * rb_prev;
+        const double rb = 1.0 / bp;
+        o[i] = (PV)rb;
+        rb_prev = rb;
+        c_prev = cc;
+      }
+      continue;
+    }
+    const double e = tab[L.eyt + (int64_t)k * L.eyt_ld + j];
+    PV* o = piv + c.piv + ((int64_t)k * Y + j) * Xp;
     for (int i = 0; i < X; i++) {
       const double2 c01 = *reinterpret_cast<const double2*>(tab + L.colc + 4LL * i);
       const double2 c23 = *reinterpret_cast<const double2*>(tab + L.colc + 4LL * i + 2);
@@ -304,25 +361,30 @@ __global__ void __launch_bounds__(NT, (MinBlocks<NT, KX>::v)) lvc_rollback_kerne
     const int LD = Lf.LD;
     S* A;
     S* B;
+    S* s_aggF;
+    S* s_aggB;
     if constexpr (GSTATE) {
-      A = args.gstate + (int64_t)blockIdx.x * args.gstate_per_cta;
-      B = A + Lf.grid_elems / 2;
+      S* g = args.gstate + (int64_t)blockIdx.x * args.gstate_per_cta;
+      A = g + Lf.gA;
+      B = g + Lf.gB;
+      s_aggF = g + Lf.gaggF;
+      s_aggB = g + Lf.gaggB;
     } else {
       A = sm + Lf.A;
       B = sm + Lf.B;
+      s_aggF = sm + Lf.aggF;
+      s_aggB = sm + Lf.aggB;
     }
     S* s_colc = sm + Lf.colc;
     S* s_rowc = sm + Lf.rowc;
     S* s_tab[2] = {sm + Lf.tab0, sm + Lf.tab1};
-    S* s_aggF = sm + Lf.aggF;
-    S* s_aggB = sm + Lf.aggB;
     S* s_blkF = sm + Lf.blkF;
     S* s_blkB = sm + Lf.blkB;
     S* s_zin = sm + Lf.zin;
     S* s_xin = sm + Lf.xin;
     const StepTab st = step_tab(Ycs, Lf.P);
     const double* tabc = args.tabs + c.tab;
-    const TabLayout Lt = tab_layout(X, Y, T, Xp);
+    const TabLayout Lt = tab_layout(X, Y, T, Xp, kKindChunk);
     const double strike = 0.001 * (double)item.strike;  // strikes (:247)
     const int steps = T > 1 ? T - 1 : 0;
 

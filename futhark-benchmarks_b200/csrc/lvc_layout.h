@@ -21,11 +21,19 @@ namespace lvc {
 
 constexpr int kKY = 16;          // rows per Y-sweep unit (one warp, 32 columns)
 constexpr int kMaxCluster = 16;  // CTAs per instance (16 needs the non-portable opt-in)
+constexpr int kLineK = 16;       // line-kernel chunk: elements of a line per lane
+
+// Rollback kernel family of a calibration.
+enum : int32_t {
+  kKindChunk = 0,  // lanes own 8/16-element chunks of a row (any numX <= 512, HBM-state capable)
+  kKindLine = 1,   // lanes own whole lines of the grid (numX <= 256, on chip)
+};
 
 // One calibration, as the device sees it.  Filled by the host runtime.
 struct CalibDev {
-  int32_t numX, numY, numT, Xp;    // Xp: numX padded to a power of two >= 8
+  int32_t numX, numY, numT, Xp;      // Xp: numX padded to a power of two >= 8
   int32_t outer, xindex, yindex, C;  // C: CTAs (cluster size) per instance
+  int32_t kind, Ycs, pad0, pad1;     // kernel family; rows per CTA
   double s0, t, alpha, nu, beta;
   int64_t tab;  // offset (doubles) of the operator tables in the table arena
   int64_t piv;  // offset (elements) of the X-direction pivots in the pivot arena
@@ -35,36 +43,60 @@ struct CalibDev {
 LVC_HD int64_t al2(int64_t n) { return (n + 1) & ~int64_t(1); }
 
 // Operator-table layout, offsets in doubles from CalibDev::tab.  Every
-// sub-table starts on a 16-byte boundary.
+// sub-table starts on a 16-byte boundary.  Shared by both kernel families:
+// colc, rowc, x, dtinv.  Chunk family: eyt, yco.  Line family: wcol, stab.
 struct TabLayout {
   int64_t colc;   // [Xp][4]  eX_i = exp(2*beta*log x_i), 0.5*Dxx_i[0..2]   (zero for i >= numX)
   int64_t rowc;   // [Y][4]   0.5*nu^2*Dyy_j[0..2], 0
   int64_t x;      // [Xp]     the spot grid myX (zero padded)
   int64_t dtinv;  // [T-1]    1/(t_{k+1} - t_k)
-  int64_t eyt;    // [T-1][eyt_ld]  exp(2*(y_j - 0.5*nu^2*t_k))
-  int64_t yco;    // [T-1][Y][4]    Y-sweep multipliers: mY_j, nY_j, 1/b'_j, 0
+  int64_t eyt;    // [T-1][eyt_ld]  exp(2*(y_j - 0.5*nu^2*t_k))            (chunk family)
+  int64_t yco;    // [T-1][Y][4]    Y-sweep multipliers: mY_j, nY_j, 1/b'_j, 0  (chunk family)
+  int64_t wcol;   // [3][xa]  W_k(i) = 0.25 * eX_i * Dxx_i[k]                 (line family)
+  int64_t stab;   // [T-1][Y][8]    e_j, mY_j, nY_j, 1/b'_j, cp_j, cq_j, 0, 0 (line family)
   int64_t total;
-  int64_t eyt_ld;
+  int64_t eyt_ld, xa;
 };
 
-LVC_HD TabLayout tab_layout(int X, int Y, int T, int Xp) {
-  (void)X;
+LVC_HD TabLayout tab_layout(int X, int Y, int T, int Xp, int kind) {
   TabLayout L;
   const int64_t steps = T > 1 ? T - 1 : 0;
+  L.xa = al2(X);
+  L.eyt_ld = al2(Y);
   L.colc = 0;
   L.rowc = L.colc + 4LL * Xp;
   L.x = L.rowc + 4LL * Y;
   L.dtinv = L.x + Xp;
-  L.eyt_ld = al2(Y);
-  L.eyt = L.dtinv + al2(steps);
-  L.yco = L.eyt + steps * L.eyt_ld;
-  L.total = L.yco + steps * 4LL * Y;
+  int64_t o = L.dtinv + al2(steps);
+  if (kind == kKindChunk) {
+    L.eyt = o;
+    o += steps * L.eyt_ld;
+    L.yco = o;
+    o += steps * 4LL * Y;
+    L.wcol = L.stab = o;
+  } else {
+    L.wcol = o;
+    o += 3 * L.xa;
+    L.stab = o;
+    o += steps * 8LL * Y;
+    L.eyt = L.yco = o;
+  }
+  L.total = o;
   return L;
 }
 
-// Elements of the X-direction pivot array rbX[T-1][Y][Xp] of one calibration.
-LVC_HD int64_t piv_elems(int Y, int T, int Xp) {
-  return (T > 1 ? (int64_t)(T - 1) : 0) * Y * Xp;
+// Line family: the pivot rows are stored exactly as the kernel's shared-memory
+// image of them -- row j of step k at ((k*Y4 + j) * LD) with the odd row
+// stride LD = numX | 1 -- so one bulk copy moves a CTA's rows.
+LVC_HD int line_ld(int X) { return X | 1; }
+LVC_HD int64_t round4(int64_t n) { return (n + 3) & ~int64_t(3); }
+
+// Elements of the X-direction pivot array of one calibration (plus 4 of
+// padding so that bulk copies rounded up to 16 bytes stay in bounds):
+// chunk family rbX[T-1][Y][Xp]; line family rbL[T-1][Y4][LD].
+LVC_HD int64_t piv_elems(int X, int Y, int T, int Xp, int kind) {
+  const int64_t steps = T > 1 ? (int64_t)(T - 1) : 0;
+  return kind == kKindChunk ? steps * Y * Xp : steps * round4(Y) * line_ld(X) + 4;
 }
 
 // Row padding of the on-chip grid: PADS elements after every 8, so that the
@@ -86,7 +118,8 @@ LVC_HD int ceil_div(int a, int b) { return (a + b - 1) / b; }
 struct SmemLayout {
   int LD, Ycs, G, P, U;
   int A, B, colc, rowc, tab0, tab1, tabsz, aggF, aggB, blkF, blkB, zin, xin, misc, total;
-  int grid_elems;
+  int grid_elems;            // per-CTA HBM scratch when !onchip: A, B, aggF, aggB
+  int gA, gB, gaggF, gaggB;  // their offsets in that scratch
 };
 
 template <typename S> LVC_HD SmemLayout smem_layout(int Xp, int X, int Ycs, bool onchip) {
@@ -107,15 +140,19 @@ template <typename S> LVC_HD SmemLayout smem_layout(int Xp, int X, int Ycs, bool
   L.tabsz = up(6 * Ycs + 2 * L.P + 2);
   L.tab0 = o; o += L.tabsz;
   L.tab1 = o; o += L.tabsz;
-  L.aggF = o; o += up(L.U * 32);
-  L.aggB = o; o += up(L.U * 32);
+  L.aggF = o; if (onchip) o += up(L.U * 32);
+  L.aggB = o; if (onchip) o += up(L.U * 32);
   L.blkF = o; o += up(L.G * 32);
   L.blkB = o; o += up(L.G * 32);
   L.zin = o; o += up(L.G * 32);
   L.xin = o; o += up(L.G * 32);
   L.misc = o; o += up(8);
   L.total = o;
-  L.grid_elems = 2 * up(Ycs * L.LD);  // A + B, wherever they live
+  L.gA = 0;
+  L.gB = up(Ycs * L.LD);
+  L.gaggF = 2 * up(Ycs * L.LD);
+  L.gaggB = L.gaggF + up(L.U * 32);
+  L.grid_elems = onchip ? 2 * up(Ycs * L.LD) : L.gaggB + up(L.U * 32);
   return L;
 }
 

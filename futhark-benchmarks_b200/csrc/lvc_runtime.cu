@@ -26,6 +26,8 @@
 
 #include "LocVolCalib.h"
 #include "lvc_kernels.cuh"
+#include "lvc_line.cuh"
+#include "lvc_probe.cuh"
 
 using namespace lvc;
 
@@ -49,7 +51,7 @@ struct futhark_f64_1d {
 namespace {
 
 struct Launch {
-  int NT, KX, C;
+  int kind, NT, KX, C;
   bool gstate;
   int item_off, n_items, grid;
   size_t smem_bytes;
@@ -163,7 +165,14 @@ template <typename S, typename PV>
 using RbFn = void (*)(RollbackArgs<S, PV>);
 
 template <typename S, typename PV>
-RbFn<S, PV> rollback_fn(int NT, int KX, bool gs) {
+RbFn<S, PV> rollback_fn(int kind, int NT, int KX, bool gs) {
+  if (kind == kKindLine) {
+    if (NT == 64) return lvc_line_kernel<S, PV, 64>;
+    if (NT == 128) return lvc_line_kernel<S, PV, 128>;
+    if (NT == 256) return lvc_line_kernel<S, PV, 256>;
+    if (NT == 512) return lvc_line_kernel<S, PV, 512>;
+    return nullptr;
+  }
 #define LVC_CASE(nt, kx, g) \
   if (NT == nt && KX == kx && gs == g) return lvc_rollback_kernel<S, PV, nt, kx, g>;
   LVC_CASE(128, 8, false)
@@ -185,16 +194,46 @@ int state_size() { return (int)sizeof(S); }
 
 // Kernel configuration of one calibration.
 struct Config {
-  int NT, KX, C;
+  int kind, NT, KX, C;
   bool gstate;
   int Ycs;
   size_t smem_bytes;
   int64_t grid_elems;
 };
 
+// Line family: one lane per grid line; needs numX <= 256 and at most 16
+// warps of units per CTA, which fixes the cluster size.
+template <typename S>
+bool choose_line(int X, int Y, int max_smem, Config& cf) {
+  if (X > 256) return false;
+  for (int C = 1; C <= kMaxCluster; C *= 2) {
+    // rows per CTA: a multiple of 4 when split, so every CTA's bulk copies
+    // start on a 16-byte boundary
+    const int Ycs = C == 1 ? Y : (int)round4(ceil_div(Y, C));
+    if (C > 1 && (C - 1) * Ycs >= Y) break;
+    const LineLayout L16 = line_layout<S>(X, Ycs, 16);
+    if (L16.Ux > 16 || L16.Uy > 16) continue;
+    const int NT = std::max(64, 32 * pow2ceil(std::max(L16.Ux, L16.Uy)));
+    const LineLayout L = line_layout<S>(X, Ycs, NT / 32);
+    if (L.total > max_smem) continue;
+    cf.kind = kKindLine;
+    cf.NT = NT;
+    cf.KX = kLineK;
+    cf.C = C;
+    cf.gstate = false;
+    cf.Ycs = Ycs;
+    cf.smem_bytes = (size_t)L.total;
+    cf.grid_elems = 0;
+    return true;
+  }
+  return false;
+}
+
 template <typename S>
 Config choose_config(int X, int Y, int max_smem) {
   Config cf;
+  if (choose_line<S>(X, Y, max_smem, cf)) return cf;
+  cf.kind = kKindChunk;
   const int Xp = std::max(8, pow2ceil(X));
   cf.KX = Xp <= 256 ? 8 : 16;
   cf.gstate = true;
@@ -222,10 +261,12 @@ Config choose_config(int X, int Y, int max_smem) {
 
 template <typename S, typename PV>
 int prepare_launch(futhark_context* ctx, Launch& L) {
-  RbFn<S, PV> fn = rollback_fn<S, PV>(L.NT, L.KX, L.gstate);
+  RbFn<S, PV> fn = rollback_fn<S, PV>(L.kind, L.NT, L.KX, L.gstate);
   if (!fn) return set_error(ctx, FUTHARK_PROGRAM_ERROR, "no rollback kernel for this configuration");
+  // Several launch classes may share one kernel instantiation with different
+  // shared-memory sizes: allow the device maximum once for all of them.
   LVC_CUDA(ctx, cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)L.smem_bytes));
+                                     ctx->max_smem));
   if (L.C > 8)
     LVC_CUDA(ctx, cudaFuncSetAttribute((const void*)fn,
                                        cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
@@ -284,7 +325,7 @@ cudaError_t launch_rollback(lvc_plan* P, const Launch& L, cudaStream_t s) {
     cfg.attrs = &attr;
     cfg.numAttrs = 1;
   }
-  return cudaLaunchKernelEx(&cfg, rollback_fn<S, PV>(L.NT, L.KX, L.gstate), a);
+  return cudaLaunchKernelEx(&cfg, rollback_fn<S, PV>(L.kind, L.NT, L.KX, L.gstate), a);
 }
 
 // Enqueue one run of a plan.  `ev` (optional) receives a start/stop event
@@ -351,8 +392,8 @@ int plan_build(futhark_context* ctx, const lvc_calibration* cs, int n, lvc_plan*
   P->params.assign(cs, cs + n);
   P->calibs.resize(n);
   P->row_start.assign(n + 1, 0);
-  std::map<std::tuple<int, int, int, bool>, std::vector<std::pair<int64_t, Item>>> classes;
-  std::map<std::tuple<int, int, int, bool>, Config> class_cfg;
+  std::map<std::tuple<int, int, int, int, bool>, std::vector<std::pair<int64_t, Item>>> classes;
+  std::map<std::tuple<int, int, int, int, bool>, Config> class_cfg;
   int64_t tab_off = 0, piv_off = 0, out_off = 0;
   for (int i = 0; i < n; i++) {
     const lvc_calibration& c = cs[i];
@@ -365,15 +406,18 @@ int plan_build(futhark_context* ctx, const lvc_calibration* cs, int n, lvc_plan*
     d.Xp = std::max(8, pow2ceil(c.numX));
     d.outer = c.outer;
     d.C = cf.C;
+    d.kind = cf.kind;
+    d.Ycs = cf.Ycs;
+    d.pad0 = d.pad1 = 0;
     fill_scalars(d, c);
     d.tab = tab_off;
-    tab_off += al2(tab_layout(c.numX, c.numY, c.numT, d.Xp).total);
+    tab_off += al2(tab_layout(c.numX, c.numY, c.numT, d.Xp, d.kind).total);
     d.piv = piv_off;
-    piv_off += piv_elems(c.numY, c.numT, d.Xp);
+    piv_off += (piv_elems(c.numX, c.numY, c.numT, d.Xp, d.kind) + 3) & ~int64_t(3);
     d.out = out_off;
     out_off += c.outer;
     P->row_start[i + 1] = P->row_start[i] + (int64_t)(c.numT > 1 ? c.numT - 1 : 0) * c.numY;
-    const auto key = std::make_tuple(cf.NT, cf.KX, cf.C, cf.gstate);
+    const auto key = std::make_tuple(cf.kind, cf.NT, cf.KX, cf.C, cf.gstate);
     auto& cls = classes[key];
     auto it = class_cfg.find(key);
     if (it == class_cfg.end()) {
@@ -398,6 +442,7 @@ int plan_build(futhark_context* ctx, const lvc_calibration* cs, int n, lvc_plan*
                      });
     const Config& cf = class_cfg[kv.first];
     Launch L;
+    L.kind = cf.kind;
     L.NT = cf.NT;
     L.KX = cf.KX;
     L.C = cf.C;
@@ -869,5 +914,44 @@ int lvc_batch(struct futhark_context* ctx, const struct lvc_calibration* calibs,
 }
 
 void* lvc_context_stream(struct futhark_context* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+int lvc_probe_peaks(struct futhark_context* ctx, double* fp64_tflops, double* smem_gbs) {
+  std::lock_guard<std::mutex> g(ctx->mu);
+  if (!ctx->ok) return set_error(ctx, FUTHARK_PROGRAM_ERROR, "context has no usable CUDA device");
+  LVC_CUDA(ctx, cudaSetDevice(ctx->device));
+  void* scratch = nullptr;
+  LVC_CUDA(ctx, cudaMalloc(&scratch, 1 << 20));
+  cudaEvent_t a, b;
+  LVC_CUDA(ctx, cudaEventCreate(&a));
+  LVC_CUDA(ctx, cudaEventCreate(&b));
+  const int dgrid = ctx->num_sms * 8, diters = 20000;
+  const int sgrid = ctx->num_sms * 4, siters = 20000;
+  float best_d = 1e30f, best_s = 1e30f;
+  for (int rep = 0; rep < 4; rep++) {
+    float ms = 0.f;
+    LVC_CUDA(ctx, cudaEventRecord(a, ctx->stream));
+    lvc_probe_dfma_kernel<<<dgrid, 256, 0, ctx->stream>>>((double*)scratch, diters, 0.9999999, 1e-7);
+    LVC_CUDA(ctx, cudaGetLastError());
+    LVC_CUDA(ctx, cudaEventRecord(b, ctx->stream));
+    LVC_CUDA(ctx, cudaEventSynchronize(b));
+    LVC_CUDA(ctx, cudaEventElapsedTime(&ms, a, b));
+    if (rep > 0) best_d = std::min(best_d, ms);
+    LVC_CUDA(ctx, cudaEventRecord(a, ctx->stream));
+    lvc_probe_smem_kernel<<<sgrid, 512, 0, ctx->stream>>>((unsigned long long*)scratch, siters);
+    LVC_CUDA(ctx, cudaGetLastError());
+    LVC_CUDA(ctx, cudaEventRecord(b, ctx->stream));
+    LVC_CUDA(ctx, cudaEventSynchronize(b));
+    LVC_CUDA(ctx, cudaEventElapsedTime(&ms, a, b));
+    if (rep > 0) best_s = std::min(best_s, ms);
+  }
+  const double flops = 2.0 * kProbeChains * (double)diters * 256.0 * dgrid;
+  const double bytes = 16.0 * 4.0 * (double)siters * 512.0 * sgrid;
+  *fp64_tflops = flops / (best_d * 1e-3) / 1e12;
+  *smem_gbs = bytes / (best_s * 1e-3) / 1e9;
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaFree(scratch);
+  return 0;
+}
 
 }  // extern "C"

@@ -153,6 +153,12 @@ LVC_API int32_t lvc_plan_num_launches(const struct lvc_plan *plan);
 LVC_API int lvc_batch(struct futhark_context *ctx, const struct lvc_calibration *calibs, int32_t n,
               int32_t precision, double *prices);
 
+/* Peak probes of the context's device: FP64 FMA throughput (TFLOP/s, 2 flops
+ * per FMA, every SM busy) and shared-memory load bandwidth (GB/s summed over
+ * SMs), each the best of three timed microbenchmark launches.  These are the
+ * two ceilings of the rollback kernel. */
+LVC_API int lvc_probe_peaks(struct futhark_context *ctx, double *fp64_tflops, double *smem_gbs);
+
 /* The cudaStream_t the context launches on (as void*). */
 LVC_API void *lvc_context_stream(struct futhark_context *ctx);
 
