@@ -955,3 +955,176 @@ int lvc_probe_peaks(struct futhark_context* ctx, double* fp64_tflops, double* sm
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Entry point without device allocation.
+//
+// Some callers cannot call cudaMalloc at the moment they need a price: a
+// serving loop that must never trigger the implicit device synchronisation of
+// cudaMalloc/cudaFree, code running under a caching allocator or a memory
+// budget that owns every byte of the device, or a host that has already handed
+// the rest of HBM to other work.  For them lvc_entry_main_f64_noalloc runs
+// the same setup, pivot and rollback kernels as futhark_entry_main_f64, with
+// every scratch buffer (calibration record, work list, operator tables, pivot
+// rows, error flag) carved from one fixed static device array instead of
+// device allocations.  The array exists once per device that loads this
+// library and is held until the process exits.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = (size_t)LVC_NOALLOC_SCRATCH_BYTES;
+static __device__ __align__(256) unsigned char lvc_noalloc_scratch[kNoAllocScratchBytes];
+
+// Device address of lvc_noalloc_scratch, looked up once per device.  In host
+// code the symbol is only a host-side stand-in; kernels must be given this
+// address.
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[kMaxDevices] = {};
+
+int noalloc_scratch(futhark_context* ctx, unsigned char** out) {
+  if (ctx->device < 0 || ctx->device >= kMaxDevices)
+    return set_error(ctx, FUTHARK_PROGRAM_ERROR, "device ordinal out of range for the static scratch");
+  std::lock_guard<std::mutex> g(g_noalloc_mu);
+  if (!g_noalloc_addr[ctx->device]) {
+    void* p = nullptr;  // the current device is ctx->device (set by the caller)
+    cudaError_t e = cudaGetSymbolAddress(&p, lvc_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaGetSymbolAddress(lvc_noalloc_scratch)");
+    if (!p) return set_error(ctx, FUTHARK_PROGRAM_ERROR, "static scratch has no device address");
+    g_noalloc_addr[ctx->device] = p;
+  }
+  *out = static_cast<unsigned char*>(g_noalloc_addr[ctx->device]);
+  return 0;
+}
+
+__global__ void lvc_noalloc_items_kernel(Item* items, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    items[i] = Item{0, i};
+}
+
+size_t up256(size_t n) { return (n + 255) & ~size_t(255); }
+
+}  // namespace
+
+extern "C" int lvc_entry_main_f64_noalloc(struct futhark_context* ctx, double* prices,
+                                          const int32_t outer, const int32_t numX,
+                                          const int32_t numY, const int32_t numT, const double s0,
+                                          const double t, const double alpha, const double nu,
+                                          const double beta) {
+  std::lock_guard<std::mutex> g(ctx->mu);
+  if (!ctx->ok) return set_error(ctx, FUTHARK_PROGRAM_ERROR, "context has no usable CUDA device");
+  LVC_CUDA(ctx, cudaSetDevice(ctx->device));
+  const lvc_calibration c{outer, numX, numY, numT, s0, t, alpha, nu, beta};
+  if (int rc = validate(ctx, c, 0)) return rc;
+  if (outer > 0 && !prices) return set_error(ctx, FUTHARK_PROGRAM_ERROR, "null price buffer");
+  unsigned char* base = nullptr;
+  if (int rc = noalloc_scratch(ctx, &base)) return rc;
+
+  const Config cf = choose_config<double>(numX, numY, ctx->max_smem);
+  if (cf.gstate)
+    return set_error(ctx, FUTHARK_PROGRAM_ERROR,
+                     "lvc_entry_main_f64_noalloc: this grid does not fit on chip; its HBM state "
+                     "needs the allocating entry point futhark_entry_main_f64");
+  CalibDev d;
+  memset(&d, 0, sizeof d);
+  d.numX = numX;
+  d.numY = numY;
+  d.numT = numT;
+  d.Xp = std::max(8, pow2ceil(numX));
+  d.outer = outer;
+  d.C = cf.C;
+  d.kind = cf.kind;
+  d.Ycs = cf.Ycs;
+  fill_scalars(d, c);
+  d.tab = 0;
+  d.piv = 0;
+  d.out = 0;
+  const int64_t tab_elems = al2(tab_layout(numX, numY, numT, d.Xp, d.kind).total);
+  const int64_t piv_n = (piv_elems(numX, numY, numT, d.Xp, d.kind) + 3) & ~int64_t(3);
+  // scratch carve-up
+  const size_t o_calib = 0;
+  const size_t o_err = up256(o_calib + sizeof(CalibDev));
+  const size_t o_rows = up256(o_err + sizeof(int));
+  const size_t o_items = up256(o_rows + 2 * sizeof(int64_t));
+  const size_t o_tabs = up256(o_items + sizeof(Item) * (size_t)std::max(1, outer));
+  const size_t o_piv = up256(o_tabs + sizeof(double) * (size_t)tab_elems);
+  const size_t need = o_piv + sizeof(double) * (size_t)piv_n;
+  if (need > kNoAllocScratchBytes) {
+    char buf[256];
+    snprintf(buf, sizeof buf,
+             "lvc_entry_main_f64_noalloc: this calibration needs %zu bytes of scratch, more than "
+             "the static %zu bytes; use futhark_entry_main_f64",
+             need, kNoAllocScratchBytes);
+    return set_error(ctx, FUTHARK_PROGRAM_ERROR, buf);
+  }
+  CalibDev* d_calib = reinterpret_cast<CalibDev*>(base + o_calib);
+  int* d_err = reinterpret_cast<int*>(base + o_err);
+  int64_t* d_rows = reinterpret_cast<int64_t*>(base + o_rows);
+  Item* d_items = reinterpret_cast<Item*>(base + o_items);
+  double* d_tabs = reinterpret_cast<double*>(base + o_tabs);
+  double* d_piv = reinterpret_cast<double*>(base + o_piv);
+  const int64_t rows[2] = {0, (int64_t)(numT > 1 ? numT - 1 : 0) * numY};
+  cudaStream_t s = ctx->stream;
+
+  // the array keeps the previous call's contents: reset what must start at zero
+  LVC_CUDA(ctx, cudaMemsetAsync(d_err, 0, sizeof(int), s));
+  LVC_CUDA(ctx, cudaMemcpyAsync(d_calib, &d, sizeof d, cudaMemcpyHostToDevice, s));
+  LVC_CUDA(ctx, cudaMemcpyAsync(d_rows, rows, sizeof rows, cudaMemcpyHostToDevice, s));
+  if (outer > 0) {
+    lvc_noalloc_items_kernel<<<(outer + 255) / 256, 256, 0, s>>>(d_items, outer);
+    LVC_CUDA(ctx, cudaGetLastError());
+  }
+  lvc_setup_kernel<<<1, 256, 0, s>>>(d_calib, d_tabs);
+  LVC_CUDA(ctx, cudaGetLastError());
+  if (rows[1] > 0) {
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((rows[1] + 127) / 128, 64LL * ctx->num_sms));
+    lvc_pivot_kernel<double><<<grid, 128, 0, s>>>(d_calib, d_rows, 1, d_tabs, d_piv);
+    LVC_CUDA(ctx, cudaGetLastError());
+  }
+  if (outer > 0) {
+    Launch L;
+    L.kind = cf.kind;
+    L.NT = cf.NT;
+    L.KX = cf.KX;
+    L.C = cf.C;
+    L.gstate = false;
+    L.item_off = 0;
+    L.n_items = outer;
+    L.smem_bytes = cf.smem_bytes;
+    L.gstate_per_cta = 0;
+    L.gstate_off = 0;
+    if (int rc = prepare_launch<double, double>(ctx, L)) return rc;
+    RollbackArgs<double, double> a;
+    a.calibs = d_calib;
+    a.items = d_items;
+    a.n_items = outer;
+    a.C = L.C;
+    a.smem_elems = (int)(L.smem_bytes / sizeof(double));
+    a.tabs = d_tabs;
+    a.piv = d_piv;
+    a.out = prices;
+    a.gstate = nullptr;
+    a.gstate_per_cta = 0;
+    a.err = d_err;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(L.grid);
+    cfg.blockDim = dim3(L.NT);
+    cfg.dynamicSmemBytes = L.smem_bytes;
+    cfg.stream = s;
+    cudaLaunchAttribute attr;
+    if (L.C > 1) {
+      attr.id = cudaLaunchAttributeClusterDimension;
+      attr.val.clusterDim.x = L.C;
+      attr.val.clusterDim.y = 1;
+      attr.val.clusterDim.z = 1;
+      cfg.attrs = &attr;
+      cfg.numAttrs = 1;
+    }
+    LVC_CUDA(ctx, cudaLaunchKernelEx(&cfg, rollback_fn<double, double>(L.kind, L.NT, L.KX, false), a));
+  }
+  int h = 0;
+  LVC_CUDA(ctx, cudaMemcpyAsync(&h, d_err, sizeof(int), cudaMemcpyDeviceToHost, s));
+  LVC_CUDA(ctx, cudaStreamSynchronize(s));
+  if (h) return set_error(ctx, FUTHARK_PROGRAM_ERROR, "rollback kernel rejected a work item");
+  return 0;
+}

@@ -153,6 +153,32 @@ LVC_API int32_t lvc_plan_num_launches(const struct lvc_plan *plan);
 LVC_API int lvc_batch(struct futhark_context *ctx, const struct lvc_calibration *calibs, int32_t n,
               int32_t precision, double *prices);
 
+/*
+ * No counterpart in the reference.  `main` at f64 for callers that cannot
+ * allocate device memory when they price (a serving loop that must not incur
+ * the device-wide synchronisation of cudaMalloc/cudaFree, a host whose
+ * allocator or memory budget already owns all of HBM).  Same inputs, checks
+ * and errors as futhark_entry_main_f64, but the prices go to `prices`, a
+ * device buffer of outer_loop_count doubles owned by the caller, and all
+ * scratch comes from one static device array of LVC_NOALLOC_SCRATCH_BYTES
+ * (64 MiB) that every device loading this library holds until exit; the call
+ * allocates no device memory.  Calibrations whose scratch exceeds that size
+ * (8 * (numX|1) * numY * (numT-1) bytes of pivots plus 64 * numY * (numT-1)
+ * bytes of tables; all three reference datasets fit) or whose grid does not
+ * fit on chip are rejected with an error.
+ * The first call on each device looks up the array's device address
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * Runs on the context's stream and returns after the prices are written.
+ * Every call uses the same array, so calls that overlap on the GPU (other
+ * contexts or threads using this entry point at the same time) race.
+ */
+#define LVC_NOALLOC_SCRATCH_BYTES (64u << 20)
+LVC_API int lvc_entry_main_f64_noalloc(struct futhark_context *ctx, double *prices,
+                                       const int32_t outer_loop_count, const int32_t numX,
+                                       const int32_t numY, const int32_t numT, const double s0,
+                                       const double t, const double alpha, const double nu,
+                                       const double beta);
+
 /* Peak probes of the context's device: FP64 FMA throughput (TFLOP/s, 2 flops
  * per FMA, every SM busy) and shared-memory load bandwidth (GB/s summed over
  * SMs), each the best of three timed microbenchmark launches.  These are the
