@@ -439,3 +439,456 @@ __global__ void __launch_bounds__(NT, (NT >= 512 ? 1 : 512 / NT)) lvc_line_kerne
 }
 
 }  // namespace lvc
+
+namespace lvc {
+
+// ---------------------------------------------------------------------------
+// Full-tile line kernel: the same algorithm for grids whose line chunks, row
+// groups and CTA row blocks are all full (numX % 32 == 0, rows per CTA a
+// multiple of 32, numY divisible by the cluster size) -- every shape of the
+// reference datasets and of the uneven calibration mix.  Each warp owns UPW
+// units in each sweep (two independent recurrence chains per lane), which
+// doubles the instruction-level parallelism and lets the register budget
+// (up to 255 per thread with 8 warps) hold the chunk state without spilling.
+// Without partial tiles there is no per-element predication; the grid buffer
+// carries one halo row above and below (zero at the global boundary, written
+// by the neighbouring CTA of the cluster during its Y sweep otherwise).
+// ---------------------------------------------------------------------------
+struct FullLayout {
+  int LD, Ycs, CHx, Ux, CGy, CHy, Uy;
+  int bar, A, B, wcol, grow, tab0, tab1, xfa, xfb, xba, xbb, yf, yb, blkF, blkB, zin, xin, tot, total;
+};
+
+template <typename S>
+LVC_HD FullLayout full_layout(int X, int Ycs, int NU) {
+  FullLayout L;
+  auto up = [](int n) { return (n + 15) / 16 * 16; };
+  const int s = (int)sizeof(S);
+  L.LD = line_ld(X);
+  L.Ycs = Ycs;
+  L.CHx = X / kLineK;
+  L.Ux = (Ycs / 32) * L.CHx;
+  L.CGy = (X + 31) / 32;
+  L.CHy = Ycs / kLineK;
+  L.Uy = L.CGy * L.CHy;
+  int o = 0;
+  L.bar = o; o += 16;
+  L.A = o; o += up((Ycs + 2) * L.LD * s);   // rows -1 .. Ycs (halo rows at both ends)
+  L.B = o; o += up(Ycs * L.LD * s + 16);
+  L.wcol = o; o += up(4 * X * s);           // [X][4]: W0, W1, W2, 0
+  L.grow = o; o += up(4 * Ycs * s);
+  L.tab0 = o; o += up(8 * Ycs * 8);
+  L.tab1 = o; o += up(8 * Ycs * 8);
+  L.xfa = o; o += up(NU * 32 * s);
+  L.xfb = o; o += up(NU * 32 * s);
+  L.xba = o; o += up(NU * 32 * s);
+  L.xbb = o; o += up(NU * 32 * s);
+  L.yf = o; o += up(NU * 32 * s);
+  L.yb = o; o += up(NU * 32 * s);
+  L.blkF = o; o += up(L.CGy * 32 * s);
+  L.blkB = o; o += up(L.CGy * 32 * s);
+  L.zin = o; o += up(L.CGy * 32 * s);
+  L.xin = o; o += up(L.CGy * 32 * s);
+  L.tot = o; o += up(4 * s);
+  L.total = o;
+  return L;
+}
+
+template <typename S> struct V2;
+template <> struct V2<double> {
+  static __device__ __forceinline__ double2 ld(const double* p) { return *reinterpret_cast<const double2*>(p); }
+};
+template <> struct V2<float> {
+  static __device__ __forceinline__ float2 ld(const float* p) { return *reinterpret_cast<const float2*>(p); }
+};
+
+template <int NT> struct FullMinBlocks {
+  static constexpr int v = NT >= 256 ? 1 : 256 / NT;
+};
+
+template <typename S, typename PV, int NT, int UPW>
+__global__ void __launch_bounds__(NT, (FullMinBlocks<NT>::v)) lvc_line_full_kernel(RollbackArgs<S, PV> args) {
+  constexpr int K = kLineK;
+  constexpr int NW = NT / 32;
+  constexpr int NU = NW * UPW;  // units per sweep
+  static_assert(sizeof(S) == sizeof(PV), "pivots are copied verbatim into the state buffer");
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int C = args.C;
+  const bool clustered = C > 1;
+  int rank = 0;
+  if (clustered) rank = (int)cg::this_cluster().block_rank();
+  const int cid = blockIdx.x / C, ncl = gridDim.x / C;
+  unsigned sc = 0, phase = 0;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem);
+  if (tid == 0) {
+    mbar_init(bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+
+  for (int it = cid; it < args.n_items; it += ncl) {
+    const Item item = args.items[it];
+    const CalibDev c = args.calibs[item.calib];
+    const int X = c.numX, Y = c.numY, T = c.numT;
+    const int Ycs = c.Ycs;
+    const int r0 = rank * Ycs;
+    const FullLayout Ls = full_layout<S>(X, Ycs, NU);
+    if (c.kind != kKindLine || c.C != C || Ls.total > args.smem_elems * (int)sizeof(S) || Ls.Ux != NU ||
+        Ls.Uy != NU || (X % 32) || (Ycs % 32) || Ycs * C != Y) {
+      if (tid == 0) atomicExch(args.err, 4);
+      continue;
+    }
+    const int LD = Ls.LD;
+    S* A = reinterpret_cast<S*>(smem + Ls.A);  // row r of the block at A + (r + 1) * LD
+    S* B = reinterpret_cast<S*>(smem + Ls.B);
+    const S* sW = reinterpret_cast<const S*>(smem + Ls.wcol);
+    const S* sG = reinterpret_cast<const S*>(smem + Ls.grow);
+    double* sT[2] = {reinterpret_cast<double*>(smem + Ls.tab0), reinterpret_cast<double*>(smem + Ls.tab1)};
+    S* xfa = reinterpret_cast<S*>(smem + Ls.xfa);
+    S* xfb = reinterpret_cast<S*>(smem + Ls.xfb);
+    S* xba = reinterpret_cast<S*>(smem + Ls.xba);
+    S* xbb = reinterpret_cast<S*>(smem + Ls.xbb);
+    S* yf = reinterpret_cast<S*>(smem + Ls.yf);
+    S* yb = reinterpret_cast<S*>(smem + Ls.yb);
+    S* blkF = reinterpret_cast<S*>(smem + Ls.blkF);
+    S* blkB = reinterpret_cast<S*>(smem + Ls.blkB);
+    S* s_zin = reinterpret_cast<S*>(smem + Ls.zin);
+    S* s_xin = reinterpret_cast<S*>(smem + Ls.xin);
+    S* s_tot = reinterpret_cast<S*>(smem + Ls.tot);
+    const double* tabc = args.tabs + c.tab;
+    const TabLayout Lt = tab_layout(X, Y, T, c.Xp, kKindLine);
+    const double strike = 0.001 * (double)item.strike;  // strikes (:247)
+    const int steps = T > 1 ? T - 1 : 0;
+    const PV* piv = args.piv + c.piv;
+    const int64_t Y4 = round4(Y);
+    S* halo_prev = nullptr;  // bottom halo row of rank - 1
+    S* halo_next = nullptr;  // top halo row of rank + 1
+    if (clustered) {
+      cg::cluster_group cl = cg::this_cluster();
+      if (rank > 0) halo_prev = cl.map_shared_rank(A + (Ycs + 1) * LD, rank - 1);
+      if (rank < C - 1) halo_next = cl.map_shared_rank(A, rank + 1);
+    }
+
+    // The previous instance is done with every buffer, and -- across the
+    // cluster -- every neighbour has finished pushing its last halo rows into
+    // this CTA before they are re-initialised below.
+    if (clustered) cg::this_cluster().sync(); else __syncthreads();
+    // setPayoff (:46-47) on the block and on the halo rows (the payoff does not
+    // depend on the row; halos at the global boundary are zero)
+    for (int e = tid; e < (Ycs + 2) * LD; e += NT) {
+      const int r = e / LD, i = e - r * LD;
+      const bool boundary = (r == 0 && rank == 0) || (r == Ycs + 1 && rank == C - 1);
+      A[e] = (i < X && !boundary) ? (S)fmax(tabc[Lt.x + i] - strike, 0.0) : (S)0;
+    }
+    for (int e = tid; e < 4 * X; e += NT) {
+      const int i = e >> 2, k = e & 3;
+      const_cast<S*>(sW)[e] = k < 3 ? (S)tabc[Lt.wcol + k * (int64_t)((X + 1) & ~1) + i] : (S)0;
+    }
+    for (int e = tid; e < 4 * Ycs; e += NT) const_cast<S*>(sG)[e] = (S)tabc[Lt.rowc + 4LL * r0 + e];
+
+    if (steps == 0) {
+      if (tid == 0 && c.yindex >= r0 && c.yindex < r0 + Ycs)
+        args.out[c.out + item.strike] = fmax(tabc[Lt.x + c.xindex] - strike, 0.0);
+      continue;
+    }
+    const unsigned piv_bytes = (unsigned)((Ycs * LD * (int)sizeof(S) + 15) & ~15);
+    const unsigned tab_bytes = (unsigned)(Ycs * 64);
+    auto issue_copies = [&](int k, double* tdst) {
+      if (tid == 0) {
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        mbar_expect_tx(bar, piv_bytes + tab_bytes);
+        bulk_g2s(B, piv + ((int64_t)k * Y4 + r0) * LD, piv_bytes, bar);
+        bulk_g2s(tdst, tabc + Lt.stab + ((int64_t)k * Y + r0) * 8, tab_bytes, bar);
+      }
+    };
+    issue_copies(steps - 1, sT[sc & 1]);
+
+    // unit geometry (u = warp + slot * NW)
+    int rgx[UPW], chx[UPW], jl[UPW], cgy[UPW], chy[UPW], colv[UPW];
+#pragma unroll
+    for (int q = 0; q < UPW; q++) {
+      const int u = warp + q * NW;
+      rgx[q] = u / Ls.CHx;
+      chx[q] = u - rgx[q] * Ls.CHx;
+      jl[q] = rgx[q] * 32 + lane;
+      cgy[q] = u / Ls.CHy;
+      chy[q] = u - cgy[q] * Ls.CHy;
+      colv[q] = cgy[q] * 32 + lane;
+    }
+    // output lane: the unit and element holding myResult[myYindex, myXindex]
+    int out_q = -1, out_m = 0;
+#pragma unroll
+    for (int q = 0; q < UPW; q++) {
+      const int jy = c.yindex - r0 - chy[q] * K;
+      if (colv[q] == c.xindex && jy >= 0 && jy < K) {
+        out_q = q;
+        out_m = jy;
+      }
+    }
+
+    for (int s = 0; s < steps; s++, sc++) {
+      const int k = steps - 1 - s;
+      if (!mbar_wait(bar, phase)) atomicExch(args.err, 3);
+      phase ^= 1u;
+      if (clustered) cg::this_cluster().sync(); else __syncthreads();
+      const double* tb = sT[sc & 1];
+      const S dt = (S)tabc[Lt.dtinv + k];
+
+      // -------- X sweep pass 1: explicitX + explicitY, forward recurrence (chunk-local) --------
+      S z[UPW][K], PQ[UPW][K];
+      {
+        S e[UPW], g0[UPW], g1[UPW], g2[UPW], Rl[UPW], Rc[UPW], rbp[UPW], zl[UPW], Pl[UPW];
+#pragma unroll
+        for (int q = 0; q < UPW; q++) {
+          const int ib = chx[q] * K;
+          const S* Arow = A + (jl[q] + 1) * LD;
+          e[q] = (S)tb[jl[q] * 8];
+          g0[q] = sG[4 * jl[q]];
+          g1[q] = sG[4 * jl[q] + 1];
+          g2[q] = sG[4 * jl[q] + 2];
+          Rl[q] = ib > 0 ? Arow[ib - 1] : (S)0;
+          Rc[q] = Arow[ib];
+          rbp[q] = ib > 0 ? B[jl[q] * LD + ib - 1] : (S)0;
+          zl[q] = 0;
+          Pl[q] = 1;
+        }
+#pragma unroll
+        for (int m = 0; m < K; m++) {
+#pragma unroll
+          for (int q = 0; q < UPW; q++) {
+            const int i = chx[q] * K + m;
+            const S* Arow = A + (jl[q] + 1) * LD;
+            const S Rn = Arow[i + 1];  // column numX is zero padding
+            const S up = Arow[i - LD];  // rows j-1 and j+1 (halo rows at the block edges)
+            const S dn = Arow[i + LD];
+            const auto w01 = V2<S>::ld(sW + 4 * i);
+            const S w2 = sW[4 * i + 2];
+            const S v = g0[q] * up + g1[q] * Rc[q] + g2[q] * dn;            // explicitY (:199)
+            const S sx = w01.x * Rl[q] + w01.y * Rc[q] + w2 * Rn;           // explicitX / (0.5 e)
+            const S u = e[q] * sx + (dt * Rc[q] + v);                       // :195-200
+            const S mult = (e[q] * w01.x) * rbp[q];                         // -a_i / b'_{i-1}
+            zl[q] = u + mult * zl[q];
+            Pl[q] = mult * Pl[q];
+            z[q][m] = zl[q];
+            PQ[q][m] = Pl[q];
+            rbp[q] = B[jl[q] * LD + i];
+            Rl[q] = Rc[q];
+            Rc[q] = Rn;
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < UPW; q++) {
+          const int u = warp + q * NW;
+          xfa[u * 32 + lane] = zl[q];
+          xfb[u * 32 + lane] = Pl[q];
+        }
+      }
+      __syncthreads();
+      // -------- pass 2: forward fix-up, backward recurrence (chunk-local) --------
+      {
+        S zin[UPW], xl[UPW], Ql[UPW], e[UPW];
+#pragma unroll
+        for (int q = 0; q < UPW; q++) {
+          zin[q] = 0;
+#pragma unroll 4
+          for (int c2 = 0; c2 < chx[q]; c2++) {
+            const int u = rgx[q] * Ls.CHx + c2;
+            zin[q] = xfa[u * 32 + lane] + xfb[u * 32 + lane] * zin[q];
+          }
+          xl[q] = 0;
+          Ql[q] = 1;
+          e[q] = (S)tb[jl[q] * 8];
+        }
+#pragma unroll
+        for (int m = K - 1; m >= 0; m--) {
+#pragma unroll
+          for (int q = 0; q < UPW; q++) {
+            const int i = chx[q] * K + m;
+            const S zz = z[q][m] + PQ[q][m] * zin[q];
+            const S rbm = B[jl[q] * LD + i];
+            const S aR = e[q] * sW[4 * i + 2];
+            xl[q] = rbm * (zz + aR * xl[q]);  // x_i = (z_i - c_i x_{i+1}) / b'_i
+            Ql[q] = (aR * rbm) * Ql[q];
+            z[q][m] = xl[q];
+            PQ[q][m] = Ql[q];
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < UPW; q++) {
+          const int u = warp + q * NW;
+          xba[u * 32 + lane] = xl[q];
+          xbb[u * 32 + lane] = Ql[q];
+        }
+      }
+      __syncthreads();
+      // -------- pass 3: backward fix-up; dtInv * u goes to B (:205) --------
+      {
+        S xin[UPW];
+#pragma unroll
+        for (int q = 0; q < UPW; q++) {
+          xin[q] = 0;
+#pragma unroll 4
+          for (int c2 = Ls.CHx - 1; c2 > chx[q]; c2--) {
+            const int u = rgx[q] * Ls.CHx + c2;
+            xin[q] = xba[u * 32 + lane] + xbb[u * 32 + lane] * xin[q];
+          }
+        }
+#pragma unroll
+        for (int m = 0; m < K; m++) {
+#pragma unroll
+          for (int q = 0; q < UPW; q++) {
+            const int i = chx[q] * K + m;
+            B[jl[q] * LD + i] = dt * (z[q][m] + PQ[q][m] * xin[q]);
+          }
+        }
+      }
+      __syncthreads();
+
+      // -------- Y sweep --------
+      S y[UPW][K];
+      {
+        S zz[UPW], Ru[UPW], Rm[UPW];
+#pragma unroll
+        for (int q = 0; q < UPW; q++) {
+          zz[q] = 0;
+          const int j0 = chy[q] * K;
+          Ru[q] = A[j0 * LD + colv[q]];        // row j0 - 1 (halo row at the block edge)
+          Rm[q] = A[(j0 + 1) * LD + colv[q]];  // row j0
+        }
+#pragma unroll
+        for (int m = 0; m < K; m++) {
+#pragma unroll
+          for (int q = 0; q < UPW; q++) {
+            const int j = chy[q] * K + m;
+            const S Rd = A[(j + 2) * LD + colv[q]];  // row j + 1
+            const auto g01 = V2<S>::ld(sG + 4 * j);
+            const S v = g01.x * Ru[q] + g01.y * Rm[q] + sG[4 * j + 2] * Rd;  // explicitY (:199)
+            const S rhs = B[j * LD + colv[q]] - (S)0.5 * v;                   // :205
+            zz[q] = rhs + (S)tb[j * 8 + 1] * zz[q];
+            y[q][m] = zz[q];
+            Ru[q] = Rm[q];
+            Rm[q] = Rd;
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < UPW; q++) yf[(warp + q * NW) * 32 + lane] = zz[q];
+      }
+      __syncthreads();
+      if (s + 1 < steps) issue_copies(k - 1, sT[(sc + 1) & 1]);
+      if (clustered) {
+        for (int qq = tid; qq < Ls.CGy * 32; qq += NT) {
+          const int g = qq >> 5, ln = qq & 31;
+          S a = 0;
+          for (int c2 = 0; c2 < Ls.CHy; c2++) a = yf[(g * Ls.CHy + c2) * 32 + ln] + (S)tb[(c2 * K + K - 1) * 8 + 4] * a;
+          blkF[qq] = a;
+        }
+        if (tid == 0) {
+          S b = 1;
+          for (int c2 = 0; c2 < Ls.CHy; c2++) b = (S)tb[(c2 * K + K - 1) * 8 + 4] * b;
+          s_tot[0] = b;
+        }
+        cg::cluster_group cl = cg::this_cluster();
+        cl.sync();
+        for (int qq = tid; qq < Ls.CGy * 32; qq += NT) {
+          S zv = 0;
+          for (int r = 0; r < rank; r++) {
+            const S* rf = cl.map_shared_rank(blkF, r);
+            const S* rt = cl.map_shared_rank(s_tot, r);
+            zv = rf[qq] + rt[0] * zv;
+          }
+          s_zin[qq] = zv;
+        }
+        __syncthreads();
+      }
+      {
+        S zin[UPW], xx[UPW];
+#pragma unroll
+        for (int q = 0; q < UPW; q++) {
+          zin[q] = clustered ? s_zin[cgy[q] * 32 + lane] : (S)0;
+#pragma unroll 4
+          for (int c2 = 0; c2 < chy[q]; c2++)
+            zin[q] = yf[(cgy[q] * Ls.CHy + c2) * 32 + lane] + (S)tb[(c2 * K + K - 1) * 8 + 4] * zin[q];
+          xx[q] = 0;
+        }
+#pragma unroll
+        for (int m = K - 1; m >= 0; m--) {
+#pragma unroll
+          for (int q = 0; q < UPW; q++) {
+            const int j = chy[q] * K + m;
+            const double2 nr = *reinterpret_cast<const double2*>(tb + j * 8 + 2);  // nY, rbY
+            const S zv = y[q][m] + (S)tb[j * 8 + 4] * zin[q];
+            xx[q] = (S)nr.y * zv + (S)nr.x * xx[q];
+            y[q][m] = xx[q];
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < UPW; q++) yb[(warp + q * NW) * 32 + lane] = xx[q];
+      }
+      __syncthreads();
+      if (clustered) {
+        for (int qq = tid; qq < Ls.CGy * 32; qq += NT) {
+          const int g = qq >> 5, ln = qq & 31;
+          S a = 0;
+          for (int c2 = Ls.CHy - 1; c2 >= 0; c2--) a = yb[(g * Ls.CHy + c2) * 32 + ln] + (S)tb[(c2 * K) * 8 + 5] * a;
+          blkB[qq] = a;
+        }
+        if (tid == 0) {
+          S b = 1;
+          for (int c2 = Ls.CHy - 1; c2 >= 0; c2--) b = (S)tb[(c2 * K) * 8 + 5] * b;
+          s_tot[1] = b;
+        }
+        cg::cluster_group cl = cg::this_cluster();
+        cl.sync();
+        for (int qq = tid; qq < Ls.CGy * 32; qq += NT) {
+          S xv = 0;
+          for (int r = C - 1; r > rank; r--) {
+            const S* rb_ = cl.map_shared_rank(blkB, r);
+            const S* rt = cl.map_shared_rank(s_tot, r);
+            xv = rb_[qq] + rt[1] * xv;
+          }
+          s_xin[qq] = xv;
+        }
+        __syncthreads();
+      }
+      {
+        S xin[UPW];
+#pragma unroll
+        for (int q = 0; q < UPW; q++) {
+          xin[q] = clustered ? s_xin[cgy[q] * 32 + lane] : (S)0;
+#pragma unroll 4
+          for (int c2 = Ls.CHy - 1; c2 > chy[q]; c2--)
+            xin[q] = yb[(cgy[q] * Ls.CHy + c2) * 32 + lane] + (S)tb[(c2 * K) * 8 + 5] * xin[q];
+        }
+#pragma unroll
+        for (int m = 0; m < K; m++) {
+#pragma unroll
+          for (int q = 0; q < UPW; q++) {
+            const int j = chy[q] * K + m;
+            const S xv = y[q][m] + (S)tb[j * 8 + 5] * xin[q];
+            y[q][m] = xv;
+            A[(j + 1) * LD + colv[q]] = xv;
+          }
+        }
+        // halo rows of the cluster neighbours, and the price on the last step
+#pragma unroll
+        for (int q = 0; q < UPW; q++) {
+          if (halo_prev && chy[q] == 0) halo_prev[colv[q]] = y[q][0];
+          if (halo_next && chy[q] == Ls.CHy - 1) halo_next[colv[q]] = y[q][K - 1];
+        }
+        if (s == steps - 1 && out_q >= 0) {
+          S pv = 0;
+#pragma unroll
+          for (int q = 0; q < UPW; q++)
+#pragma unroll
+            for (int m = 0; m < K; m++)
+              if (q == out_q && m == out_m) pv = y[q][m];
+          args.out[c.out + item.strike] = (double)pv;  // myResult[myYindex, myXindex]
+        }
+      }
+    }
+  }
+  if (clustered) cg::this_cluster().sync();
+}
+
+}  // namespace lvc

@@ -53,6 +53,7 @@ namespace {
 struct Launch {
   int kind, NT, KX, C;
   bool gstate;
+  bool full = false;
   int item_off, n_items, grid;
   size_t smem_bytes;
   int64_t gstate_per_cta;  // elements of the state type
@@ -165,7 +166,14 @@ template <typename S, typename PV>
 using RbFn = void (*)(RollbackArgs<S, PV>);
 
 template <typename S, typename PV>
-RbFn<S, PV> rollback_fn(int kind, int NT, int KX, bool gs) {
+RbFn<S, PV> rollback_fn(int kind, int NT, int KX, bool gs, bool full = false) {
+  if (kind == kKindLine && full) {
+    if (NT == 32) return lvc_line_full_kernel<S, PV, 32, 2>;
+    if (NT == 64) return lvc_line_full_kernel<S, PV, 64, 2>;
+    if (NT == 128) return lvc_line_full_kernel<S, PV, 128, 2>;
+    if (NT == 256) return lvc_line_full_kernel<S, PV, 256, 2>;
+    return nullptr;
+  }
   if (kind == kKindLine) {
     if (NT == 64) return lvc_line_kernel<S, PV, 64>;
     if (NT == 128) return lvc_line_kernel<S, PV, 128>;
@@ -196,6 +204,7 @@ int state_size() { return (int)sizeof(S); }
 struct Config {
   int kind, NT, KX, C;
   bool gstate;
+  bool full = false;
   int Ycs;
   size_t smem_bytes;
   int64_t grid_elems;
@@ -207,6 +216,25 @@ template <typename S>
 bool choose_line(int X, int Y, int max_smem, Config& cf) {
   if (X > 256) return false;
   for (int C = 1; C <= kMaxCluster; C *= 2) {
+    // full tiles: every line chunk, row group and CTA block complete; two
+    // units per warp, one unit per 512 cells
+    if (X % 32 == 0 && Y % C == 0 && (Y / C) % 32 == 0) {
+      const int Ycs = Y / C;
+      const int units = X * Ycs / 512;
+      const FullLayout F = full_layout<S>(X, Ycs, units);
+      if (units >= 2 && units <= 16 && F.Ux == units && F.Uy == units && F.total <= max_smem) {
+        cf.kind = kKindLine;
+        cf.full = true;
+        cf.NT = 16 * units;  // 32 lanes x units / 2 units per warp
+        cf.KX = kLineK;
+        cf.C = C;
+        cf.gstate = false;
+        cf.Ycs = Ycs;
+        cf.smem_bytes = (size_t)F.total;
+        cf.grid_elems = 0;
+        return true;
+      }
+    }
     // rows per CTA: a multiple of 4 when split, so every CTA's bulk copies
     // start on a 16-byte boundary
     const int Ycs = C == 1 ? Y : (int)round4(ceil_div(Y, C));
@@ -217,6 +245,7 @@ bool choose_line(int X, int Y, int max_smem, Config& cf) {
     const LineLayout L = line_layout<S>(X, Ycs, NT / 32);
     if (L.total > max_smem) continue;
     cf.kind = kKindLine;
+    cf.full = false;
     cf.NT = NT;
     cf.KX = kLineK;
     cf.C = C;
@@ -261,7 +290,7 @@ Config choose_config(int X, int Y, int max_smem) {
 
 template <typename S, typename PV>
 int prepare_launch(futhark_context* ctx, Launch& L) {
-  RbFn<S, PV> fn = rollback_fn<S, PV>(L.kind, L.NT, L.KX, L.gstate);
+  RbFn<S, PV> fn = rollback_fn<S, PV>(L.kind, L.NT, L.KX, L.gstate, L.full);
   if (!fn) return set_error(ctx, FUTHARK_PROGRAM_ERROR, "no rollback kernel for this configuration");
   // Several launch classes may share one kernel instantiation with different
   // shared-memory sizes: allow the device maximum once for all of them.
@@ -325,7 +354,7 @@ cudaError_t launch_rollback(lvc_plan* P, const Launch& L, cudaStream_t s) {
     cfg.attrs = &attr;
     cfg.numAttrs = 1;
   }
-  return cudaLaunchKernelEx(&cfg, rollback_fn<S, PV>(L.kind, L.NT, L.KX, L.gstate), a);
+  return cudaLaunchKernelEx(&cfg, rollback_fn<S, PV>(L.kind, L.NT, L.KX, L.gstate, L.full), a);
 }
 
 // Enqueue one run of a plan.  `ev` (optional) receives a start/stop event
@@ -392,8 +421,8 @@ int plan_build(futhark_context* ctx, const lvc_calibration* cs, int n, lvc_plan*
   P->params.assign(cs, cs + n);
   P->calibs.resize(n);
   P->row_start.assign(n + 1, 0);
-  std::map<std::tuple<int, int, int, int, bool>, std::vector<std::pair<int64_t, Item>>> classes;
-  std::map<std::tuple<int, int, int, int, bool>, Config> class_cfg;
+  std::map<std::tuple<int, int, int, int, bool, bool>, std::vector<std::pair<int64_t, Item>>> classes;
+  std::map<std::tuple<int, int, int, int, bool, bool>, Config> class_cfg;
   int64_t tab_off = 0, piv_off = 0, out_off = 0;
   for (int i = 0; i < n; i++) {
     const lvc_calibration& c = cs[i];
@@ -417,7 +446,7 @@ int plan_build(futhark_context* ctx, const lvc_calibration* cs, int n, lvc_plan*
     d.out = out_off;
     out_off += c.outer;
     P->row_start[i + 1] = P->row_start[i] + (int64_t)(c.numT > 1 ? c.numT - 1 : 0) * c.numY;
-    const auto key = std::make_tuple(cf.kind, cf.NT, cf.KX, cf.C, cf.gstate);
+    const auto key = std::make_tuple(cf.kind, cf.NT, cf.KX, cf.C, cf.gstate, cf.full);
     auto& cls = classes[key];
     auto it = class_cfg.find(key);
     if (it == class_cfg.end()) {
@@ -443,6 +472,7 @@ int plan_build(futhark_context* ctx, const lvc_calibration* cs, int n, lvc_plan*
     const Config& cf = class_cfg[kv.first];
     Launch L;
     L.kind = cf.kind;
+    L.full = cf.full;
     L.NT = cf.NT;
     L.KX = cf.KX;
     L.C = cf.C;
@@ -1084,6 +1114,7 @@ extern "C" int lvc_entry_main_f64_noalloc(struct futhark_context* ctx, double* p
   if (outer > 0) {
     Launch L;
     L.kind = cf.kind;
+    L.full = cf.full;
     L.NT = cf.NT;
     L.KX = cf.KX;
     L.C = cf.C;
@@ -1120,7 +1151,7 @@ extern "C" int lvc_entry_main_f64_noalloc(struct futhark_context* ctx, double* p
       cfg.attrs = &attr;
       cfg.numAttrs = 1;
     }
-    LVC_CUDA(ctx, cudaLaunchKernelEx(&cfg, rollback_fn<double, double>(L.kind, L.NT, L.KX, false), a));
+    LVC_CUDA(ctx, cudaLaunchKernelEx(&cfg, rollback_fn<double, double>(L.kind, L.NT, L.KX, false, L.full), a));
   }
   int h = 0;
   LVC_CUDA(ctx, cudaMemcpyAsync(&h, d_err, sizeof(int), cudaMemcpyDeviceToHost, s));

@@ -112,6 +112,17 @@ def test_ragged_sizes_match_oracle(ctx, oracle, shape):
     assert rel_err(got, oracle_for(oracle, c)) <= F64_RTOL
 
 
+@pytest.mark.parametrize("shape", [(128, 128), (256, 64), (64, 256)])
+def test_cluster_runs_many_instances_per_cluster(ctx, oracle, shape):
+    # more strikes than resident clusters: every cluster prices several
+    # instances in a row, which exercises the hand-over of halo rows between them
+    X, Y = shape
+    c = wl.Calibration(300, X, Y, 5, 0.03, 5.0, 0.2, 0.6, 0.5)
+    got = ctx.main_f64(*[getattr(c, k) for k in FIELDS])
+    idx = list(range(0, 300, 23)) + [299]
+    assert rel_err(got[idx], oracle_for(oracle, c, idx)) <= F64_RTOL
+
+
 def test_hbm_state_fallback_matches_oracle(ctx, oracle):
     # 512 x 512 f64 does not fit on chip even over a 16-CTA cluster
     c = wl.Calibration(2, 512, 512, 3, 0.03, 5.0, 0.2, 0.6, 0.5)
