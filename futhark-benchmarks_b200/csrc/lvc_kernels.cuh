@@ -157,16 +157,16 @@ __global__ void __launch_bounds__(256) lvc_setup_kernel(const CalibDev* __restri
           const int je = min(r1, jb + kLineK);
           double pr = 1.0;
           for (int j = jb; j < je; j++) {
-            pr = pr * yc[8 * j + 1];
-            yc[8 * j + 4] = pr;
+            pr = pr * yc[8 * j + kSlotMY];
+            yc[8 * j + kSlotCP] = pr;
           }
           pr = 1.0;
           for (int j = je - 1; j >= jb; j--) {
-            pr = pr * yc[8 * j + 2];
-            yc[8 * j + 5] = pr;
+            pr = pr * yc[8 * j + kSlotNY];
+            yc[8 * j + kSlotCQ] = pr;
           }
           for (int j = jb; j < je; j++) {
-            yc[8 * j + 6] = 0.0;
+            yc[8 * j + 5] = 0.0;
             yc[8 * j + 7] = 0.0;
           }
         }

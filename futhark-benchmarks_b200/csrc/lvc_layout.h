@@ -53,7 +53,7 @@ struct TabLayout {
   int64_t eyt;    // [T-1][eyt_ld]  exp(2*(y_j - 0.5*nu^2*t_k))            (chunk family)
   int64_t yco;    // [T-1][Y][4]    Y-sweep multipliers: mY_j, nY_j, 1/b'_j, 0  (chunk family)
   int64_t wcol;   // [3][xa]  W_k(i) = 0.25 * eX_i * Dxx_i[k]                 (line family)
-  int64_t stab;   // [T-1][Y][8]    e_j, mY_j, nY_j, 1/b'_j, cp_j, cq_j, 0, 0 (line family)
+  int64_t stab;   // [T-1][Y][8]    step-table rows, slots kSlot* below       (line family)
   int64_t total;
   int64_t eyt_ld, xa;
 };
@@ -84,6 +84,18 @@ LVC_HD TabLayout tab_layout(int X, int Y, int T, int Xp, int kind) {
   L.total = o;
   return L;
 }
+
+// Slots of a line-family step-table row (8 doubles; slots 5 and 7 are zero).
+// The pair that kernels read as one 16-byte vector, (nY, 1/b'), starts on an
+// even slot.
+enum : int {
+  kSlotE = 0,   // exp(2 (y_j - 0.5 nu^2 t_k))
+  kSlotMY = 1,  // forward multiplier -a_j / b'_{j-1}
+  kSlotNY = 2,  // backward multiplier -c_j / b'_j
+  kSlotRB = 3,  // 1 / b'_j
+  kSlotCQ = 4,  // suffix product of nY inside the chunk
+  kSlotCP = 6,  // prefix product of mY inside the chunk
+};
 
 // Line family: the pivot rows are stored exactly as the kernel's shared-memory
 // image of them -- row j of step k at ((k*Y4 + j) * LD) with the odd row

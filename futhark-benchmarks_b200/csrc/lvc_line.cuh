@@ -239,7 +239,7 @@ __global__ void __launch_bounds__(NT, (NT >= 512 ? 1 : 512 / NT)) lvc_line_kerne
       const double* tb = sT[sc & 1];
       const S dt = (S)tabc[Lt.dtinv + k];
       const S half = (S)0.5;
-      const S e = vr ? (S)tb[jl * 8] : (S)0;
+      const S e = vr ? (S)tb[jl * 8 + kSlotE] : (S)0;
       const S g0 = vr ? sG[4 * jl] : (S)0, g1 = vr ? sG[4 * jl + 1] : (S)0, g2 = vr ? sG[4 * jl + 2] : (S)0;
 
       // -------- X sweep pass 1: explicitX + explicitY, implicitX forward (chunk-local) --------
@@ -336,7 +336,7 @@ __global__ void __launch_bounds__(NT, (NT >= 512 ? 1 : 512 / NT)) lvc_line_kerne
           if (m < ny) {
             const int j = jb + m;
             const S v = vc ? B[j * LD + col] : (S)0;
-            zz = v + (S)tb[j * 8 + 1] * zz;
+            zz = v + (S)tb[j * 8 + kSlotMY] * zz;
             y[m] = zz;
           }
         }
@@ -351,13 +351,13 @@ __global__ void __launch_bounds__(NT, (NT >= 512 ? 1 : 512 / NT)) lvc_line_kerne
           S a = 0;
           for (int c2 = 0; c2 < CHy; c2++) {
             const int je = min(Yc, c2 * K + K);
-            a = yf[(g * Ls.CHy + c2) * 32 + ln] + (S)tb[(je - 1) * 8 + 4] * a;
+            a = yf[(g * Ls.CHy + c2) * 32 + ln] + (S)tb[(je - 1) * 8 + kSlotCP] * a;
           }
           blkF[q] = a;
         }
         if (tid == 0) {
           S b = 1;
-          for (int c2 = 0; c2 < CHy; c2++) b = (S)tb[(min(Yc, c2 * K + K) - 1) * 8 + 4] * b;
+          for (int c2 = 0; c2 < CHy; c2++) b = (S)tb[(min(Yc, c2 * K + K) - 1) * 8 + kSlotCP] * b;
           s_tot[0] = b;
         }
         cg::cluster_group cl = cg::this_cluster();
@@ -377,13 +377,13 @@ __global__ void __launch_bounds__(NT, (NT >= 512 ? 1 : 512 / NT)) lvc_line_kerne
       if (ny > 0) {
         S zin = clustered ? s_zin[cgy * 32 + lane] : (S)0;
         for (int c2 = 0; c2 < chy; c2++)
-          zin = yf[(cgy * Ls.CHy + c2) * 32 + lane] + (S)tb[(c2 * K + K - 1) * 8 + 4] * zin;
+          zin = yf[(cgy * Ls.CHy + c2) * 32 + lane] + (S)tb[(c2 * K + K - 1) * 8 + kSlotCP] * zin;
 #pragma unroll
         for (int m = K - 1; m >= 0; m--) {
           if (m < ny) {
             const int j = jb + m;
-            const S zv = y[m] + (S)tb[j * 8 + 4] * zin;
-            xx = (S)tb[j * 8 + 3] * zv + (S)tb[j * 8 + 2] * xx;
+            const S zv = y[m] + (S)tb[j * 8 + kSlotCP] * zin;
+            xx = (S)tb[j * 8 + kSlotRB] * zv + (S)tb[j * 8 + kSlotNY] * xx;
             y[m] = xx;
           }
         }
@@ -394,12 +394,12 @@ __global__ void __launch_bounds__(NT, (NT >= 512 ? 1 : 512 / NT)) lvc_line_kerne
         for (int q = tid; q < Ls.CGy * 32; q += NT) {
           const int g = q >> 5, ln = q & 31;
           S a = 0;
-          for (int c2 = CHy - 1; c2 >= 0; c2--) a = yb[(g * Ls.CHy + c2) * 32 + ln] + (S)tb[(c2 * K) * 8 + 5] * a;
+          for (int c2 = CHy - 1; c2 >= 0; c2--) a = yb[(g * Ls.CHy + c2) * 32 + ln] + (S)tb[(c2 * K) * 8 + kSlotCQ] * a;
           blkB[q] = a;
         }
         if (tid == 0) {
           S b = 1;
-          for (int c2 = CHy - 1; c2 >= 0; c2--) b = (S)tb[(c2 * K) * 8 + 5] * b;
+          for (int c2 = CHy - 1; c2 >= 0; c2--) b = (S)tb[(c2 * K) * 8 + kSlotCQ] * b;
           s_tot[1] = b;
         }
         cg::cluster_group cl = cg::this_cluster();
@@ -418,12 +418,12 @@ __global__ void __launch_bounds__(NT, (NT >= 512 ? 1 : 512 / NT)) lvc_line_kerne
       if (ny > 0) {
         S xin = clustered ? s_xin[cgy * 32 + lane] : (S)0;
         for (int c2 = CHy - 1; c2 > chy; c2--)
-          xin = yb[(cgy * Ls.CHy + c2) * 32 + lane] + (S)tb[(c2 * K) * 8 + 5] * xin;
+          xin = yb[(cgy * Ls.CHy + c2) * 32 + lane] + (S)tb[(c2 * K) * 8 + kSlotCQ] * xin;
 #pragma unroll
         for (int m = 0; m < K; m++) {
           if (m < ny) {
             const int j = jb + m;
-            const S xv = y[m] + (S)tb[j * 8 + 5] * xin;
+            const S xv = y[m] + (S)tb[j * 8 + kSlotCQ] * xin;
             if (vc) {
               A[j * LD + col] = xv;
               if (s == steps - 1 && col == c.xindex && r0 + j == c.yindex)
@@ -643,7 +643,7 @@ __global__ void __launch_bounds__(NT, (FullMinBlocks<NT>::v)) lvc_line_full_kern
         for (int q = 0; q < UPW; q++) {
           const int ib = chx[q] * K;
           const S* Arow = A + (jl[q] + 1) * LD;
-          e[q] = (S)tb[jl[q] * 8];
+          e[q] = (S)tb[jl[q] * 8 + kSlotE];
           g0[q] = sG[4 * jl[q]];
           g1[q] = sG[4 * jl[q] + 1];
           g2[q] = sG[4 * jl[q] + 2];
@@ -698,7 +698,7 @@ __global__ void __launch_bounds__(NT, (FullMinBlocks<NT>::v)) lvc_line_full_kern
           }
           xl[q] = 0;
           Ql[q] = 1;
-          e[q] = (S)tb[jl[q] * 8];
+          e[q] = (S)tb[jl[q] * 8 + kSlotE];
         }
 #pragma unroll
         for (int m = K - 1; m >= 0; m--) {
@@ -765,7 +765,7 @@ __global__ void __launch_bounds__(NT, (FullMinBlocks<NT>::v)) lvc_line_full_kern
             const auto g01 = V2<S>::ld(sG + 4 * j);
             const S v = g01.x * Ru[q] + g01.y * Rm[q] + sG[4 * j + 2] * Rd;  // explicitY (:199)
             const S rhs = B[j * LD + colv[q]] - (S)0.5 * v;                   // :205
-            zz[q] = rhs + (S)tb[j * 8 + 1] * zz[q];
+            zz[q] = rhs + (S)tb[j * 8 + kSlotMY] * zz[q];
             y[q][m] = zz[q];
             Ru[q] = Rm[q];
             Rm[q] = Rd;
@@ -780,12 +780,12 @@ __global__ void __launch_bounds__(NT, (FullMinBlocks<NT>::v)) lvc_line_full_kern
         for (int qq = tid; qq < Ls.CGy * 32; qq += NT) {
           const int g = qq >> 5, ln = qq & 31;
           S a = 0;
-          for (int c2 = 0; c2 < Ls.CHy; c2++) a = yf[(g * Ls.CHy + c2) * 32 + ln] + (S)tb[(c2 * K + K - 1) * 8 + 4] * a;
+          for (int c2 = 0; c2 < Ls.CHy; c2++) a = yf[(g * Ls.CHy + c2) * 32 + ln] + (S)tb[(c2 * K + K - 1) * 8 + kSlotCP] * a;
           blkF[qq] = a;
         }
         if (tid == 0) {
           S b = 1;
-          for (int c2 = 0; c2 < Ls.CHy; c2++) b = (S)tb[(c2 * K + K - 1) * 8 + 4] * b;
+          for (int c2 = 0; c2 < Ls.CHy; c2++) b = (S)tb[(c2 * K + K - 1) * 8 + kSlotCP] * b;
           s_tot[0] = b;
         }
         cg::cluster_group cl = cg::this_cluster();
@@ -808,7 +808,7 @@ __global__ void __launch_bounds__(NT, (FullMinBlocks<NT>::v)) lvc_line_full_kern
           zin[q] = clustered ? s_zin[cgy[q] * 32 + lane] : (S)0;
 #pragma unroll 4
           for (int c2 = 0; c2 < chy[q]; c2++)
-            zin[q] = yf[(cgy[q] * Ls.CHy + c2) * 32 + lane] + (S)tb[(c2 * K + K - 1) * 8 + 4] * zin[q];
+            zin[q] = yf[(cgy[q] * Ls.CHy + c2) * 32 + lane] + (S)tb[(c2 * K + K - 1) * 8 + kSlotCP] * zin[q];
           xx[q] = 0;
         }
 #pragma unroll
@@ -816,8 +816,8 @@ __global__ void __launch_bounds__(NT, (FullMinBlocks<NT>::v)) lvc_line_full_kern
 #pragma unroll
           for (int q = 0; q < UPW; q++) {
             const int j = chy[q] * K + m;
-            const double2 nr = *reinterpret_cast<const double2*>(tb + j * 8 + 2);  // nY, rbY
-            const S zv = y[q][m] + (S)tb[j * 8 + 4] * zin[q];
+            const double2 nr = *reinterpret_cast<const double2*>(tb + j * 8 + kSlotNY);  // nY, 1/b'
+            const S zv = y[q][m] + (S)tb[j * 8 + kSlotCP] * zin[q];
             xx[q] = (S)nr.y * zv + (S)nr.x * xx[q];
             y[q][m] = xx[q];
           }
@@ -830,12 +830,12 @@ __global__ void __launch_bounds__(NT, (FullMinBlocks<NT>::v)) lvc_line_full_kern
         for (int qq = tid; qq < Ls.CGy * 32; qq += NT) {
           const int g = qq >> 5, ln = qq & 31;
           S a = 0;
-          for (int c2 = Ls.CHy - 1; c2 >= 0; c2--) a = yb[(g * Ls.CHy + c2) * 32 + ln] + (S)tb[(c2 * K) * 8 + 5] * a;
+          for (int c2 = Ls.CHy - 1; c2 >= 0; c2--) a = yb[(g * Ls.CHy + c2) * 32 + ln] + (S)tb[(c2 * K) * 8 + kSlotCQ] * a;
           blkB[qq] = a;
         }
         if (tid == 0) {
           S b = 1;
-          for (int c2 = Ls.CHy - 1; c2 >= 0; c2--) b = (S)tb[(c2 * K) * 8 + 5] * b;
+          for (int c2 = Ls.CHy - 1; c2 >= 0; c2--) b = (S)tb[(c2 * K) * 8 + kSlotCQ] * b;
           s_tot[1] = b;
         }
         cg::cluster_group cl = cg::this_cluster();
@@ -858,14 +858,14 @@ __global__ void __launch_bounds__(NT, (FullMinBlocks<NT>::v)) lvc_line_full_kern
           xin[q] = clustered ? s_xin[cgy[q] * 32 + lane] : (S)0;
 #pragma unroll 4
           for (int c2 = Ls.CHy - 1; c2 > chy[q]; c2--)
-            xin[q] = yb[(cgy[q] * Ls.CHy + c2) * 32 + lane] + (S)tb[(c2 * K) * 8 + 5] * xin[q];
+            xin[q] = yb[(cgy[q] * Ls.CHy + c2) * 32 + lane] + (S)tb[(c2 * K) * 8 + kSlotCQ] * xin[q];
         }
 #pragma unroll
         for (int m = 0; m < K; m++) {
 #pragma unroll
           for (int q = 0; q < UPW; q++) {
             const int j = chy[q] * K + m;
-            const S xv = y[q][m] + (S)tb[j * 8 + 5] * xin[q];
+            const S xv = y[q][m] + (S)tb[j * 8 + kSlotCQ] * xin[q];
             y[q][m] = xv;
             A[(j + 1) * LD + colv[q]] = xv;
           }
