@@ -59,6 +59,10 @@ def parse():
     ap.add_argument("--plain-calibs", type=int, default=0,
                     help="time the plain per-call form on the first N calibrations (0 = all)")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--serving-rates", default="100,1000,5000,20000",
+                    help="Poisson arrival rates (requests/s) of the serving sweep")
+    ap.add_argument("--serving-requests", type=int, default=300)
     ap.add_argument("--cpu-seconds", type=float, default=15.0,
                     help="target CPU time of the bounded CPU-baseline sample")
     return ap.parse_args()
@@ -207,6 +211,48 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_serving(pkg, wl, ctx, args, rank, precision):
+    """Poisson request streams through the serving runtime (continuous batching)."""
+    import numpy as np
+    out = []
+    reqs = wl.uneven_mix(args.serving_requests, seed=1000 + args.seed + rank)
+    with pkg.Server(ctx, precision=precision) as srv:
+        # warm-up: kernels and pool
+        for t in [srv.submit(c) for c in reqs[:8]]:
+            srv.result(t)
+        check = None
+        for rate in [float(r) for r in args.serving_rates.split(",") if r]:
+            srv.reset_stats()
+            arrivals = wl.poisson_arrivals(rate, len(reqs), seed=7 + int(rate))
+            t0 = time.perf_counter()
+            tickets = []
+            for c, ta in zip(reqs, arrivals):
+                dt = t0 + ta - time.perf_counter()
+                if dt > 0:
+                    time.sleep(dt)
+                tickets.append(srv.submit(c))
+            res = [srv.result(t) for t in tickets]
+            st = srv.stats()
+            out.append({"rate_req_per_s": rate, "requests": len(reqs),
+                        "throughput_options_per_s": st["throughput_options_per_s"],
+                        "throughput_req_per_s": st["completed"] / st["span_s"] if st["span_s"] else None,
+                        "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "max_ms": st["max_ms"],
+                        "batches": st["batches"], "failed": st["failed"]})
+            if check is None:
+                check = res
+    # max relative error vs the FP64 oracle on the first few requests
+    err = None
+    if rank == 0 and check is not None and precision == pkg.F64:
+        from oracle import oracle
+        k = 3
+        ref = oracle.batch_f64(reqs[:k])
+        got = np.concatenate(check[:k])
+        err = float(np.max(np.abs(got - ref) / np.abs(ref)))
+    return {"sweep": out, "max_rel_err_vs_fp64_oracle": err,
+            "oracle_sample": "first 3 requests of the stream",
+            "workload": f"{len(reqs)} requests per rate drawn as the uneven mix (seed 1000+rank)"}
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -310,6 +356,10 @@ def run_ours(args):
         plain = {"value": sum(c.outer for c in sub) / dt, "unit": UNIT,
                  "calls": len(sub), "form": "futhark_entry_main_f64 once per calibration"}
 
+    serving = None
+    if not args.no_serving:
+        serving = run_serving(pkg, wl, ctx, args, rank, precision)
+
     cpu = None
     if rank == 0 and world == 1:
         cpu = cpu_baseline(calibs, args.cpu_seconds)
@@ -337,6 +387,7 @@ def run_ours(args):
                                         "(MEASURED_PEAKS.json has no FP64 figure)",
                          "smem_peak_gbs": smem_peak},
             "plain_per_call": plain,
+            "serving": serving,
             "batched_vs_plain": (value / plain["value"]) if plain else None,
             "cpu_baseline": cpu,
             "clocks": clk,

@@ -69,6 +69,20 @@ class Calibration:
         return self.outer * self.numX * self.numY * max(self.numT - 1, 0)
 
 
+class _ServerConfig(ctypes.Structure):
+    _fields_ = [("precision", ctypes.c_int32), ("max_inflight_requests", ctypes.c_int32),
+                ("max_batch_requests", ctypes.c_int32), ("num_streams", ctypes.c_int32),
+                ("hbm_budget_bytes", ctypes.c_int64)]
+
+
+class _ServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_int64), ("completed", ctypes.c_int64), ("failed", ctypes.c_int64),
+                ("options", ctypes.c_int64), ("batches", ctypes.c_int64), ("hbm_reserved_bytes", ctypes.c_int64),
+                ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double), ("mean_ms", ctypes.c_double),
+                ("max_ms", ctypes.c_double), ("throughput_options_per_s", ctypes.c_double),
+                ("span_s", ctypes.c_double)]
+
+
 def load_library(path: str = LIB_PATH):
     """Load liblvc.so and declare its C signatures."""
     global _lib
@@ -114,6 +128,13 @@ def load_library(path: str = LIB_PATH):
         "lvc_batch": (ctypes.c_int, [vp, ctypes.POINTER(_Calib), i32, i32, vp]),
         "lvc_context_stream": (vp, [vp]),
         "lvc_probe_peaks": (ctypes.c_int, [vp, ctypes.POINTER(f64), ctypes.POINTER(f64)]),
+        "lvc_server_new": (ctypes.c_int, [vp, ctypes.POINTER(_ServerConfig), ctypes.POINTER(vp)]),
+        "lvc_server_submit": (ctypes.c_int, [vp, ctypes.POINTER(_Calib), ctypes.POINTER(ctypes.c_uint64)]),
+        "lvc_server_poll": (ctypes.c_int, [vp, ctypes.c_uint64, ctypes.POINTER(i32)]),
+        "lvc_server_wait": (ctypes.c_int, [vp, ctypes.c_uint64, vp, f64]),
+        "lvc_server_stats": (ctypes.c_int, [vp, ctypes.POINTER(_ServerStats)]),
+        "lvc_server_reset_stats": (ctypes.c_int, [vp]),
+        "lvc_server_free": (ctypes.c_int, [vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -304,3 +325,62 @@ def run_dataset(ctx: Context, path: str, f64: bool = False) -> np.ndarray:
         raise ValueError(f"{path}: expected the 9 inputs of main, got {len(vals)} values")
     args = [int(v) for v in vals[:4]] + [float(v) for v in vals[4:]]
     return ctx.main_f64(*args) if f64 else ctx.main(*args)
+
+
+class Server:
+    """lvc_server: continuous batching of calibration requests on one device.
+
+    submit() returns a ticket at once; result(ticket) blocks until that
+    request's prices are ready.  Requests that arrive while others run are
+    admitted as streams, the HBM budget and SMs free up, and run concurrently.
+    """
+
+    def __init__(self, ctx: Context, precision: int = F64, max_inflight_requests: int = 0,
+                 max_batch_requests: int = 0, num_streams: int = 0, hbm_budget_bytes: int = 0):
+        self.ctx = ctx
+        cfg = _ServerConfig(precision, max_inflight_requests, max_batch_requests, num_streams, hbm_budget_bytes)
+        self._s = ctypes.c_void_p()
+        ctx._check(ctx.lib.lvc_server_new(ctx._ctx, ctypes.byref(cfg), ctypes.byref(self._s)))
+        self._outer = {}
+
+    def submit(self, c: Calibration) -> int:
+        t = ctypes.c_uint64()
+        self.ctx._check(self.ctx.lib.lvc_server_submit(self._s, ctypes.byref(_Calib(*astuple(c))), ctypes.byref(t)))
+        self._outer[t.value] = c.outer
+        return t.value
+
+    def done(self, ticket: int) -> bool:
+        d = ctypes.c_int32()
+        self.ctx._check(self.ctx.lib.lvc_server_poll(self._s, ticket, ctypes.byref(d)))
+        return bool(d.value)
+
+    def result(self, ticket: int, timeout_s: float = 0.0) -> np.ndarray:
+        n = self._outer.pop(ticket)
+        out = np.empty(max(n, 1), dtype=np.float64)
+        self.ctx._check(self.ctx.lib.lvc_server_wait(self._s, ticket, out.ctypes.data, timeout_s))
+        return out[:n]
+
+    def stats(self) -> dict:
+        st = _ServerStats()
+        self.ctx._check(self.ctx.lib.lvc_server_stats(self._s, ctypes.byref(st)))
+        return {k: getattr(st, k) for k, _ in _ServerStats._fields_}
+
+    def reset_stats(self):
+        self.ctx.lib.lvc_server_reset_stats(self._s)
+
+    def close(self):
+        if self._s:
+            self.ctx.lib.lvc_server_free(self._s)
+            self._s = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -14,7 +14,12 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
+#include <condition_variable>
+#include <deque>
+#include <thread>
+#include <unordered_map>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -50,6 +55,85 @@ struct futhark_f64_1d {
 
 namespace {
 
+// Grow-only pool of device memory with a first-fit free list.  Plans built
+// for the entry points and for the serving runtime take their buffers from a
+// pool, so steady-state calls do not reach cudaMalloc/cudaFree (which
+// synchronise the device).  With a budget, allocation fails instead of
+// growing past it -- the serving runtime's HBM admission control.
+struct DevicePool {
+  std::mutex mu;
+  size_t budget = 0;               // 0: unlimited
+  size_t chunk = size_t(256) << 20;
+  std::vector<char*> blocks;
+  std::map<char*, size_t> free_;   // start -> size
+  std::map<char*, size_t> used_;
+  size_t reserved = 0, in_use = 0;
+
+  ~DevicePool() {
+    for (char* b : blocks) cudaFree(b);
+  }
+  bool grow(size_t sz) {
+    if (budget && reserved + sz > budget) return false;
+    char* p = nullptr;
+    if (cudaMalloc(&p, sz) != cudaSuccess) {
+      cudaGetLastError();
+      return false;
+    }
+    blocks.push_back(p);
+    reserved += sz;
+    insert_free(p, sz);
+    return true;
+  }
+  void insert_free(char* p, size_t sz) {
+    auto nx = free_.lower_bound(p);
+    if (nx != free_.end() && p + sz == nx->first) {
+      sz += nx->second;
+      nx = free_.erase(nx);
+    }
+    if (nx != free_.begin()) {
+      auto pv = std::prev(nx);
+      if (pv->first + pv->second == p) {
+        pv->second += sz;
+        return;
+      }
+    }
+    free_[p] = sz;
+  }
+  void* alloc(size_t bytes) {
+    bytes = (std::max<size_t>(bytes, 1) + 255) & ~size_t(255);
+    std::lock_guard<std::mutex> g(mu);
+    for (int attempt = 0; attempt < 2; attempt++) {
+      for (auto it = free_.begin(); it != free_.end(); ++it) {
+        if (it->second >= bytes) {
+          char* p = it->first;
+          const size_t rem = it->second - bytes;
+          free_.erase(it);
+          if (rem) free_[p + bytes] = rem;
+          used_[p] = bytes;
+          in_use += bytes;
+          return p;
+        }
+      }
+      if (attempt == 0) {
+        size_t sz = std::max(bytes, chunk);
+        if (budget && reserved + sz > budget) sz = bytes;
+        if (!grow(sz)) return nullptr;
+      }
+    }
+    return nullptr;
+  }
+  void release(void* vp) {
+    if (!vp) return;
+    std::lock_guard<std::mutex> g(mu);
+    auto it = used_.find(static_cast<char*>(vp));
+    if (it == used_.end()) return;
+    const size_t sz = it->second;
+    used_.erase(it);
+    in_use -= sz;
+    insert_free(static_cast<char*>(vp), sz);
+  }
+};
+
 struct Launch {
   int kind, NT, KX, C;
   bool gstate;
@@ -58,6 +142,7 @@ struct Launch {
   size_t smem_bytes;
   int64_t gstate_per_cta;  // elements of the state type
   int64_t gstate_off;      // elements
+  double sm_per_cta = 1.0; // SMs one CTA of this launch occupies at full residency
 };
 
 }  // namespace
@@ -84,6 +169,10 @@ struct lvc_plan {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   double rollback_ms = 0.0;
+  DevicePool* pool = nullptr;  // where the buffers come from (null: cudaMalloc)
+  bool use_graph = true;       // capture one run into a CUDA graph
+  int max_sms = 0;             // cap on the SMs a launch may occupy (0: all)
+  double sms = 0.0;            // SMs the widest launch occupies
 };
 
 struct futhark_context {
@@ -96,6 +185,7 @@ struct futhark_context {
   int max_smem = 0;
   bool ok = false;
   lvc_plan* entry_plan = nullptr;  // reused by the entry points while sizes repeat
+  DevicePool* pool = nullptr;      // buffers of the entry points' plans
 };
 
 namespace {
@@ -289,7 +379,7 @@ Config choose_config(int X, int Y, int max_smem) {
 }
 
 template <typename S, typename PV>
-int prepare_launch(futhark_context* ctx, Launch& L) {
+int prepare_launch(futhark_context* ctx, Launch& L, int max_sms = 0) {
   RbFn<S, PV> fn = rollback_fn<S, PV>(L.kind, L.NT, L.KX, L.gstate, L.full);
   if (!fn) return set_error(ctx, FUTHARK_PROGRAM_ERROR, "no rollback kernel for this configuration");
   // Several launch classes may share one kernel instantiation with different
@@ -299,11 +389,16 @@ int prepare_launch(futhark_context* ctx, Launch& L) {
   if (L.C > 8)
     LVC_CUDA(ctx, cudaFuncSetAttribute((const void*)fn,
                                        cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+  // max_sms < 0: one CTA (cluster) per work item instead of a persistent
+  // grid, so the block scheduler shares SMs among concurrent launches
+  const bool per_item = max_sms < 0;
+  const int sms = (max_sms > 0 && max_sms < ctx->num_sms) ? max_sms : ctx->num_sms;
   int resident = 0;
   if (L.C == 1) {
     int per_sm = 0;
     LVC_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, L.NT, L.smem_bytes));
-    resident = per_sm * ctx->num_sms;
+    resident = per_sm * sms;
+    L.sm_per_cta = per_sm > 0 ? 1.0 / per_sm : 1.0;
   } else {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(L.C * std::max(1, L.n_items));
@@ -318,11 +413,13 @@ int prepare_launch(futhark_context* ctx, Launch& L) {
     cfg.numAttrs = 1;
     int ncl = 0;
     LVC_CUDA(ctx, cudaOccupancyMaxActiveClusters(&ncl, fn, &cfg));
-    resident = ncl;
+    L.sm_per_cta = ncl > 0 ? (double)ctx->num_sms / ((double)ncl * L.C) : 1.0;
+    resident = (int)((int64_t)ncl * sms / ctx->num_sms);
+    if (resident < 1 && ncl > 0) resident = 1;
   }
   if (resident <= 0)
     return set_error(ctx, FUTHARK_PROGRAM_ERROR, "rollback configuration does not fit on the device");
-  L.grid = std::min(L.n_items, resident) * L.C;
+  L.grid = (per_item ? L.n_items : std::min(L.n_items, resident)) * L.C;
   return 0;
 }
 
@@ -390,14 +487,11 @@ void plan_release(lvc_plan* P) {
   if (!P) return;
   if (P->exec) cudaGraphExecDestroy(P->exec);
   if (P->graph) cudaGraphDestroy(P->graph);
-  cudaFree(P->d_calibs);
-  cudaFree(P->d_tabs);
-  cudaFree(P->d_piv);
-  cudaFree(P->d_out);
-  cudaFree(P->d_rowstart);
-  cudaFree(P->d_items);
-  cudaFree(P->d_gstate);
-  cudaFree(P->d_err);
+  void* bufs[] = {P->d_calibs, P->d_tabs, P->d_piv, P->d_out, P->d_rowstart, P->d_items, P->d_gstate, P->d_err};
+  for (void* b : bufs) {
+    if (!b) continue;
+    if (P->pool) P->pool->release(b); else cudaFree(b);
+  }
   delete P;
 }
 
@@ -483,7 +577,8 @@ int plan_build(futhark_context* ctx, const lvc_calibration* cs, int n, lvc_plan*
     L.gstate_per_cta = cf.gstate ? cf.grid_elems : 0;
     for (auto& e : v) P->items.push_back(e.second);
     if (L.n_items > 0) {
-      if (int rc = prepare_launch<S, PV>(ctx, L)) return rc;
+      if (int rc = prepare_launch<S, PV>(ctx, L, P->max_sms)) return rc;
+      P->sms = std::max(P->sms, std::min<double>(L.grid * L.sm_per_cta, ctx->num_sms));
     } else {
       L.grid = 0;
     }
@@ -496,14 +591,24 @@ int plan_build(futhark_context* ctx, const lvc_calibration* cs, int n, lvc_plan*
   P->pivot_grid = (int)std::max<int64_t>(1, std::min<int64_t>((rows + 127) / 128, 64LL * ctx->num_sms));
 
   // device buffers
-  LVC_CUDA(ctx, cudaMalloc(&P->d_calibs, sizeof(CalibDev) * std::max(1, n)));
-  LVC_CUDA(ctx, cudaMalloc(&P->d_tabs, sizeof(double) * std::max<int64_t>(2, P->tab_elems)));
-  LVC_CUDA(ctx, cudaMalloc(&P->d_piv, sizeof(PV) * std::max<int64_t>(4, P->piv_elems)));
-  LVC_CUDA(ctx, cudaMalloc(&P->d_out, sizeof(double) * std::max<int64_t>(1, P->nprices)));
-  LVC_CUDA(ctx, cudaMalloc(&P->d_rowstart, sizeof(int64_t) * (n + 1)));
-  LVC_CUDA(ctx, cudaMalloc(&P->d_items, sizeof(Item) * std::max<size_t>(1, P->items.size())));
-  if (P->gstate_elems > 0) LVC_CUDA(ctx, cudaMalloc(&P->d_gstate, sizeof(S) * P->gstate_elems));
-  LVC_CUDA(ctx, cudaMalloc(&P->d_err, sizeof(int)));
+  auto dalloc = [&](void** dst, size_t bytes) -> int {
+    if (P->pool) {
+      *dst = P->pool->alloc(bytes);
+      if (!*dst) return set_error(ctx, FUTHARK_OUT_OF_MEMORY, "device memory pool exhausted");
+      return 0;
+    }
+    LVC_CUDA(ctx, cudaMalloc(dst, bytes));
+    return 0;
+  };
+  if (int rc = dalloc((void**)&P->d_calibs, sizeof(CalibDev) * std::max(1, n))) return rc;
+  if (int rc = dalloc((void**)&P->d_tabs, sizeof(double) * std::max<int64_t>(2, P->tab_elems))) return rc;
+  if (int rc = dalloc(&P->d_piv, sizeof(PV) * std::max<int64_t>(4, P->piv_elems))) return rc;
+  if (int rc = dalloc((void**)&P->d_out, sizeof(double) * std::max<int64_t>(1, P->nprices))) return rc;
+  if (int rc = dalloc((void**)&P->d_rowstart, sizeof(int64_t) * (n + 1))) return rc;
+  if (int rc = dalloc((void**)&P->d_items, sizeof(Item) * std::max<size_t>(1, P->items.size()))) return rc;
+  if (P->gstate_elems > 0)
+    if (int rc = dalloc(&P->d_gstate, sizeof(S) * P->gstate_elems)) return rc;
+  if (int rc = dalloc((void**)&P->d_err, sizeof(int))) return rc;
   if (n > 0)
     LVC_CUDA(ctx, cudaMemcpyAsync(P->d_calibs, P->calibs.data(), sizeof(CalibDev) * n,
                                   cudaMemcpyHostToDevice, ctx->stream));
@@ -515,6 +620,7 @@ int plan_build(futhark_context* ctx, const lvc_calibration* cs, int n, lvc_plan*
   LVC_CUDA(ctx, cudaMemsetAsync(P->d_out, 0, sizeof(double) * std::max<int64_t>(1, P->nprices),
                                 ctx->stream));
   LVC_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if (!P->use_graph) return 0;
 
   // capture one run into a graph
   LVC_CUDA(ctx, cudaStreamBeginCapture(ctx->capture, cudaStreamCaptureModeThreadLocal));
@@ -532,7 +638,8 @@ int plan_build(futhark_context* ctx, const lvc_calibration* cs, int n, lvc_plan*
 }
 
 int plan_new_locked(futhark_context* ctx, const lvc_calibration* cs, int n, int precision,
-                    lvc_plan** out) {
+                    lvc_plan** out, DevicePool* pool = nullptr, bool use_graph = true,
+                    int max_sms = 0) {
   if (!ctx->ok) return set_error(ctx, FUTHARK_PROGRAM_ERROR, "context has no usable CUDA device");
   if (n < 0 || (n > 0 && !cs)) return set_error(ctx, FUTHARK_PROGRAM_ERROR, "bad calibration list");
   if (precision != LVC_F64 && precision != LVC_F32_STATE)
@@ -540,6 +647,9 @@ int plan_new_locked(futhark_context* ctx, const lvc_calibration* cs, int n, int 
   LVC_CUDA(ctx, cudaSetDevice(ctx->device));
   lvc_plan* P = new lvc_plan();
   P->precision = precision;
+  P->pool = pool;
+  P->use_graph = use_graph;
+  P->max_sms = max_sms;
   const int rc = precision == LVC_F64 ? plan_build<double, double>(ctx, cs, n, P)
                                       : plan_build<float, float>(ctx, cs, n, P);
   if (rc) {
@@ -548,6 +658,12 @@ int plan_new_locked(futhark_context* ctx, const lvc_calibration* cs, int n, int 
   }
   *out = P;
   return 0;
+}
+
+// One run of a plan on stream s: the captured graph when there is one.
+cudaError_t plan_launch(lvc_plan* P, cudaStream_t s) {
+  if (P->exec) return cudaGraphLaunch(P->exec, s);
+  return plan_enqueue(P, s, nullptr);
 }
 
 int check_device_error(futhark_context* ctx, lvc_plan* P) {
@@ -588,12 +704,13 @@ int entry_run(futhark_context* ctx, const lvc_calibration& c) {
     }
   }
   if (!P) {
-    if (int rc = plan_new_locked(ctx, &c, 1, LVC_F64, &P)) return rc;
+    if (!ctx->pool) ctx->pool = new DevicePool();
+    if (int rc = plan_new_locked(ctx, &c, 1, LVC_F64, &P, ctx->pool, /*use_graph=*/false)) return rc;
     ctx->entry_plan = P;
   } else if (int rc = set_params_locked(ctx, P, &c, 1)) {
     return rc;
   }
-  LVC_CUDA(ctx, cudaGraphLaunch(P->exec, ctx->stream));
+  LVC_CUDA(ctx, plan_launch(P, ctx->stream));
   return 0;
 }
 
@@ -683,6 +800,7 @@ void futhark_context_free(struct futhark_context* ctx) {
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
     plan_release(ctx->entry_plan);
+    delete ctx->pool;
     cudaStreamDestroy(ctx->stream);
     cudaStreamDestroy(ctx->capture);
   }
@@ -713,6 +831,8 @@ int futhark_context_clear_caches(struct futhark_context* ctx) {
   LVC_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   plan_release(ctx->entry_plan);
   ctx->entry_plan = nullptr;
+  delete ctx->pool;
+  ctx->pool = nullptr;
   return 0;
 }
 
@@ -871,7 +991,7 @@ int lvc_plan_set_params(struct futhark_context* ctx, struct lvc_plan* plan,
 int lvc_plan_run(struct futhark_context* ctx, struct lvc_plan* plan) {
   std::lock_guard<std::mutex> g(ctx->mu);
   LVC_CUDA(ctx, cudaSetDevice(ctx->device));
-  LVC_CUDA(ctx, cudaGraphLaunch(plan->exec, ctx->stream));
+  LVC_CUDA(ctx, plan_launch(plan, ctx->stream));
   return 0;
 }
 
@@ -903,7 +1023,7 @@ int lvc_plan_time(struct futhark_context* ctx, struct lvc_plan* plan, int32_t it
   LVC_CUDA(ctx, cudaEventCreate(&b));
   LVC_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   LVC_CUDA(ctx, cudaEventRecord(a, ctx->stream));
-  for (int i = 0; i < iters; i++) LVC_CUDA(ctx, cudaGraphLaunch(plan->exec, ctx->stream));
+  for (int i = 0; i < iters; i++) LVC_CUDA(ctx, plan_launch(plan, ctx->stream));
   LVC_CUDA(ctx, cudaEventRecord(b, ctx->stream));
   LVC_CUDA(ctx, cudaEventSynchronize(b));
   float ms = 0.f;
@@ -1159,3 +1279,417 @@ extern "C" int lvc_entry_main_f64_noalloc(struct futhark_context* ctx, double* p
   if (h) return set_error(ctx, FUTHARK_PROGRAM_ERROR, "rollback kernel rejected a work item");
   return 0;
 }
+
+// ---------------------------------------------------------------------------
+// Serving runtime: continuous batching of calibration requests.
+//
+// A scheduler thread owns a private context on the caller's device, a device
+// memory pool capped at the HBM budget, and a set of streams.  Pending
+// requests are admitted in FIFO order as batches whenever (a) a stream is
+// free, (b) the in-flight request count is below its cap and (c) the batch's
+// tables and pivots fit in what is left of the HBM budget.  A batch launches
+// one CTA (or cluster) per strike instance, each holding its grid in shared
+// memory for all its time steps; the block scheduler hands SMs -- i.e. their
+// shared memory -- to the waiting CTAs of all in-flight batches as running
+// instances finish, so requests that arrive while others are on the GPU start
+// as soon as memory and SMs free up and their work overlaps.  Each instance
+// runs the same kernels as every other entry point, so a price does not
+// depend on what ran beside it.
+// ---------------------------------------------------------------------------
+namespace {
+
+double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+struct SrvRequest {
+  uint64_t ticket = 0;
+  lvc_calibration c{};
+  double t_submit = 0, t_done = 0;
+  std::vector<double> prices;
+  int status = 0;  // 0 pending / running, 1 done, 2 failed
+  std::string error;
+};
+
+struct SrvBatch {
+  std::vector<SrvRequest*> reqs;
+  lvc_plan* plan = nullptr;
+  int stream = -1;
+  cudaEvent_t done = nullptr;
+  double sms = 0;
+  double t_launch = 0;
+};
+
+}  // namespace
+
+struct lvc_server {
+  futhark_context* user_ctx = nullptr;
+  futhark_context sctx;  // private context: device properties, upload stream, errors
+  lvc_server_config cfg{};
+  DevicePool pool;
+  std::vector<cudaStream_t> streams;
+  std::vector<bool> stream_busy;
+  std::vector<double*> pinned;  // per stream: staging for prices and the error flag
+  std::vector<int64_t> pinned_cap;
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done;
+  std::deque<SrvRequest*> pending;
+  std::unordered_map<uint64_t, SrvRequest*> requests;
+  std::vector<SrvBatch*> inflight;
+  uint64_t next_ticket = 1;
+  int inflight_requests = 0;
+  double sms_in_use = 0;
+  bool stop = false;
+  std::thread worker;
+  // statistics
+  std::vector<double> latencies;
+  int64_t submitted = 0, completed = 0, failed = 0, options = 0, batches = 0;
+  double t_first = 0, t_last = 0;
+};
+
+namespace {
+
+void server_retire(lvc_server* S) {
+  for (auto it = S->inflight.begin(); it != S->inflight.end();) {
+    SrvBatch* b = *it;
+    const cudaError_t q = cudaEventQuery(b->done);
+    if (q == cudaErrorNotReady) {
+      ++it;
+      continue;
+    }
+    const double t = now_s();
+    double* host = S->pinned[b->stream];
+    const int64_t np = b->plan->nprices;
+    const int derr = q == cudaSuccess ? reinterpret_cast<const int*>(host + np)[0] : 1;
+    int64_t off = 0;
+    for (SrvRequest* r : b->reqs) {
+      r->t_done = t;
+      if (q != cudaSuccess || derr) {
+        r->status = 2;
+        r->error = q != cudaSuccess ? std::string("CUDA error: ") + cudaGetErrorString(q)
+                                    : "rollback kernel rejected a work item";
+        S->failed++;
+      } else {
+        r->prices.assign(host + off, host + off + r->c.outer);
+        r->status = 1;
+        S->completed++;
+        S->options += r->c.outer;
+        S->latencies.push_back(t - r->t_submit);
+        S->t_last = t;
+      }
+      off += r->c.outer;
+    }
+    S->inflight_requests -= (int)b->reqs.size();
+    S->sms_in_use -= b->sms;
+    if (S->sms_in_use < 1e-9) S->sms_in_use = 0;
+    S->stream_busy[b->stream] = false;
+    cudaEventDestroy(b->done);
+    plan_release(b->plan);
+    delete b;
+    it = S->inflight.erase(it);
+  }
+}
+
+// Device bytes a one-calibration plan takes (tables, pivots, work list,
+// prices, state scratch), from the same layouts the plan builder uses.
+size_t request_bytes(const lvc_calibration& c, int precision, int max_smem) {
+  const bool f64 = precision == LVC_F64;
+  const Config cf = f64 ? choose_config<double>(c.numX, c.numY, max_smem)
+                        : choose_config<float>(c.numX, c.numY, max_smem);
+  const int Xp = std::max(8, pow2ceil(c.numX));
+  const size_t ps = f64 ? 8 : 4;
+  size_t b = 8 * (size_t)al2(tab_layout(c.numX, c.numY, c.numT, Xp, cf.kind).total);
+  b += ps * (size_t)(piv_elems(c.numX, c.numY, c.numT, Xp, cf.kind) + 4);
+  b += 16 * (size_t)c.outer + 4096;
+  if (cf.gstate) b += ps * (size_t)cf.grid_elems * 148 * 4;
+  return b + 8 * 256;  // allocation rounding
+}
+
+// Admits one batch from the front of the queue; returns false when nothing
+// could be admitted.  Called with S->mu held; releases it while building.
+bool server_admit(lvc_server* S, std::unique_lock<std::mutex>& lk) {
+  if (S->pending.empty()) return false;
+  int si = -1;
+  for (size_t i = 0; i < S->streams.size(); i++)
+    if (!S->stream_busy[i]) {
+      si = (int)i;
+      break;
+    }
+  if (si < 0) return false;
+  std::vector<SrvRequest*> take;
+  size_t bytes = 0;
+  const size_t free_bytes = S->pool.budget > S->pool.in_use ? S->pool.budget - S->pool.in_use : 0;
+  while (!S->pending.empty() && (int)take.size() < S->cfg.max_batch_requests &&
+         S->inflight_requests + (int)take.size() < S->cfg.max_inflight_requests) {
+    SrvRequest* r = S->pending.front();
+    const size_t rb = request_bytes(r->c, S->cfg.precision, S->sctx.max_smem);
+    if (rb > S->pool.budget) {  // can never fit: fail it now
+      S->pending.pop_front();
+      r->status = 2;
+      r->error = "request needs more device memory than the server's HBM budget";
+      r->t_done = now_s();
+      S->failed++;
+      S->cv_done.notify_all();
+      continue;
+    }
+    if (bytes + rb > free_bytes) break;
+    take.push_back(r);
+    bytes += rb;
+    S->pending.pop_front();
+  }
+  if (take.empty()) return false;
+  std::vector<lvc_calibration> cs;
+  for (SrvRequest* r : take) cs.push_back(r->c);
+  S->stream_busy[si] = true;
+  lk.unlock();
+  lvc_plan* P = nullptr;
+  int rc = plan_new_locked(&S->sctx, cs.data(), (int)cs.size(), S->cfg.precision, &P, &S->pool,
+                           /*use_graph=*/false, /*max_sms=*/-1);
+  cudaError_t e = cudaSuccess;
+  SrvBatch* b = nullptr;
+  if (!rc) {
+    b = new SrvBatch();
+    b->reqs = take;
+    b->plan = P;
+    b->stream = si;
+    b->sms = P->sms;
+    b->t_launch = now_s();
+    cudaStream_t st = S->streams[si];
+    if (S->pinned_cap[si] < P->nprices + 1) {
+      if (S->pinned[si]) cudaFreeHost(S->pinned[si]);
+      S->pinned_cap[si] = std::max<int64_t>(P->nprices + 1, 4096);
+      e = cudaMallocHost((void**)&S->pinned[si], sizeof(double) * S->pinned_cap[si]);
+    }
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = plan_enqueue(P, st, nullptr);
+    if (e == cudaSuccess && P->nprices > 0)
+      e = cudaMemcpyAsync(S->pinned[si], P->d_out, sizeof(double) * P->nprices, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) {
+      // the kernels' error flag, in the slot after the prices
+      int* flag = reinterpret_cast<int*>(S->pinned[si] + P->nprices);
+      e = cudaMemcpyAsync(flag, P->d_err, sizeof(int), cudaMemcpyDeviceToHost, st);
+    }
+    if (e == cudaSuccess) e = cudaEventRecord(b->done, st);
+  }
+  lk.lock();
+  if (rc == FUTHARK_OUT_OF_MEMORY && (!S->inflight.empty() || take.size() > 1)) {
+    // the budget is taken by running batches (or fragmented): retry with
+    // fewer requests, or when running batches complete
+    if (P) plan_release(P);
+    if (S->inflight.empty()) {
+      for (size_t i = take.size(); i-- > 1;) S->pending.push_front(take[i]);
+      S->pending.push_front(take[0]);
+      S->stream_busy[si] = false;
+      S->cfg.max_batch_requests = std::max<int32_t>(1, (int32_t)take.size() / 2);
+      return true;  // try again at once with the smaller batch size
+    }
+    for (auto it = take.rbegin(); it != take.rend(); ++it) S->pending.push_front(*it);
+    S->stream_busy[si] = false;
+    return false;
+  }
+  if (rc || e != cudaSuccess) {
+    const std::string msg = rc ? S->sctx.error : std::string("CUDA error: ") + cudaGetErrorString(e);
+    for (SrvRequest* r : take) {
+      r->status = 2;
+      r->error = msg;
+      r->t_done = now_s();
+      S->failed++;
+    }
+    if (b) {
+      if (b->done) cudaEventDestroy(b->done);
+      plan_release(b->plan);
+      delete b;
+    } else if (P) {
+      plan_release(P);
+    }
+    S->stream_busy[si] = false;
+    S->cv_done.notify_all();
+    return true;
+  }
+  S->inflight.push_back(b);
+  S->inflight_requests += (int)take.size();
+  S->sms_in_use += b->sms;
+  S->batches++;
+  return true;
+}
+
+void server_loop(lvc_server* S) {
+  cudaSetDevice(S->sctx.device);
+  std::unique_lock<std::mutex> lk(S->mu);
+  while (true) {
+    const size_t before = S->inflight.size();
+    server_retire(S);
+    if (S->inflight.size() != before) S->cv_done.notify_all();
+    while (server_admit(S, lk)) {
+    }
+    if (S->stop && S->pending.empty() && S->inflight.empty()) break;
+    if (S->inflight.empty()) {
+      S->cv_work.wait(lk, [&] { return S->stop || !S->pending.empty(); });
+    } else {
+      S->cv_work.wait_for(lk, std::chrono::microseconds(20));
+    }
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int lvc_server_new(struct futhark_context* ctx, const struct lvc_server_config* cfg,
+                   struct lvc_server** out) {
+  std::lock_guard<std::mutex> g(ctx->mu);
+  if (!ctx->ok) return set_error(ctx, FUTHARK_PROGRAM_ERROR, "context has no usable CUDA device");
+  lvc_server_config c = cfg ? *cfg : lvc_server_config{};
+  if (c.precision != LVC_F64 && c.precision != LVC_F32_STATE)
+    return set_error(ctx, FUTHARK_PROGRAM_ERROR, "unknown precision");
+  if (c.max_inflight_requests <= 0) c.max_inflight_requests = 256;
+  if (c.max_batch_requests <= 0) c.max_batch_requests = 64;
+  if (c.num_streams <= 0) c.num_streams = 8;
+  if (c.hbm_budget_bytes <= 0) c.hbm_budget_bytes = int64_t(8) << 30;
+  LVC_CUDA(ctx, cudaSetDevice(ctx->device));
+  lvc_server* S = new lvc_server();
+  S->user_ctx = ctx;
+  S->cfg = c;
+  S->sctx.device = ctx->device;
+  S->sctx.num_sms = ctx->num_sms;
+  S->sctx.max_smem = ctx->max_smem;
+  S->sctx.ok = true;
+  S->pool.budget = (size_t)c.hbm_budget_bytes;
+  cudaError_t e = cudaStreamCreateWithFlags(&S->sctx.stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&S->sctx.capture, cudaStreamNonBlocking);
+  for (int i = 0; i < c.num_streams && e == cudaSuccess; i++) {
+    cudaStream_t st;
+    e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    if (e == cudaSuccess) {
+      S->streams.push_back(st);
+      S->stream_busy.push_back(false);
+      S->pinned.push_back(nullptr);
+      S->pinned_cap.push_back(0);
+    }
+  }
+  // reserve the whole budget up front: serving never reaches cudaMalloc
+  if (e == cudaSuccess && !S->pool.grow((size_t)c.hbm_budget_bytes)) e = cudaErrorMemoryAllocation;
+  if (e != cudaSuccess) {
+    for (cudaStream_t st : S->streams) cudaStreamDestroy(st);
+    if (S->sctx.stream) cudaStreamDestroy(S->sctx.stream);
+    if (S->sctx.capture) cudaStreamDestroy(S->sctx.capture);
+    delete S;
+    return cuda_fail(ctx, e, "lvc_server_new");
+  }
+  S->worker = std::thread(server_loop, S);
+  *out = S;
+  return 0;
+}
+
+int lvc_server_submit(struct lvc_server* S, const struct lvc_calibration* c, uint64_t* ticket) {
+  {
+    std::lock_guard<std::mutex> g(S->user_ctx->mu);
+    if (int rc = validate(S->user_ctx, *c, 0)) return rc;
+  }
+  SrvRequest* r = new SrvRequest();
+  r->c = *c;
+  r->t_submit = now_s();
+  {
+    std::lock_guard<std::mutex> g(S->mu);
+    r->ticket = S->next_ticket++;
+    S->requests[r->ticket] = r;
+    S->pending.push_back(r);
+    S->submitted++;
+    if (S->t_first == 0) S->t_first = r->t_submit;
+  }
+  S->cv_work.notify_one();
+  *ticket = r->ticket;
+  return 0;
+}
+
+int lvc_server_poll(struct lvc_server* S, uint64_t ticket, int32_t* done) {
+  std::lock_guard<std::mutex> g(S->mu);
+  auto it = S->requests.find(ticket);
+  if (it == S->requests.end()) return FUTHARK_PROGRAM_ERROR;
+  *done = it->second->status != 0;
+  return 0;
+}
+
+int lvc_server_wait(struct lvc_server* S, uint64_t ticket, double* prices, double timeout_s) {
+  std::unique_lock<std::mutex> lk(S->mu);
+  auto it = S->requests.find(ticket);
+  if (it == S->requests.end()) {
+    std::lock_guard<std::mutex> g(S->user_ctx->mu);
+    return set_error(S->user_ctx, FUTHARK_PROGRAM_ERROR, "unknown ticket");
+  }
+  SrvRequest* r = it->second;
+  const auto deadline = std::chrono::steady_clock::now() +
+                        std::chrono::duration<double>(timeout_s > 0 ? timeout_s : 1e9);
+  if (!S->cv_done.wait_until(lk, deadline, [&] { return r->status != 0; })) {
+    std::lock_guard<std::mutex> g(S->user_ctx->mu);
+    return set_error(S->user_ctx, FUTHARK_PROGRAM_ERROR, "timed out waiting for the request");
+  }
+  S->requests.erase(it);
+  const int status = r->status;
+  const std::string err = r->error;
+  if (status == 1 && prices && !r->prices.empty())
+    memcpy(prices, r->prices.data(), sizeof(double) * r->prices.size());
+  delete r;
+  lk.unlock();
+  if (status != 1) {
+    std::lock_guard<std::mutex> g(S->user_ctx->mu);
+    return set_error(S->user_ctx, FUTHARK_PROGRAM_ERROR, err);
+  }
+  return 0;
+}
+
+int lvc_server_stats(struct lvc_server* S, struct lvc_server_stats* st) {
+  std::lock_guard<std::mutex> g(S->mu);
+  memset(st, 0, sizeof *st);
+  st->submitted = S->submitted;
+  st->completed = S->completed;
+  st->failed = S->failed;
+  st->options = S->options;
+  st->batches = S->batches;
+  st->span_s = S->t_last > S->t_first ? S->t_last - S->t_first : 0.0;
+  st->throughput_options_per_s = st->span_s > 0 ? S->options / st->span_s : 0.0;
+  if (!S->latencies.empty()) {
+    std::vector<double> v = S->latencies;
+    std::sort(v.begin(), v.end());
+    auto pct = [&](double p) { return 1e3 * v[std::min(v.size() - 1, (size_t)(p * (v.size() - 1) + 0.5))]; };
+    st->p50_ms = pct(0.50);
+    st->p99_ms = pct(0.99);
+    st->max_ms = 1e3 * v.back();
+    double sum = 0;
+    for (double x : v) sum += x;
+    st->mean_ms = 1e3 * sum / v.size();
+  }
+  st->hbm_reserved_bytes = (int64_t)S->pool.reserved;
+  return 0;
+}
+
+int lvc_server_reset_stats(struct lvc_server* S) {
+  std::lock_guard<std::mutex> g(S->mu);
+  S->latencies.clear();
+  S->submitted = S->completed = S->failed = S->options = S->batches = 0;
+  S->t_first = S->t_last = 0;
+  return 0;
+}
+
+int lvc_server_free(struct lvc_server* S) {
+  if (!S) return 0;
+  {
+    std::lock_guard<std::mutex> g(S->mu);
+    S->stop = true;
+  }
+  S->cv_work.notify_all();
+  if (S->worker.joinable()) S->worker.join();
+  cudaSetDevice(S->sctx.device);
+  for (auto& kv : S->requests) delete kv.second;
+  for (size_t i = 0; i < S->streams.size(); i++) {
+    cudaStreamSynchronize(S->streams[i]);
+    cudaStreamDestroy(S->streams[i]);
+    if (S->pinned[i]) cudaFreeHost(S->pinned[i]);
+  }
+  cudaStreamDestroy(S->sctx.stream);
+  cudaStreamDestroy(S->sctx.capture);
+  delete S;
+  return 0;
+}
+
+}  // extern "C"

@@ -179,6 +179,44 @@ LVC_API int lvc_entry_main_f64_noalloc(struct futhark_context *ctx, double *pric
                                        const double t, const double alpha, const double nu,
                                        const double beta);
 
+/*
+ * Serving runtime: continuous batching of calibration requests.  A
+ * scheduler thread admits queued requests in arrival order as batches while
+ * a stream is free, the in-flight request cap is not reached and the batch's
+ * tables and pivots fit in what is left of the HBM budget (reserved once at
+ * creation).  Batches run concurrently on their own streams with one CTA (or
+ * cluster) per strike instance, so SMs pass to waiting instances of any
+ * in-flight batch as running ones finish.  Latency is measured from submit to
+ * the completion of the request's batch.
+ */
+struct lvc_server;
+struct lvc_server_config {
+  int32_t precision;              /* LVC_F64 or LVC_F32_STATE */
+  int32_t max_inflight_requests;  /* 0: 256 */
+  int32_t max_batch_requests;     /* 0: 64 */
+  int32_t num_streams;            /* 0: 8 */
+  int64_t hbm_budget_bytes;       /* 0: 8 GiB */
+};
+struct lvc_server_stats {
+  int64_t submitted, completed, failed, options, batches, hbm_reserved_bytes;
+  double p50_ms, p99_ms, mean_ms, max_ms, throughput_options_per_s, span_s;
+};
+LVC_API int lvc_server_new(struct futhark_context *ctx, const struct lvc_server_config *cfg,
+                           struct lvc_server **server);
+/* Thread-safe; invalid calibrations are rejected here with the entry
+ * points' errors. */
+LVC_API int lvc_server_submit(struct lvc_server *server, const struct lvc_calibration *calib,
+                              uint64_t *ticket);
+LVC_API int lvc_server_poll(struct lvc_server *server, uint64_t ticket, int32_t *done);
+/* Blocks until the request is done (timeout_s <= 0: no limit), copies its
+ * `outer` prices and releases the ticket. */
+LVC_API int lvc_server_wait(struct lvc_server *server, uint64_t ticket, double *prices,
+                            double timeout_s);
+LVC_API int lvc_server_stats(struct lvc_server *server, struct lvc_server_stats *stats);
+LVC_API int lvc_server_reset_stats(struct lvc_server *server);
+/* Finishes the queued and running requests, then releases everything. */
+LVC_API int lvc_server_free(struct lvc_server *server);
+
 /* Peak probes of the context's device: FP64 FMA throughput (TFLOP/s, 2 flops
  * per FMA, every SM busy) and shared-memory load bandwidth (GB/s summed over
  * SMs), each the best of three timed microbenchmark launches.  These are the
