@@ -43,7 +43,7 @@ UNIT = "options/s"
 # implicit-X coefficients 12, tridiagonal X 10, combine 3, implicit-Y
 # coefficients 12, tridiagonal Y 10.
 F_ALG = 77
-CALIB_DEV_BYTES = 96  # sizeof(lvc::CalibDev), uploaded per calibration per step
+CALIB_DEV_BYTES = 112  # sizeof(lvc::CalibDev) (static_assert in lvc_layout.h), uploaded per calibration per step
 
 
 def parse():

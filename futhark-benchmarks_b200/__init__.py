@@ -69,6 +69,29 @@ class Calibration:
         return self.outer * self.numX * self.numY * max(self.numT - 1, 0)
 
 
+class Shape(ctypes.Structure):
+    """struct lvc_shape: kernel family x cluster size of a grid class."""
+    _fields_ = [("family", ctypes.c_int32), ("cluster", ctypes.c_int32), ("threads", ctypes.c_int32),
+                ("rows_per_cta", ctypes.c_int32), ("smem_bytes", ctypes.c_int32), ("hbm_state", ctypes.c_int32)]
+
+    FAMILIES = {0: "chunk", 1: "line", 2: "line_full"}
+
+    def __repr__(self):
+        fam = self.FAMILIES.get(self.family, "?") + ("_hbm" if self.hbm_state else "")
+        return (f"Shape({fam}, cluster={self.cluster}, threads={self.threads}, "
+                f"rows_per_cta={self.rows_per_cta}, smem={self.smem_bytes})")
+
+    def key(self):
+        return (self.family, self.cluster, self.hbm_state)
+
+
+class TuningEntry(ctypes.Structure):
+    """struct lvc_tuning_entry."""
+    _fields_ = [("numX", ctypes.c_int32), ("numY", ctypes.c_int32), ("precision", ctypes.c_int32),
+                ("tuned", ctypes.c_int32), ("shape", Shape), ("us_per_step_default", ctypes.c_double),
+                ("us_per_step_best", ctypes.c_double)]
+
+
 class _ServerConfig(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int32), ("max_inflight_requests", ctypes.c_int32),
                 ("max_batch_requests", ctypes.c_int32), ("num_streams", ctypes.c_int32),
@@ -100,6 +123,18 @@ def load_library(path: str = LIB_PATH):
         "futhark_context_config_set_profiling": (None, [vp, ctypes.c_int]),
         "futhark_context_config_set_logging": (None, [vp, ctypes.c_int]),
         "futhark_context_config_set_cache_file": (None, [vp, ctypes.c_char_p]),
+        "futhark_context_config_set_tuning_param": (ctypes.c_int, [vp, ctypes.c_char_p, ctypes.c_size_t]),
+        "futhark_get_tuning_param_count": (ctypes.c_int, []),
+        "futhark_get_tuning_param_name": (ctypes.c_char_p, [ctypes.c_int]),
+        "futhark_get_tuning_param_class": (ctypes.c_char_p, [ctypes.c_int]),
+        "lvc_context_set_tuning_param": (ctypes.c_int, [vp, ctypes.c_char_p, ctypes.c_size_t]),
+        "lvc_shape_candidates": (ctypes.c_int, [vp, i32, i32, i32, ctypes.POINTER(Shape), i32, ctypes.POINTER(i32)]),
+        "lvc_tuning_set": (ctypes.c_int, [vp, i32, i32, i32, ctypes.POINTER(Shape)]),
+        "lvc_tuning_get": (ctypes.c_int, [vp, i32, i32, i32, ctypes.POINTER(TuningEntry)]),
+        "lvc_tuning_entries": (i32, [vp, ctypes.POINTER(TuningEntry), i32]),
+        "lvc_autotune": (ctypes.c_int, [vp, ctypes.POINTER(_Calib), i32, i32, i32]),
+        "lvc_tuning_save": (ctypes.c_int, [vp, ctypes.c_char_p]),
+        "lvc_tuning_load": (ctypes.c_int, [vp, ctypes.c_char_p]),
         "futhark_context_new": (vp, [vp]),
         "futhark_context_free": (None, [vp]),
         "futhark_context_sync": (ctypes.c_int, [vp]),
@@ -157,11 +192,16 @@ def _calib_array(calibs: Sequence[Calibration]):
 class Context:
     """A futhark_context on one CUDA device ("#N" or a device-name substring)."""
 
-    def __init__(self, device: str | None = None):
+    def __init__(self, device: str | None = None, tuning: dict | None = None):
         self.lib = load_library()
         self._cfg = self.lib.futhark_context_config_new()
         if device is not None:
             self.lib.futhark_context_config_set_device(self._cfg, device.encode())
+        for name, value in (tuning or {}).items():
+            if self.lib.futhark_context_config_set_tuning_param(self._cfg, name.encode(), int(value)):
+                self.lib.futhark_context_config_free(self._cfg)
+                self._cfg = None
+                raise FutharkError(FUTHARK_PROGRAM_ERROR, f"unknown tuning parameter or value: {name}={value}")
         self._ctx = self.lib.futhark_context_new(self._cfg)
         if not self._ctx:
             raise FutharkError(FUTHARK_OUT_OF_MEMORY, "futhark_context_new failed")
@@ -205,6 +245,47 @@ class Context:
 
     def sync(self):
         self._check(self.lib.futhark_context_sync(self._ctx))
+
+    def set_tuning_param(self, name: str, value: int):
+        """Tuning parameter for plans created from now on ("lvc.streams", "lvc.grid")."""
+        self._check(self.lib.lvc_context_set_tuning_param(self._ctx, name.encode(), int(value)))
+
+    # -- shape autotuner ------------------------------------------------------
+    def shape_candidates(self, numX: int, numY: int, precision: int = F64) -> list:
+        """Every Shape that can run an numX x numY grid on this device."""
+        n = ctypes.c_int32()
+        self._check(self.lib.lvc_shape_candidates(self._ctx, numX, numY, precision, None, 0, ctypes.byref(n)))
+        arr = (Shape * max(1, n.value))()
+        self._check(self.lib.lvc_shape_candidates(self._ctx, numX, numY, precision, arr, n.value, ctypes.byref(n)))
+        return list(arr[:n.value])
+
+    def tuning_set(self, numX: int, numY: int, precision: int = F64, shape: Shape | None = None):
+        """Pin a shape for a grid class (None: back to the built-in choice)."""
+        self._check(self.lib.lvc_tuning_set(self._ctx, numX, numY, precision,
+                                            ctypes.byref(shape) if shape is not None else None))
+
+    def tuning_get(self, numX: int, numY: int, precision: int = F64) -> TuningEntry:
+        e = TuningEntry()
+        self._check(self.lib.lvc_tuning_get(self._ctx, numX, numY, precision, ctypes.byref(e)))
+        return e
+
+    def tuning_entries(self) -> list:
+        n = self.lib.lvc_tuning_entries(self._ctx, None, 0)
+        arr = (TuningEntry * max(1, n))()
+        n = self.lib.lvc_tuning_entries(self._ctx, arr, n)
+        return list(arr[:n])
+
+    def autotune(self, calibs: Sequence[Calibration], precision: int = F64, probe_steps: int = 8) -> list:
+        """Time every candidate shape of every grid class of `calibs`; keep the fastest."""
+        arr = _calib_array(calibs)
+        self._check(self.lib.lvc_autotune(self._ctx, arr, len(calibs), precision, probe_steps))
+        return self.tuning_entries()
+
+    def tuning_save(self, path: str):
+        self._check(self.lib.lvc_tuning_save(self._ctx, str(path).encode()))
+
+    def tuning_load(self, path: str):
+        self._check(self.lib.lvc_tuning_load(self._ctx, str(path).encode()))
 
     @property
     def stream(self) -> int:

@@ -39,6 +39,7 @@ struct CalibDev {
   int64_t piv;  // offset (elements) of the X-direction pivots in the pivot arena
   int64_t out;  // index of this calibration's first price in the output vector
 };
+static_assert(sizeof(CalibDev) == 112, "bench.py counts 112 uploaded bytes per calibration");
 
 LVC_HD int64_t al2(int64_t n) { return (n + 1) & ~int64_t(1); }
 

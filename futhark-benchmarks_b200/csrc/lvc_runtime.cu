@@ -9,8 +9,9 @@
 //     classes by kernel configuration (threads per CTA, lane chunk width,
 //     cluster size, on-chip or HBM grid) and sorted by descending work
 //     (longest-processing-time first) inside a class;
-//   * one run = setup kernel + pivot kernel + one persistent rollback launch
-//     per class, captured once into a CUDA graph.
+//   * one run = setup kernel + pivot kernel + one rollback launch per class,
+//     the classes forked over several streams (largest class first) so their
+//     tails overlap, captured once into a CUDA graph.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -36,10 +37,43 @@
 
 using namespace lvc;
 
+// Tuning parameters, set by name as in Futhark's generated API
+// (futhark_context_config_set_tuning_param) or on a live context.
+//   lvc.streams  streams a batch plan forks its launch classes over (1..8)
+//   lvc.grid     0: persistent grids sized to the resident CTAs, items taken
+//                in strides; 1: one CTA (cluster) per strike instance, the
+//                block scheduler handing out items in descending work order
+struct TuningParams {
+  int streams = 4;
+  int grid = 0;
+};
+const char* const kTuningNames[] = {"lvc.streams", "lvc.grid"};
+const char* const kTuningClasses[] = {"streams", "grid"};
+constexpr int kNumTuning = 2;
+constexpr int kMaxNumX = 512;   // largest grid the kernels take
+constexpr int kMaxNumY = 1024;
+constexpr int kMaxAux = 8;
+
+int set_tuning(TuningParams& t, const char* name, size_t v) {
+  if (!name) return 1;
+  if (!strcmp(name, "lvc.streams")) {
+    if (v < 1 || v > (size_t)kMaxAux) return 1;
+    t.streams = (int)v;
+    return 0;
+  }
+  if (!strcmp(name, "lvc.grid")) {
+    if (v > 1) return 1;
+    t.grid = (int)v;
+    return 0;
+  }
+  return 1;
+}
+
 struct futhark_context_config {
   int device = 0;
   std::string device_name;
   int debugging = 0, profiling = 0, logging = 0;
+  TuningParams tuning;
 };
 
 struct futhark_f32_1d {
@@ -134,6 +168,23 @@ struct DevicePool {
   }
 };
 
+// Kernel configuration of one calibration.
+struct Config {
+  int kind, NT, KX, C;
+  bool gstate;
+  bool full = false;
+  int Ycs;
+  size_t smem_bytes;
+  int64_t grid_elems;
+};
+
+// A tuned grid class: the configuration chosen for (numX, numY, precision).
+struct TunedShape {
+  Config cf;
+  bool tuned = false;
+  double us_default = 0.0, us_best = 0.0;
+};
+
 struct Launch {
   int kind, NT, KX, C;
   bool gstate;
@@ -171,8 +222,12 @@ struct lvc_plan {
   double rollback_ms = 0.0;
   DevicePool* pool = nullptr;  // where the buffers come from (null: cudaMalloc)
   bool use_graph = true;       // capture one run into a CUDA graph
-  int max_sms = 0;             // cap on the SMs a launch may occupy (0: all)
+  int max_sms = 0;             // cap on the SMs a launch may occupy (0: all, <0: one CTA per item)
   double sms = 0.0;            // SMs the widest launch occupies
+  int n_streams = 1;           // streams the launch classes fork over
+  cudaStream_t aux[kMaxAux] = {};
+  cudaEvent_t ev_fork = nullptr;
+  cudaEvent_t ev_join[kMaxAux] = {};
 };
 
 struct futhark_context {
@@ -186,6 +241,9 @@ struct futhark_context {
   bool ok = false;
   lvc_plan* entry_plan = nullptr;  // reused by the entry points while sizes repeat
   DevicePool* pool = nullptr;      // buffers of the entry points' plans
+  TuningParams tuning;
+  cudaStream_t aux[kMaxAux] = {};  // fork streams of the batch plans
+  std::map<std::tuple<int, int, int>, TunedShape> shapes;  // (numX, numY, precision) -> tuned shape
 };
 
 namespace {
@@ -234,7 +292,7 @@ int validate(futhark_context* ctx, const lvc_calibration& c, int idx) {
              idx, c.outer, c.numX, c.numY, c.numT);
     return set_error(ctx, FUTHARK_PROGRAM_ERROR, buf);
   }
-  if (c.numX > 512 || c.numY > 1024) {
+  if (c.numX > kMaxNumX || c.numY > kMaxNumY) {
     snprintf(buf, sizeof buf,
              "calibration %d: numX=%d numY=%d beyond the engine's limits (numX <= 512, "
              "numY <= 1024)",
@@ -290,92 +348,131 @@ RbFn<S, PV> rollback_fn(int kind, int NT, int KX, bool gs, bool full = false) {
 template <typename S>
 int state_size() { return (int)sizeof(S); }
 
-// Kernel configuration of one calibration.
-struct Config {
-  int kind, NT, KX, C;
-  bool gstate;
-  bool full = false;
-  int Ycs;
-  size_t smem_bytes;
-  int64_t grid_elems;
-};
 
-// Line family: one lane per grid line; needs numX <= 256 and at most 16
-// warps of units per CTA, which fixes the cluster size.
+// Line family, full tiles: every line chunk, row group and CTA block
+// complete; two units per warp, one unit per 512 cells.
 template <typename S>
-bool choose_line(int X, int Y, int max_smem, Config& cf) {
-  if (X > 256) return false;
-  for (int C = 1; C <= kMaxCluster; C *= 2) {
-    // full tiles: every line chunk, row group and CTA block complete; two
-    // units per warp, one unit per 512 cells
-    if (X % 32 == 0 && Y % C == 0 && (Y / C) % 32 == 0) {
-      const int Ycs = Y / C;
-      const int units = X * Ycs / 512;
-      const FullLayout F = full_layout<S>(X, Ycs, units);
-      if (units >= 2 && units <= 16 && F.Ux == units && F.Uy == units && F.total <= max_smem) {
-        cf.kind = kKindLine;
-        cf.full = true;
-        cf.NT = 16 * units;  // 32 lanes x units / 2 units per warp
-        cf.KX = kLineK;
-        cf.C = C;
-        cf.gstate = false;
-        cf.Ycs = Ycs;
-        cf.smem_bytes = (size_t)F.total;
-        cf.grid_elems = 0;
-        return true;
-      }
-    }
-    // rows per CTA: a multiple of 4 when split, so every CTA's bulk copies
-    // start on a 16-byte boundary
-    const int Ycs = C == 1 ? Y : (int)round4(ceil_div(Y, C));
-    if (C > 1 && (C - 1) * Ycs >= Y) break;
-    const LineLayout L16 = line_layout<S>(X, Ycs, 16);
-    if (L16.Ux > 16 || L16.Uy > 16) continue;
-    const int NT = std::max(64, 32 * pow2ceil(std::max(L16.Ux, L16.Uy)));
-    const LineLayout L = line_layout<S>(X, Ycs, NT / 32);
-    if (L.total > max_smem) continue;
-    cf.kind = kKindLine;
-    cf.full = false;
-    cf.NT = NT;
-    cf.KX = kLineK;
-    cf.C = C;
-    cf.gstate = false;
-    cf.Ycs = Ycs;
-    cf.smem_bytes = (size_t)L.total;
-    cf.grid_elems = 0;
-    return true;
-  }
-  return false;
+bool line_full_cfg(int X, int Y, int C, int max_smem, Config& cf) {
+  if (X > 256 || X % 32 || Y % C || (Y / C) % 32) return false;
+  const int Ycs = Y / C;
+  const int units = X * Ycs / 512;
+  if (units != 2 && units != 4 && units != 8 && units != 16) return false;  // NT = 16 * units instantiated
+  const FullLayout F = full_layout<S>(X, Ycs, units);
+  if (F.Ux != units || F.Uy != units || F.total > max_smem) return false;
+  cf.kind = kKindLine;
+  cf.full = true;
+  cf.NT = 16 * units;  // 32 lanes x units / 2 units per warp
+  cf.KX = kLineK;
+  cf.C = C;
+  cf.gstate = false;
+  cf.Ycs = Ycs;
+  cf.smem_bytes = (size_t)F.total;
+  cf.grid_elems = 0;
+  return true;
 }
 
+// Line family, any sizes: one lane per grid line; needs numX <= 256 and at
+// most 16 warps of units per CTA.  Rows per CTA are a multiple of 4 when
+// split, so every CTA's bulk copies start on a 16-byte boundary.
 template <typename S>
-Config choose_config(int X, int Y, int max_smem) {
-  Config cf;
-  if (choose_line<S>(X, Y, max_smem, cf)) return cf;
-  cf.kind = kKindChunk;
+bool line_generic_cfg(int X, int Y, int C, int max_smem, Config& cf) {
+  if (X > 256) return false;
+  const int Ycs = C == 1 ? Y : (int)round4(ceil_div(Y, C));
+  if (C > 1 && (C - 1) * Ycs >= Y) return false;  // a CTA would own no row
+  const LineLayout L16 = line_layout<S>(X, Ycs, 16);
+  if (L16.Ux > 16 || L16.Uy > 16) return false;
+  const int NT = std::max(64, 32 * pow2ceil(std::max(L16.Ux, L16.Uy)));
+  const LineLayout L = line_layout<S>(X, Ycs, NT / 32);
+  if (L.total > max_smem) return false;
+  cf.kind = kKindLine;
+  cf.full = false;
+  cf.NT = NT;
+  cf.KX = kLineK;
+  cf.C = C;
+  cf.gstate = false;
+  cf.Ycs = Ycs;
+  cf.smem_bytes = (size_t)L.total;
+  cf.grid_elems = 0;
+  return true;
+}
+
+// Chunk family: any numX up to 512; the grid on chip over C CTAs, or (gstate)
+// in HBM scratch when nothing fits.
+template <typename S>
+bool chunk_cfg(int X, int Y, int C, int max_smem, bool gstate, Config& cf) {
   const int Xp = std::max(8, pow2ceil(X));
+  const int Ycs = ceil_div(Y, C);
+  if (C > 1 && (C - 1) * Ycs >= Y) return false;
+  const SmemLayout L = smem_layout<S>(Xp, X, Ycs, !gstate);
+  if ((size_t)L.total * sizeof(S) > (size_t)max_smem) return false;
+  cf.kind = kKindChunk;
+  cf.full = false;
   cf.KX = Xp <= 256 ? 8 : 16;
-  cf.gstate = true;
-  cf.C = 1;
-  cf.Ycs = Y;
-  for (int C = 1; C <= kMaxCluster; C *= 2) {
-    const int Ycs = ceil_div(Y, C);
-    if (C > 1 && (C - 1) * Ycs >= Y) break;  // a CTA would own no row
-    const SmemLayout L = smem_layout<S>(Xp, X, Ycs, true);
-    if ((size_t)L.total * sizeof(S) <= (size_t)max_smem) {
-      cf.C = C;
-      cf.Ycs = Ycs;
-      cf.gstate = false;
-      break;
-    }
-  }
-  const SmemLayout L = smem_layout<S>(Xp, X, cf.Ycs, !cf.gstate);
+  cf.gstate = gstate;
+  cf.C = C;
+  cf.Ycs = Ycs;
   cf.smem_bytes = (size_t)L.total * sizeof(S);
   cf.grid_elems = L.grid_elems;
-  const int cells = cf.Ycs * Xp;
+  const int cells = Ycs * Xp;
   cf.NT = cells >= 4096 ? 512 : (cells >= 1024 ? 256 : 128);
   if (cf.KX == 16) cf.NT = std::min(cf.NT, 256);
+  return true;
+}
+
+// Built-in choice: the smallest cluster the line family fits in (full tiles
+// first), else the chunk family on chip, else the chunk family on HBM.
+template <typename S>
+Config default_config(int X, int Y, int max_smem) {
+  Config cf;
+  for (int C = 1; C <= kMaxCluster; C *= 2) {
+    if (line_full_cfg<S>(X, Y, C, max_smem, cf)) return cf;
+    if (line_generic_cfg<S>(X, Y, C, max_smem, cf)) return cf;
+  }
+  for (int C = 1; C <= kMaxCluster; C *= 2)
+    if (chunk_cfg<S>(X, Y, C, max_smem, false, cf)) return cf;
+  chunk_cfg<S>(X, Y, 1, max_smem, true, cf);
   return cf;
+}
+
+// Every configuration that can run an X x Y grid: the search space of the
+// autotuner, in the order the built-in choice prefers them.  Splits thinner
+// than 16 rows per CTA (line family) or 8 (chunk family) are left out: the
+// cluster folds would cost more than the rows.
+template <typename S>
+std::vector<Config> enum_configs(int X, int Y, int max_smem) {
+  std::vector<Config> v;
+  Config cf;
+  for (int C = 1; C <= kMaxCluster; C *= 2) {
+    if (line_full_cfg<S>(X, Y, C, max_smem, cf)) v.push_back(cf);
+    if (line_generic_cfg<S>(X, Y, C, max_smem, cf) && (C == 1 || cf.Ycs >= 16)) v.push_back(cf);
+  }
+  for (int C = 1; C <= kMaxCluster; C *= 2)
+    if (chunk_cfg<S>(X, Y, C, max_smem, false, cf) && (C == 1 || cf.Ycs >= 8)) v.push_back(cf);
+  if (v.empty() && chunk_cfg<S>(X, Y, 1, max_smem, true, cf)) v.push_back(cf);
+  if (v.empty()) v.push_back(default_config<S>(X, Y, max_smem));
+  return v;
+}
+
+int family_of(const Config& c) {
+  return c.kind == kKindChunk ? LVC_FAMILY_CHUNK : (c.full ? LVC_FAMILY_LINE_FULL : LVC_FAMILY_LINE);
+}
+
+bool same_shape(const Config& a, const Config& b) {
+  return family_of(a) == family_of(b) && a.C == b.C && a.gstate == b.gstate;
+}
+
+using TuneKey = std::tuple<int, int, int>;  // numX, numY, precision
+
+template <typename S>
+int precision_of() { return sizeof(S) == sizeof(double) ? LVC_F64 : LVC_F32_STATE; }
+
+// The configuration of an X x Y grid: the context's tuned shape, else the
+// built-in choice.
+template <typename S>
+Config choose_config(const futhark_context* ctx, int X, int Y) {
+  auto it = ctx->shapes.find(TuneKey{X, Y, precision_of<S>()});
+  if (it != ctx->shapes.end()) return it->second.cf;
+  return default_config<S>(X, Y, ctx->max_smem);
 }
 
 template <typename S, typename PV>
@@ -471,14 +568,33 @@ cudaError_t plan_enqueue(lvc_plan* P, cudaStream_t s, cudaEvent_t* ev) {
                                                              P->d_tabs, (float*)P->d_piv);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
+  int nonempty = 0;
+  for (const Launch& L : P->launches) nonempty += L.n_items > 0;
+  // Fork: launch j of the (largest-first) classes goes to stream j % n, so
+  // the classes run side by side and the block scheduler fills the SMs one
+  // class leaves idle with CTAs of the next.  Timed runs stay on one stream.
+  const int nf = ev ? 1 : std::min(P->n_streams, nonempty);
+  if (nf > 1) {
+    if ((e = cudaEventRecord(P->ev_fork, s)) != cudaSuccess) return e;
+    for (int j = 1; j < nf; j++)
+      if ((e = cudaStreamWaitEvent(P->aux[j - 1], P->ev_fork, 0)) != cudaSuccess) return e;
+  }
+  int j = 0;
   for (size_t i = 0; i < P->launches.size(); i++) {
     const Launch& L = P->launches[i];
     if (L.n_items == 0) continue;
-    if (ev && (e = cudaEventRecord(ev[2 * i], s)) != cudaSuccess) return e;
-    e = P->precision == LVC_F64 ? launch_rollback<double, double>(P, L, s)
-                                : launch_rollback<float, float>(P, L, s);
+    const int si = nf > 1 ? j % nf : 0;
+    j++;
+    cudaStream_t ls = si == 0 ? s : P->aux[si - 1];
+    if (ev && (e = cudaEventRecord(ev[2 * i], ls)) != cudaSuccess) return e;
+    e = P->precision == LVC_F64 ? launch_rollback<double, double>(P, L, ls)
+                                : launch_rollback<float, float>(P, L, ls);
     if (e != cudaSuccess) return e;
-    if (ev && (e = cudaEventRecord(ev[2 * i + 1], s)) != cudaSuccess) return e;
+    if (ev && (e = cudaEventRecord(ev[2 * i + 1], ls)) != cudaSuccess) return e;
+  }
+  for (int k = 1; k < nf; k++) {
+    if ((e = cudaEventRecord(P->ev_join[k - 1], P->aux[k - 1])) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(s, P->ev_join[k - 1], 0)) != cudaSuccess) return e;
   }
   return cudaSuccess;
 }
@@ -487,6 +603,9 @@ void plan_release(lvc_plan* P) {
   if (!P) return;
   if (P->exec) cudaGraphExecDestroy(P->exec);
   if (P->graph) cudaGraphDestroy(P->graph);
+  if (P->ev_fork) cudaEventDestroy(P->ev_fork);
+  for (cudaEvent_t e : P->ev_join)
+    if (e) cudaEventDestroy(e);
   void* bufs[] = {P->d_calibs, P->d_tabs, P->d_piv, P->d_out, P->d_rowstart, P->d_items, P->d_gstate, P->d_err};
   for (void* b : bufs) {
     if (!b) continue;
@@ -521,7 +640,7 @@ int plan_build(futhark_context* ctx, const lvc_calibration* cs, int n, lvc_plan*
   for (int i = 0; i < n; i++) {
     const lvc_calibration& c = cs[i];
     if (int rc = validate(ctx, c, i)) return rc;
-    const Config cf = choose_config<S>(c.numX, c.numY, ctx->max_smem);
+    const Config cf = choose_config<S>(ctx, c.numX, c.numY);
     CalibDev& d = P->calibs[i];
     d.numX = c.numX;
     d.numY = c.numY;
@@ -557,6 +676,7 @@ int plan_build(futhark_context* ctx, const lvc_calibration* cs, int n, lvc_plan*
   P->nprices = out_off;
   // launch classes, largest work first inside each
   int64_t gstate_off = 0;
+  std::vector<int64_t> class_work;
   for (auto& kv : classes) {
     auto& v = kv.second;
     std::stable_sort(v.begin(), v.end(),
@@ -575,7 +695,12 @@ int plan_build(futhark_context* ctx, const lvc_calibration* cs, int n, lvc_plan*
     L.n_items = (int)v.size();
     L.smem_bytes = cf.smem_bytes;
     L.gstate_per_cta = cf.gstate ? cf.grid_elems : 0;
-    for (auto& e : v) P->items.push_back(e.second);
+    int64_t work = 0;
+    for (auto& e : v) {
+      P->items.push_back(e.second);
+      work += e.first;
+    }
+    class_work.push_back(work);
     if (L.n_items > 0) {
       if (int rc = prepare_launch<S, PV>(ctx, L, P->max_sms)) return rc;
       P->sms = std::max(P->sms, std::min<double>(L.grid * L.sm_per_cta, ctx->num_sms));
@@ -587,6 +712,14 @@ int plan_build(futhark_context* ctx, const lvc_calibration* cs, int n, lvc_plan*
     P->launches.push_back(L);
   }
   P->gstate_elems = gstate_off;
+  {  // largest class first: it starts first and sets the critical path
+    std::vector<size_t> ord(P->launches.size());
+    for (size_t i = 0; i < ord.size(); i++) ord[i] = i;
+    std::stable_sort(ord.begin(), ord.end(), [&](size_t a, size_t b) { return class_work[a] > class_work[b]; });
+    std::vector<Launch> sorted;
+    for (size_t i : ord) sorted.push_back(P->launches[i]);
+    P->launches.swap(sorted);
+  }
   const int64_t rows = P->row_start[n];
   P->pivot_grid = (int)std::max<int64_t>(1, std::min<int64_t>((rows + 127) / 128, 64LL * ctx->num_sms));
 
@@ -650,6 +783,14 @@ int plan_new_locked(futhark_context* ctx, const lvc_calibration* cs, int n, int 
   P->pool = pool;
   P->use_graph = use_graph;
   P->max_sms = max_sms;
+  if (use_graph && max_sms == 0) {  // batch plans follow the context's tuning
+    P->max_sms = ctx->tuning.grid == 1 ? -1 : 0;
+    P->n_streams = ctx->tuning.streams;
+    for (int k = 0; k < kMaxAux; k++) P->aux[k] = ctx->aux[k];
+    LVC_CUDA(ctx, cudaEventCreateWithFlags(&P->ev_fork, cudaEventDisableTiming));
+    for (int k = 0; k + 1 < P->n_streams; k++)
+      LVC_CUDA(ctx, cudaEventCreateWithFlags(&P->ev_join[k], cudaEventDisableTiming));
+  }
   const int rc = precision == LVC_F64 ? plan_build<double, double>(ctx, cs, n, P)
                                       : plan_build<float, float>(ctx, cs, n, P);
   if (rc) {
@@ -744,6 +885,18 @@ void futhark_context_config_set_cache_file(struct futhark_context_config* cfg, c
   (void)cfg;
   (void)f;
 }
+int futhark_context_config_set_tuning_param(struct futhark_context_config* cfg, const char* param_name,
+                                            size_t new_value) {
+  if (!cfg) return 1;
+  return set_tuning(cfg->tuning, param_name, new_value);
+}
+int futhark_get_tuning_param_count(void) { return kNumTuning; }
+const char* futhark_get_tuning_param_name(int i) {
+  return (i >= 0 && i < kNumTuning) ? kTuningNames[i] : nullptr;
+}
+const char* futhark_get_tuning_param_class(int i) {
+  return (i >= 0 && i < kNumTuning) ? kTuningClasses[i] : nullptr;
+}
 
 struct futhark_context* futhark_context_new(struct futhark_context_config* cfg) {
   futhark_context* ctx = new (std::nothrow) futhark_context();
@@ -790,6 +943,12 @@ struct futhark_context* futhark_context_new(struct futhark_context_config* cfg) 
     ctx->error = std::string("cannot create stream: ") + cudaGetErrorString(e);
     return ctx;
   }
+  for (int k = 0; k < kMaxAux; k++)
+    if ((e = cudaStreamCreateWithFlags(&ctx->aux[k], cudaStreamNonBlocking)) != cudaSuccess) {
+      ctx->error = std::string("cannot create stream: ") + cudaGetErrorString(e);
+      return ctx;
+    }
+  if (cfg) ctx->tuning = cfg->tuning;
   ctx->ok = true;
   return ctx;
 }
@@ -803,6 +962,8 @@ void futhark_context_free(struct futhark_context* ctx) {
     delete ctx->pool;
     cudaStreamDestroy(ctx->stream);
     cudaStreamDestroy(ctx->capture);
+    for (cudaStream_t a : ctx->aux)
+      if (a) cudaStreamDestroy(a);
   }
   delete ctx;
 }
@@ -1065,6 +1226,301 @@ int lvc_batch(struct futhark_context* ctx, const struct lvc_calibration* calibs,
 
 void* lvc_context_stream(struct futhark_context* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
 
+int lvc_context_set_tuning_param(struct futhark_context* ctx, const char* param_name, size_t new_value) {
+  std::lock_guard<std::mutex> g(ctx->mu);
+  if (set_tuning(ctx->tuning, param_name, new_value))
+    return set_error(ctx, FUTHARK_PROGRAM_ERROR,
+                     std::string("unknown tuning parameter or value: ") + (param_name ? param_name : "(null)"));
+  return 0;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Shape autotuner.  For every grid class (numX, numY) of a workload it times
+// each configuration that can run the class -- kernel family, cluster size
+// and the CTA shape that follows from them -- on the class's own number of
+// strike instances for a few time steps, and keeps the fastest in the
+// context's tuning table, which every plan, entry point and server built
+// from the context then uses.  The table is written and read as a tuning
+// file of `name=value` lines, the form of Futhark's own tuning files.
+// ---------------------------------------------------------------------------
+namespace {
+
+const char* family_name(int fam, bool gstate) {
+  if (fam == LVC_FAMILY_LINE_FULL) return "line_full";
+  if (fam == LVC_FAMILY_LINE) return "line";
+  return gstate ? "chunk_hbm" : "chunk";
+}
+
+void to_shape(const Config& c, lvc_shape* o) {
+  o->family = family_of(c);
+  o->cluster = c.C;
+  o->threads = c.NT;
+  o->rows_per_cta = c.Ycs;
+  o->smem_bytes = (int32_t)c.smem_bytes;
+  o->hbm_state = c.gstate ? 1 : 0;
+}
+
+int check_grid(futhark_context* ctx, int X, int Y, int precision) {
+  if (precision != LVC_F64 && precision != LVC_F32_STATE)
+    return set_error(ctx, FUTHARK_PROGRAM_ERROR, "unknown precision");
+  if (X < 3 || Y < 3 || X > kMaxNumX || Y > kMaxNumY)
+    return set_error(ctx, FUTHARK_PROGRAM_ERROR, "grid size out of range");
+  return 0;
+}
+
+std::vector<Config> candidates(const futhark_context* ctx, int X, int Y, int precision) {
+  return precision == LVC_F64 ? enum_configs<double>(X, Y, ctx->max_smem)
+                              : enum_configs<float>(X, Y, ctx->max_smem);
+}
+
+Config builtin(const futhark_context* ctx, int X, int Y, int precision) {
+  return precision == LVC_F64 ? default_config<double>(X, Y, ctx->max_smem)
+                              : default_config<float>(X, Y, ctx->max_smem);
+}
+
+// Microseconds per time step of the rollback launch of calibration c under
+// the context's current table (median of `reps` timed runs after one warm-up).
+constexpr double kTuneMargin = 1.03;  // a shape replaces the built-in one only when 3% faster
+
+int probe_us_per_step(futhark_context* ctx, const lvc_calibration& c, int precision, int reps, double* us) {
+  if (!ctx->pool) ctx->pool = new DevicePool();
+  lvc_plan* P = nullptr;
+  const int max_sms = ctx->tuning.grid == 1 ? -1 : 0;
+  if (int rc = plan_new_locked(ctx, &c, 1, precision, &P, ctx->pool, /*use_graph=*/false, max_sms)) return rc;
+  std::vector<cudaEvent_t> ev(2 * P->launches.size(), nullptr);
+  for (auto& x : ev) {
+    cudaError_t e = cudaEventCreate(&x);
+    if (e != cudaSuccess) {
+      for (auto& y : ev)
+        if (y) cudaEventDestroy(y);
+      plan_release(P);
+      return cuda_fail(ctx, e, "cudaEventCreate");
+    }
+  }
+  std::vector<double> t;
+  int rc = 0;
+  for (int r = 0; r <= reps && !rc; r++) {
+    cudaError_t e = plan_enqueue(P, ctx->stream, ev.data());
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) {
+      rc = cuda_fail(ctx, e, "autotune probe");
+      break;
+    }
+    double ms = 0.0;
+    for (size_t l = 0; l < P->launches.size(); l++) {
+      if (P->launches[l].n_items == 0) continue;
+      float x = 0.f;
+      cudaEventElapsedTime(&x, ev[2 * l], ev[2 * l + 1]);
+      ms += x;
+    }
+    if (r > 0) t.push_back(ms);
+  }
+  if (!rc) rc = check_device_error(ctx, P);
+  for (auto& x : ev) cudaEventDestroy(x);
+  plan_release(P);
+  if (rc) return rc;
+  std::sort(t.begin(), t.end());
+  *us = t.empty() ? 0.0 : 1e3 * t[t.size() / 2] / std::max(1, c.numT - 1);
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lvc_shape_candidates(struct futhark_context* ctx, int32_t numX, int32_t numY, int32_t precision,
+                         struct lvc_shape* out, int32_t max, int32_t* count) {
+  std::lock_guard<std::mutex> g(ctx->mu);
+  if (int rc = check_grid(ctx, numX, numY, precision)) return rc;
+  const std::vector<Config> v = candidates(ctx, numX, numY, precision);
+  for (int i = 0; i < (int)v.size() && i < max; i++) to_shape(v[i], &out[i]);
+  if (count) *count = (int32_t)v.size();
+  return 0;
+}
+
+int lvc_tuning_set(struct futhark_context* ctx, int32_t numX, int32_t numY, int32_t precision,
+                   const struct lvc_shape* shape) {
+  std::lock_guard<std::mutex> g(ctx->mu);
+  if (int rc = check_grid(ctx, numX, numY, precision)) return rc;
+  const TuneKey key{numX, numY, precision};
+  if (!shape) {
+    ctx->shapes.erase(key);
+    return 0;
+  }
+  for (const Config& c : candidates(ctx, numX, numY, precision)) {
+    if (family_of(c) == shape->family && c.C == shape->cluster && (c.gstate ? 1 : 0) == shape->hbm_state) {
+      TunedShape t;
+      t.cf = c;
+      t.tuned = true;
+      ctx->shapes[key] = t;
+      return 0;
+    }
+  }
+  return set_error(ctx, FUTHARK_PROGRAM_ERROR, "no such shape for this grid size on this device");
+}
+
+int lvc_tuning_get(struct futhark_context* ctx, int32_t numX, int32_t numY, int32_t precision,
+                   struct lvc_tuning_entry* out) {
+  std::lock_guard<std::mutex> g(ctx->mu);
+  if (int rc = check_grid(ctx, numX, numY, precision)) return rc;
+  *out = lvc_tuning_entry{};
+  out->numX = numX;
+  out->numY = numY;
+  out->precision = precision;
+  auto it = ctx->shapes.find(TuneKey{numX, numY, precision});
+  if (it != ctx->shapes.end()) {
+    to_shape(it->second.cf, &out->shape);
+    out->tuned = it->second.tuned ? 1 : 0;
+    out->us_per_step_default = it->second.us_default;
+    out->us_per_step_best = it->second.us_best;
+  } else {
+    to_shape(builtin(ctx, numX, numY, precision), &out->shape);
+  }
+  return 0;
+}
+
+int32_t lvc_tuning_entries(struct futhark_context* ctx, struct lvc_tuning_entry* out, int32_t max) {
+  std::lock_guard<std::mutex> g(ctx->mu);
+  int32_t n = 0;
+  for (const auto& kv : ctx->shapes) {
+    if (out && n < max) {
+      lvc_tuning_entry& e = out[n];
+      e = lvc_tuning_entry{};
+      e.numX = std::get<0>(kv.first);
+      e.numY = std::get<1>(kv.first);
+      e.precision = std::get<2>(kv.first);
+      e.tuned = kv.second.tuned ? 1 : 0;
+      to_shape(kv.second.cf, &e.shape);
+      e.us_per_step_default = kv.second.us_default;
+      e.us_per_step_best = kv.second.us_best;
+    }
+    n++;
+  }
+  return n;
+}
+
+int lvc_autotune(struct futhark_context* ctx, const struct lvc_calibration* calibs, int32_t n,
+                 int32_t precision, int32_t probe_steps) {
+  std::lock_guard<std::mutex> g(ctx->mu);
+  if (!ctx->ok) return set_error(ctx, FUTHARK_PROGRAM_ERROR, "context has no usable CUDA device");
+  if (precision != LVC_F64 && precision != LVC_F32_STATE)
+    return set_error(ctx, FUTHARK_PROGRAM_ERROR, "unknown precision");
+  if (n < 0 || (n > 0 && !calibs)) return set_error(ctx, FUTHARK_PROGRAM_ERROR, "bad calibration list");
+  LVC_CUDA(ctx, cudaSetDevice(ctx->device));
+  if (probe_steps <= 0) probe_steps = 8;
+  // grid classes: instance count and a representative calibration
+  std::map<std::pair<int, int>, std::pair<int64_t, lvc_calibration>> classes;
+  for (int i = 0; i < n; i++) {
+    if (int rc = validate(ctx, calibs[i], i)) return rc;
+    if (calibs[i].outer == 0 || calibs[i].numT < 2) continue;
+    auto& e = classes[{calibs[i].numX, calibs[i].numY}];
+    if (e.first == 0) e.second = calibs[i];
+    e.first += calibs[i].outer;
+  }
+  for (const auto& kv : classes) {
+    const int X = kv.first.first, Y = kv.first.second;
+    const TuneKey key{X, Y, precision};
+    const std::vector<Config> cands = candidates(ctx, X, Y, precision);
+    const Config def = builtin(ctx, X, Y, precision);
+    lvc_calibration probe = kv.second.second;
+    probe.outer = (int32_t)std::min<int64_t>(kv.second.first, 1 << 14);
+    probe.numT = probe_steps + 1;
+    TunedShape best;
+    best.cf = def;
+    best.tuned = true;
+    double best_us = 0.0, def_us = 0.0;
+    bool any = false;
+    for (const Config& c : cands) {
+      TunedShape t;
+      t.cf = c;
+      t.tuned = true;
+      ctx->shapes[key] = t;
+      double us = 0.0;
+      if (probe_us_per_step(ctx, probe, precision, 3, &us)) {
+        ctx->error.clear();  // a shape that cannot run here is skipped
+        continue;
+      }
+      if (same_shape(c, def)) def_us = us;
+      // the built-in shape is kept unless another wins by a clear margin: a
+      // class's probe runs alone, while in a plan it overlaps other classes
+      const double margin = same_shape(c, def) ? 1.0 / kTuneMargin : (same_shape(best.cf, def) ? kTuneMargin : 1.0);
+      if (!any || us * margin < best_us) {
+        best.cf = c;
+        best_us = us;
+        any = true;
+      }
+    }
+    if (any && same_shape(best.cf, def) && def_us > 0.0) best_us = def_us;
+    if (!any) {
+      ctx->shapes.erase(key);
+      return set_error(ctx, FUTHARK_PROGRAM_ERROR, "autotune: no shape ran for a grid class");
+    }
+    best.us_best = best_us;
+    best.us_default = def_us;
+    ctx->shapes[key] = best;
+  }
+  return 0;
+}
+
+int lvc_tuning_save(struct futhark_context* ctx, const char* path) {
+  std::lock_guard<std::mutex> g(ctx->mu);
+  FILE* f = path ? fopen(path, "w") : nullptr;
+  if (!f) return set_error(ctx, FUTHARK_PROGRAM_ERROR, std::string("cannot write tuning file ") + (path ? path : ""));
+  fprintf(f, "lvc.streams=%d\nlvc.grid=%d\n", ctx->tuning.streams, ctx->tuning.grid);
+  for (const auto& kv : ctx->shapes)
+    fprintf(f, "lvc.shape.%s.%dx%d=%s,%d\n", std::get<2>(kv.first) == LVC_F64 ? "f64" : "f32state",
+            std::get<0>(kv.first), std::get<1>(kv.first),
+            family_name(family_of(kv.second.cf), kv.second.cf.gstate), kv.second.cf.C);
+  fclose(f);
+  return 0;
+}
+
+int lvc_tuning_load(struct futhark_context* ctx, const char* path) {
+  FILE* f = path ? fopen(path, "r") : nullptr;
+  if (!f) {
+    std::lock_guard<std::mutex> g(ctx->mu);
+    return set_error(ctx, FUTHARK_PROGRAM_ERROR, std::string("cannot read tuning file ") + (path ? path : ""));
+  }
+  char line[256];
+  int lineno = 0, rc = 0;
+  while (!rc && fgets(line, sizeof line, f)) {
+    lineno++;
+    char* nl = strpbrk(line, "\r\n");
+    if (nl) *nl = 0;
+    if (!line[0] || line[0] == '#') continue;
+    char prec[16], fam[16];
+    int X = 0, Y = 0, C = 0;
+    unsigned long v = 0;
+    char name[128];
+    if (sscanf(line, "lvc.shape.%15[a-z0-9].%dx%d=%15[a-z_],%d", prec, &X, &Y, fam, &C) == 5) {
+      lvc_shape sh{};
+      sh.cluster = C;
+      const std::string fs(fam);
+      sh.family = fs == "line_full" ? LVC_FAMILY_LINE_FULL : fs == "line" ? LVC_FAMILY_LINE : LVC_FAMILY_CHUNK;
+      sh.hbm_state = fs == "chunk_hbm" ? 1 : 0;
+      const bool known = fs == "line_full" || fs == "line" || fs == "chunk" || fs == "chunk_hbm";
+      const int p = !strcmp(prec, "f64") ? LVC_F64 : !strcmp(prec, "f32state") ? LVC_F32_STATE : -1;
+      if (!known || p < 0) rc = 1;
+      else rc = lvc_tuning_set(ctx, X, Y, p, &sh);
+    } else if (sscanf(line, "%127[a-z.]=%lu", name, &v) == 2) {
+      std::lock_guard<std::mutex> g(ctx->mu);
+      rc = set_tuning(ctx->tuning, name, v) ? 1 : 0;
+    } else {
+      rc = 1;
+    }
+  }
+  fclose(f);
+  if (rc) {
+    std::lock_guard<std::mutex> g(ctx->mu);
+    char buf[160];
+    snprintf(buf, sizeof buf, "tuning file %s: line %d not understood or not valid on this device", path, lineno);
+    return set_error(ctx, FUTHARK_PROGRAM_ERROR, buf);
+  }
+  return 0;
+}
+
 int lvc_probe_peaks(struct futhark_context* ctx, double* fp64_tflops, double* smem_gbs) {
   std::lock_guard<std::mutex> g(ctx->mu);
   if (!ctx->ok) return set_error(ctx, FUTHARK_PROGRAM_ERROR, "context has no usable CUDA device");
@@ -1170,7 +1626,7 @@ extern "C" int lvc_entry_main_f64_noalloc(struct futhark_context* ctx, double* p
   unsigned char* base = nullptr;
   if (int rc = noalloc_scratch(ctx, &base)) return rc;
 
-  const Config cf = choose_config<double>(numX, numY, ctx->max_smem);
+  const Config cf = choose_config<double>(ctx, numX, numY);
   if (cf.gstate)
     return set_error(ctx, FUTHARK_PROGRAM_ERROR,
                      "lvc_entry_main_f64_noalloc: this grid does not fit on chip; its HBM state "
@@ -1392,10 +1848,10 @@ void server_retire(lvc_server* S) {
 
 // Device bytes a one-calibration plan takes (tables, pivots, work list,
 // prices, state scratch), from the same layouts the plan builder uses.
-size_t request_bytes(const lvc_calibration& c, int precision, int max_smem) {
+size_t request_bytes(const futhark_context* ctx, const lvc_calibration& c, int precision) {
   const bool f64 = precision == LVC_F64;
-  const Config cf = f64 ? choose_config<double>(c.numX, c.numY, max_smem)
-                        : choose_config<float>(c.numX, c.numY, max_smem);
+  const Config cf = f64 ? choose_config<double>(ctx, c.numX, c.numY)
+                        : choose_config<float>(ctx, c.numX, c.numY);
   const int Xp = std::max(8, pow2ceil(c.numX));
   const size_t ps = f64 ? 8 : 4;
   size_t b = 8 * (size_t)al2(tab_layout(c.numX, c.numY, c.numT, Xp, cf.kind).total);
@@ -1422,7 +1878,7 @@ bool server_admit(lvc_server* S, std::unique_lock<std::mutex>& lk) {
   while (!S->pending.empty() && (int)take.size() < S->cfg.max_batch_requests &&
          S->inflight_requests + (int)take.size() < S->cfg.max_inflight_requests) {
     SrvRequest* r = S->pending.front();
-    const size_t rb = request_bytes(r->c, S->cfg.precision, S->sctx.max_smem);
+    const size_t rb = request_bytes(&S->sctx, r->c, S->cfg.precision);
     if (rb > S->pool.budget) {  // can never fit: fail it now
       S->pending.pop_front();
       r->status = 2;
@@ -1553,6 +2009,11 @@ int lvc_server_new(struct futhark_context* ctx, const struct lvc_server_config* 
   S->sctx.device = ctx->device;
   S->sctx.num_sms = ctx->num_sms;
   S->sctx.max_smem = ctx->max_smem;
+  {
+    std::lock_guard<std::mutex> g(ctx->mu);
+    S->sctx.shapes = ctx->shapes;  // the server prices with the shapes tuned so far
+    S->sctx.tuning = ctx->tuning;
+  }
   S->sctx.ok = true;
   S->pool.budget = (size_t)c.hbm_budget_bytes;
   cudaError_t e = cudaStreamCreateWithFlags(&S->sctx.stream, cudaStreamNonBlocking);

@@ -59,6 +59,20 @@ LVC_API void futhark_context_config_set_logging(struct futhark_context_config *c
  * cache file (its kernels are compiled ahead of time for sm_100a). */
 LVC_API void futhark_context_config_set_cache_file(struct futhark_context_config *cfg, const char *f);
 
+/* Tuning parameters by name, as the generated API of a Futhark program
+ * exposes them (futhark_context_config_set_tuning_param and the
+ * futhark_get_tuning_param_* enumeration).  Returns 0, or 1 for an unknown
+ * name or an out-of-range value.  Names:
+ *   "lvc.streams"  streams a batch plan forks its launch classes over (1..8, default 4)
+ *   "lvc.grid"     0 (default): persistent grids, items taken in strides; 1: one
+ *                  CTA or cluster per strike instance, handed out by the block
+ *                  scheduler in descending order of work */
+LVC_API int futhark_context_config_set_tuning_param(struct futhark_context_config *cfg,
+                                                    const char *param_name, size_t new_value);
+LVC_API int futhark_get_tuning_param_count(void);
+LVC_API const char *futhark_get_tuning_param_name(int i);
+LVC_API const char *futhark_get_tuning_param_class(int i);
+
 /* lys/shared.c:47 -- returns NULL only on allocation failure; a context whose
  * device could not be initialised reports that from futhark_context_get_error. */
 LVC_API struct futhark_context *futhark_context_new(struct futhark_context_config *cfg);
@@ -225,6 +239,63 @@ LVC_API int lvc_probe_peaks(struct futhark_context *ctx, double *fp64_tflops, do
 
 /* The cudaStream_t the context launches on (as void*). */
 LVC_API void *lvc_context_stream(struct futhark_context *ctx);
+
+/* The same tuning parameters on a live context; plans created afterwards use
+ * them.  0, or FUTHARK_PROGRAM_ERROR for an unknown name or value. */
+LVC_API int lvc_context_set_tuning_param(struct futhark_context *ctx, const char *param_name,
+                                         size_t new_value);
+
+/* Shape autotuner.  A grid class (numX, numY, precision) can run under
+ * several shapes: kernel family x cluster size, which fix the CTA's threads,
+ * rows and shared memory.  The context keeps a table of chosen shapes that
+ * every plan, entry point, no-alloc call and server built from it uses;
+ * classes not in the table take the built-in choice. */
+#define LVC_FAMILY_CHUNK 0     /* chunked lines, any numX <= 512; grid on chip or in HBM */
+#define LVC_FAMILY_LINE 1      /* one lane per grid line, any sizes with numX <= 256 */
+#define LVC_FAMILY_LINE_FULL 2 /* line family on full 32 x 32 tiles (numX, rows per CTA multiples of 32) */
+
+struct lvc_shape {
+  int32_t family;       /* LVC_FAMILY_* */
+  int32_t cluster;      /* CTAs per strike instance (a thread-block cluster when > 1) */
+  int32_t threads;      /* threads per CTA */
+  int32_t rows_per_cta; /* numY rows each CTA holds */
+  int32_t smem_bytes;   /* dynamic shared memory per CTA */
+  int32_t hbm_state;    /* 1: the grid lives in HBM scratch (chunk family only) */
+};
+
+struct lvc_tuning_entry {
+  int32_t numX, numY, precision;
+  int32_t tuned;              /* 1: chosen by lvc_autotune or set by lvc_tuning_set */
+  struct lvc_shape shape;
+  double us_per_step_default; /* autotune probe time of the built-in shape (0: not measured) */
+  double us_per_step_best;    /* autotune probe time of the chosen shape (0: not measured) */
+};
+
+/* Every shape that can run the grid class on this device; *count receives
+ * the number (entries beyond `max` are not written). */
+LVC_API int lvc_shape_candidates(struct futhark_context *ctx, int32_t numX, int32_t numY,
+                                 int32_t precision, struct lvc_shape *out, int32_t max,
+                                 int32_t *count);
+/* Pins a shape (matched on family, cluster and hbm_state) for a grid class;
+ * NULL returns the class to the built-in choice. */
+LVC_API int lvc_tuning_set(struct futhark_context *ctx, int32_t numX, int32_t numY,
+                           int32_t precision, const struct lvc_shape *shape);
+/* The shape the class runs under now (tuned or built-in). */
+LVC_API int lvc_tuning_get(struct futhark_context *ctx, int32_t numX, int32_t numY,
+                           int32_t precision, struct lvc_tuning_entry *out);
+/* Entries of the table (up to `max` written); returns how many there are. */
+LVC_API int32_t lvc_tuning_entries(struct futhark_context *ctx, struct lvc_tuning_entry *out,
+                                   int32_t max);
+/* For every grid class of the calibrations: times each candidate shape's
+ * rollback on the class's own instance count (capped at 16384) for
+ * probe_steps time steps (<= 0: 8), and keeps the fastest.  Synchronous. */
+LVC_API int lvc_autotune(struct futhark_context *ctx, const struct lvc_calibration *calibs,
+                         int32_t n, int32_t precision, int32_t probe_steps);
+/* The tuning parameters and the table as a tuning file of name=value lines:
+ *   lvc.streams=4
+ *   lvc.shape.f64.256x256=line_full,8      (family: line_full|line|chunk|chunk_hbm, cluster) */
+LVC_API int lvc_tuning_save(struct futhark_context *ctx, const char *path);
+LVC_API int lvc_tuning_load(struct futhark_context *ctx, const char *path);
 
 #ifdef __cplusplus
 }

@@ -58,3 +58,21 @@ def test_config_api_is_callable_without_gpu(pkg):
     lib.futhark_context_config_set_debugging(cfg, 1)
     lib.futhark_context_config_set_cache_file(cfg, b"/nonexistent")
     lib.futhark_context_config_free(cfg)
+
+
+def test_tuning_parameters_by_name(pkg):
+    # the Futhark-generated API's tuning-parameter surface; no device needed
+    lib = pkg.load_library()
+    names = [lib.futhark_get_tuning_param_name(i).decode() for i in range(lib.futhark_get_tuning_param_count())]
+    assert names == ["lvc.streams", "lvc.grid"]
+    assert lib.futhark_get_tuning_param_name(len(names)) is None
+    cfg = lib.futhark_context_config_new()
+    try:
+        assert lib.futhark_context_config_set_tuning_param(cfg, b"lvc.streams", 2) == 0
+        assert lib.futhark_context_config_set_tuning_param(cfg, b"lvc.grid", 1) == 0
+        assert lib.futhark_context_config_set_tuning_param(cfg, b"lvc.streams", 0) == 1
+        assert lib.futhark_context_config_set_tuning_param(cfg, b"lvc.streams", 9) == 1
+        assert lib.futhark_context_config_set_tuning_param(cfg, b"lvc.grid", 2) == 1
+        assert lib.futhark_context_config_set_tuning_param(cfg, b"no.such.param", 1) == 1
+    finally:
+        lib.futhark_context_config_free(cfg)
