@@ -25,7 +25,7 @@ ORACLE_DIR = os.path.join(REPO, "oracle")
 ORACLE_LIB = os.path.join(ORACLE_DIR, "liblvc_oracle.so")
 
 SOURCES = ["lvc_runtime.cu"]
-HEADERS = ["lvc_kernels.cuh", "lvc_layout.h", "lvc_probe.cuh", "lvc_line.cuh"]
+HEADERS = ["lvc_kernels.cuh", "lvc_layout.h", "lvc_probe.cuh", "lvc_line.cuh", "lvc_pair.cuh"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",

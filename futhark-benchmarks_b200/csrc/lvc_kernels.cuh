@@ -204,9 +204,9 @@ __global__ void __launch_bounds__(128) lvc_pivot_kernel(const CalibDev* __restri
       // b'_i = (dt - e W1_i) - (e W0_i)(e W2_{i-1}) / b'_{i-1}, stored as rows of
       // stride LD (the line kernel's shared-memory image)
       const double e = tab[L.stab + ((int64_t)k * Y + j) * 8];
-      const int LDl = line_ld(X);
+      const int LDl = c.ld;
       PV* o = piv + c.piv + ((int64_t)k * round4(Y) + j) * LDl;
-      if (LDl > X) o[X] = (PV)0;
+      for (int i = X; i < LDl; i++) o[i] = (PV)0;
       const double* W0 = tab + L.wcol;
       const double* W1 = W0 + L.xa;
       const double* W2 = W1 + L.xa;

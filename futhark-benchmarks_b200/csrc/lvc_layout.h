@@ -33,7 +33,7 @@ enum : int32_t {
 struct CalibDev {
   int32_t numX, numY, numT, Xp;      // Xp: numX padded to a power of two >= 8
   int32_t outer, xindex, yindex, C;  // C: CTAs (cluster size) per instance
-  int32_t kind, Ycs, pad0, pad1;     // kernel family; rows per CTA
+  int32_t kind, Ycs, ld, pad1;       // kernel family; rows per CTA; line family: row stride
   double s0, t, alpha, nu, beta;
   int64_t tab;  // offset (doubles) of the operator tables in the table arena
   int64_t piv;  // offset (elements) of the X-direction pivots in the pivot arena
@@ -99,17 +99,21 @@ enum : int {
 };
 
 // Line family: the pivot rows are stored exactly as the kernel's shared-memory
-// image of them -- row j of step k at ((k*Y4 + j) * LD) with the odd row
-// stride LD = numX | 1 -- so one bulk copy moves a CTA's rows.
+// image of them -- row j of step k at ((k*Y4 + j) * LD) -- so one bulk copy
+// moves a CTA's rows.  The row stride is CalibDev::ld: the odd LD = numX | 1
+// (8-byte accesses down a column conflict-free) for the line and full-tile
+// kernels, LD = numX + 2 (2 mod 4: 16-byte pair accesses conflict-free and
+// aligned) for the paired kernel.
 LVC_HD int line_ld(int X) { return X | 1; }
+LVC_HD int pair_ld(int X) { return X + 2; }
 LVC_HD int64_t round4(int64_t n) { return (n + 3) & ~int64_t(3); }
 
 // Elements of the X-direction pivot array of one calibration (plus 4 of
 // padding so that bulk copies rounded up to 16 bytes stay in bounds):
-// chunk family rbX[T-1][Y][Xp]; line family rbL[T-1][Y4][LD].
-LVC_HD int64_t piv_elems(int X, int Y, int T, int Xp, int kind) {
+// chunk family rbX[T-1][Y][Xp]; line family rbL[T-1][Y4][ld].
+LVC_HD int64_t piv_elems(int X, int Y, int T, int Xp, int kind, int ld) {
   const int64_t steps = T > 1 ? (int64_t)(T - 1) : 0;
-  return kind == kKindChunk ? steps * Y * Xp : steps * round4(Y) * line_ld(X) + 4;
+  return kind == kKindChunk ? steps * Y * Xp : steps * round4(Y) * ld + 4;
 }
 
 // Row padding of the on-chip grid: PADS elements after every 8, so that the

@@ -133,7 +133,7 @@ __global__ void __launch_bounds__(NT, (NT >= 512 ? 1 : 512 / NT)) lvc_line_kerne
     const int Yc = max(0, min(Ycs, Y - r0));
     const LineLayout Ls = line_layout<S>(X, Ycs, NW);
     // uniform over the cluster (every CTA of a cluster sees the same item)
-    if (c.kind != kKindLine || c.C != C || Ls.total > args.smem_elems * (int)sizeof(S) ||
+    if (c.kind != kKindLine || c.C != C || c.ld != Ls.LD || Ls.total > args.smem_elems * (int)sizeof(S) ||
         Ls.Ux > NW || Ls.Uy > NW || Yc < 1 || (C > 1 && (Ycs & 3))) {
       if (tid == 0) atomicExch(args.err, 2);
       continue;
@@ -534,8 +534,8 @@ __global__ void __launch_bounds__(NT, (FullMinBlocks<NT>::v)) lvc_line_full_kern
     const int Ycs = c.Ycs;
     const int r0 = rank * Ycs;
     const FullLayout Ls = full_layout<S>(X, Ycs, NU);
-    if (c.kind != kKindLine || c.C != C || Ls.total > args.smem_elems * (int)sizeof(S) || Ls.Ux != NU ||
-        Ls.Uy != NU || (X % 32) || (Ycs % 32) || Ycs * C != Y) {
+    if (c.kind != kKindLine || c.C != C || c.ld != Ls.LD || Ls.total > args.smem_elems * (int)sizeof(S) ||
+        Ls.Ux != NU || Ls.Uy != NU || (X % 32) || (Ycs % 32) || Ycs * C != Y) {
       if (tid == 0) atomicExch(args.err, 4);
       continue;
     }

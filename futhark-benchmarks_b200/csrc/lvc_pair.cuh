@@ -1,0 +1,529 @@
+// Paired line kernel: the full-tile line kernel's algorithm with every
+// shared-memory access widened to two adjacent grid columns.
+//
+// The rollback of finpar/LocVolCalib.fut:180-209 per time step, on an
+// X x Ycs block of the grid held in shared memory (one CTA per strike
+// instance, or Ycs rows per CTA of a cluster):
+//   X sweep  lane = grid row, a warp unit = 32 rows x 16 columns; the lane
+//            walks its 16 columns two at a time, reading the grid, the
+//            rows above and below and the pivots as 16-byte pairs, and the
+//            column weights W0, W1, W2 as pair broadcasts (planar arrays);
+//   Y sweep  lane = two adjacent columns, a warp unit = 64 columns x 16
+//            rows; every per-row table entry it broadcasts serves both
+//            column recurrences, and grid rows move as 16-byte pairs.
+// The row stride LD = numX + 2 is 2 mod 4 doubles, so the 32 lanes of a warp
+// reading one 16-byte pair from 32 consecutive rows fall into 4 conflict-free
+// wavefronts (8 lanes cover the 32 banks), and rows start 16-byte aligned for
+// the pair accesses of the Y sweep.  Columns numX and numX + 1 are zero.
+// Needs numX % 64 == 0 (whole 64-column Y units), rows per CTA % 32 == 0 and
+// numY = cluster size x rows per CTA.
+#pragma once
+
+#include "lvc_line.cuh"
+
+namespace lvc {
+
+struct PairLayout {
+  int LD, Ycs, CHx, Ux, CG2, CHy, Uy;
+  int bar, A, B, w0, w1, w2, grow, tab0, tab1, xfa, xfb, xba, xbb, yf, yb, blkF, blkB, zin, xin, tot, total;
+};
+
+// Byte offsets of the shared-memory buffers.
+template <typename S>
+LVC_HD PairLayout pair_layout(int X, int Ycs) {
+  PairLayout L;
+  auto up = [](int n) { return (n + 15) / 16 * 16; };
+  const int s = (int)sizeof(S);
+  L.LD = pair_ld(X);
+  L.Ycs = Ycs;
+  L.CHx = X / kLineK;
+  L.Ux = (Ycs / 32) * L.CHx;  // X units: 2 per warp
+  L.CG2 = X / 64;
+  L.CHy = Ycs / kLineK;
+  L.Uy = L.CG2 * L.CHy;       // Y units: 1 per warp
+  int o = 0;
+  L.bar = o; o += 16;
+  L.A = o; o += up((Ycs + 2) * L.LD * s);  // rows -1 .. Ycs (halo rows at both ends)
+  L.B = o; o += up(Ycs * L.LD * s);
+  L.w0 = o; o += up(X * s);               // W_k(i), planar
+  L.w1 = o; o += up(X * s);
+  L.w2 = o; o += up(X * s);
+  L.grow = o; o += up(4 * Ycs * s);
+  L.tab0 = o; o += up(8 * Ycs * 8);
+  L.tab1 = o; o += up(8 * Ycs * 8);
+  L.xfa = o; o += up(L.Ux * 32 * s);
+  L.xfb = o; o += up(L.Ux * 32 * s);
+  L.xba = o; o += up(L.Ux * 32 * s);
+  L.xbb = o; o += up(L.Ux * 32 * s);
+  L.yf = o; o += up(L.Uy * 64 * s);
+  L.yb = o; o += up(L.Uy * 64 * s);
+  L.blkF = o; o += up(X * s);
+  L.blkB = o; o += up(X * s);
+  L.zin = o; o += up(X * s);
+  L.xin = o; o += up(X * s);
+  L.tot = o; o += up(4 * s);
+  L.total = o;
+  return L;
+}
+
+template <typename S> struct P2;
+template <> struct P2<double> {
+  using T = double2;
+  static __device__ __forceinline__ double2 ld(const double* p) { return *reinterpret_cast<const double2*>(p); }
+  static __device__ __forceinline__ void st(double* p, double a, double b) {
+    *reinterpret_cast<double2*>(p) = make_double2(a, b);
+  }
+};
+template <> struct P2<float> {
+  using T = float2;
+  static __device__ __forceinline__ float2 ld(const float* p) { return *reinterpret_cast<const float2*>(p); }
+  static __device__ __forceinline__ void st(float* p, float a, float b) {
+    *reinterpret_cast<float2*>(p) = make_float2(a, b);
+  }
+};
+
+template <typename S, typename PV, int NT>
+__global__ void __launch_bounds__(NT, (FullMinBlocks<NT>::v)) lvc_line_pair_kernel(RollbackArgs<S, PV> args) {
+  constexpr int K = kLineK;
+  constexpr int NW = NT / 32;
+  constexpr int UPW = 2;        // X units per warp
+  constexpr int NU = NW * UPW;  // X units per sweep
+  static_assert(sizeof(S) == sizeof(PV), "pivots are copied verbatim into the state buffer");
+  static_assert(K % 2 == 0, "columns are walked in pairs");
+  using V = P2<S>;
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int C = args.C;
+  const bool clustered = C > 1;
+  int rank = 0;
+  if (clustered) rank = (int)cg::this_cluster().block_rank();
+  const int cid = blockIdx.x / C, ncl = gridDim.x / C;
+  unsigned sc = 0, phase = 0;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem);
+  if (tid == 0) {
+    mbar_init(bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+
+  for (int it = cid; it < args.n_items; it += ncl) {
+    const Item item = args.items[it];
+    const CalibDev c = args.calibs[item.calib];
+    const int X = c.numX, Y = c.numY, T = c.numT;
+    const int Ycs = c.Ycs;
+    const int r0 = rank * Ycs;
+    const PairLayout Ls = pair_layout<S>(X, Ycs);
+    // uniform over the cluster (every CTA of a cluster sees the same item)
+    if (c.kind != kKindLine || c.C != C || c.ld != Ls.LD || Ls.total > args.smem_elems * (int)sizeof(S) ||
+        Ls.Ux != NU || Ls.Uy != NW || (X % 64) || (Ycs % 32) || Ycs * C != Y) {
+      if (tid == 0) atomicExch(args.err, 5);
+      continue;
+    }
+    const int LD = Ls.LD;
+    S* A = reinterpret_cast<S*>(smem + Ls.A);  // row r of the block at A + (r + 1) * LD
+    S* B = reinterpret_cast<S*>(smem + Ls.B);
+    S* sW0 = reinterpret_cast<S*>(smem + Ls.w0);
+    S* sW1 = reinterpret_cast<S*>(smem + Ls.w1);
+    S* sW2 = reinterpret_cast<S*>(smem + Ls.w2);
+    S* sG = reinterpret_cast<S*>(smem + Ls.grow);
+    double* const sT0 = reinterpret_cast<double*>(smem + Ls.tab0);
+    double* const sT1 = reinterpret_cast<double*>(smem + Ls.tab1);
+    S* xfa = reinterpret_cast<S*>(smem + Ls.xfa);
+    S* xfb = reinterpret_cast<S*>(smem + Ls.xfb);
+    S* xba = reinterpret_cast<S*>(smem + Ls.xba);
+    S* xbb = reinterpret_cast<S*>(smem + Ls.xbb);
+    S* yf = reinterpret_cast<S*>(smem + Ls.yf);
+    S* yb = reinterpret_cast<S*>(smem + Ls.yb);
+    S* blkF = reinterpret_cast<S*>(smem + Ls.blkF);
+    S* blkB = reinterpret_cast<S*>(smem + Ls.blkB);
+    S* s_zin = reinterpret_cast<S*>(smem + Ls.zin);
+    S* s_xin = reinterpret_cast<S*>(smem + Ls.xin);
+    S* s_tot = reinterpret_cast<S*>(smem + Ls.tot);
+    const double* tabc = args.tabs + c.tab;
+    const TabLayout Lt = tab_layout(X, Y, T, c.Xp, kKindLine);
+    const double strike = 0.001 * (double)item.strike;  // strikes (:247)
+    const int steps = T > 1 ? T - 1 : 0;
+    const PV* piv = args.piv + c.piv;
+    const int64_t Y4 = round4(Y);
+    S* halo_prev = nullptr;  // bottom halo row of rank - 1
+    S* halo_next = nullptr;  // top halo row of rank + 1
+    if (clustered) {
+      cg::cluster_group cl = cg::this_cluster();
+      if (rank > 0) halo_prev = cl.map_shared_rank(A + (Ycs + 1) * LD, rank - 1);
+      if (rank < C - 1) halo_next = cl.map_shared_rank(A, rank + 1);
+    }
+
+    // The previous instance is done with every buffer, and -- across the
+    // cluster -- every neighbour has finished pushing its last halo rows into
+    // this CTA before they are re-initialised below.
+    if (clustered) cg::this_cluster().sync(); else __syncthreads();
+    // setPayoff (:46-47) on the block and the halo rows (zero at the global
+    // boundary and in the two padding columns)
+    for (int e = tid; e < (Ycs + 2) * LD; e += NT) {
+      const int r = e / LD, i = e - r * LD;
+      const bool boundary = (r == 0 && rank == 0) || (r == Ycs + 1 && rank == C - 1);
+      A[e] = (i < X && !boundary) ? (S)fmax(tabc[Lt.x + i] - strike, 0.0) : (S)0;
+    }
+    for (int e = tid; e < 3 * X; e += NT) {
+      const int k = e / X, i = e - k * X;
+      (k == 0 ? sW0 : k == 1 ? sW1 : sW2)[i] = (S)tabc[Lt.wcol + k * (int64_t)((X + 1) & ~1) + i];
+    }
+    for (int e = tid; e < 4 * Ycs; e += NT) sG[e] = (S)tabc[Lt.rowc + 4LL * r0 + e];
+
+    if (steps == 0) {
+      if (tid == 0 && c.yindex >= r0 && c.yindex < r0 + Ycs)
+        args.out[c.out + item.strike] = fmax(tabc[Lt.x + c.xindex] - strike, 0.0);
+      continue;
+    }
+    const unsigned piv_bytes = (unsigned)(Ycs * LD * (int)sizeof(S));  // a multiple of 16
+    const unsigned tab_bytes = (unsigned)(Ycs * 64);
+    auto issue_copies = [&](int k, double* tdst) {
+      if (tid == 0) {
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        mbar_expect_tx(bar, piv_bytes + tab_bytes);
+        bulk_g2s(B, piv + ((int64_t)k * Y4 + r0) * LD, piv_bytes, bar);
+        bulk_g2s(tdst, tabc + Lt.stab + ((int64_t)k * Y + r0) * 8, tab_bytes, bar);
+      }
+    };
+    issue_copies(steps - 1, (sc & 1) ? sT1 : sT0);
+
+    // X units u = warp + q * NW: rows rgx*32 + lane, columns chx*16 ..
+    int rgx[UPW], chx[UPW], jl[UPW];
+#pragma unroll
+    for (int q = 0; q < UPW; q++) {
+      const int u = warp + q * NW;
+      rgx[q] = u / Ls.CHx;
+      chx[q] = u - rgx[q] * Ls.CHx;
+      jl[q] = rgx[q] * 32 + lane;
+    }
+    // the two units of a warp fold their chunk prefixes in one pass when
+    // they lie on the same rows
+    const bool xchain = rgx[1] == rgx[0] && chx[1] > chx[0];
+    // Y unit u = warp: columns cg2*64 + 2*lane (+1), rows chy*16 ..
+    const int cg2 = warp / Ls.CHy, chy = warp - cg2 * Ls.CHy;
+    const int col0 = cg2 * 64 + 2 * lane;
+    // output lane: the column half and element holding myResult[myYindex, myXindex]
+    int out_h = -1, out_m = 0;
+    {
+      const int jy = c.yindex - r0 - chy * K;
+      if ((c.xindex & ~1) == col0 && jy >= 0 && jy < K) {
+        out_h = c.xindex & 1;
+        out_m = jy;
+      }
+    }
+
+    for (int s = 0; s < steps; s++, sc++) {
+      const int k = steps - 1 - s;
+      if (!mbar_wait(bar, phase)) atomicExch(args.err, 3);
+      phase ^= 1u;
+      if (clustered) cg::this_cluster().sync(); else __syncthreads();
+      const double* tb = (sc & 1) ? sT1 : sT0;
+      const S dt = (S)tabc[Lt.dtinv + k];
+
+      // -------- X sweep pass 1: explicitX + explicitY, forward recurrence (chunk-local) --------
+      S z[UPW][K], PQ[UPW][K];
+      {
+        S e[UPW], g0[UPW], g1[UPW], g2[UPW], Rl[UPW], rbp[UPW], zl[UPW], Pl[UPW];
+        typename V::T Rc[UPW];
+#pragma unroll
+        for (int q = 0; q < UPW; q++) {
+          const int ib = chx[q] * K;
+          const S* Arow = A + (jl[q] + 1) * LD;
+          e[q] = (S)tb[jl[q] * 8 + kSlotE];
+          g0[q] = sG[4 * jl[q]];
+          g1[q] = sG[4 * jl[q] + 1];
+          g2[q] = sG[4 * jl[q] + 2];
+          Rl[q] = ib > 0 ? Arow[ib - 1] : (S)0;
+          Rc[q] = V::ld(Arow + ib);
+          rbp[q] = ib > 0 ? B[jl[q] * LD + ib - 1] : (S)0;
+          zl[q] = 0;
+          Pl[q] = 1;
+        }
+#pragma unroll
+        for (int p = 0; p < K / 2; p++) {
+#pragma unroll
+          for (int q = 0; q < UPW; q++) {
+            const int i = chx[q] * K + 2 * p;
+            const S* Arow = A + (jl[q] + 1) * LD;
+            const auto Rn = V::ld(Arow + i + 2);   // columns i+2, i+3 (numX, numX+1 are zero)
+            const auto up = V::ld(Arow + i - LD);  // rows j-1 and j+1 (halo rows at the block edges)
+            const auto dn = V::ld(Arow + i + LD);
+            const auto w0 = V::ld(sW0 + i);
+            const auto w1 = V::ld(sW1 + i);
+            const auto w2 = V::ld(sW2 + i);
+            const auto rb = V::ld(B + jl[q] * LD + i);
+            {  // column i
+              const S v = g0[q] * up.x + g1[q] * Rc[q].x + g2[q] * dn.x;    // explicitY (:199)
+              const S sx = w0.x * Rl[q] + w1.x * Rc[q].x + w2.x * Rc[q].y;   // explicitX / (0.5 e)
+              const S u = e[q] * sx + (dt * Rc[q].x + v);                    // :195-200
+              const S mult = (e[q] * w0.x) * rbp[q];                         // -a_i / b'_{i-1}
+              zl[q] = u + mult * zl[q];
+              Pl[q] = mult * Pl[q];
+              z[q][2 * p] = zl[q];
+              PQ[q][2 * p] = Pl[q];
+            }
+            {  // column i + 1
+              const S v = g0[q] * up.y + g1[q] * Rc[q].y + g2[q] * dn.y;
+              const S sx = w0.y * Rc[q].x + w1.y * Rc[q].y + w2.y * Rn.x;
+              const S u = e[q] * sx + (dt * Rc[q].y + v);
+              const S mult = (e[q] * w0.y) * rb.x;
+              zl[q] = u + mult * zl[q];
+              Pl[q] = mult * Pl[q];
+              z[q][2 * p + 1] = zl[q];
+              PQ[q][2 * p + 1] = Pl[q];
+            }
+            rbp[q] = rb.y;
+            Rl[q] = Rc[q].y;
+            Rc[q] = Rn;
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < UPW; q++) {
+          const int u = warp + q * NW;
+          xfa[u * 32 + lane] = zl[q];
+          xfb[u * 32 + lane] = Pl[q];
+        }
+      }
+      __syncthreads();
+      // -------- pass 2: forward fix-up, backward recurrence (chunk-local) --------
+      {
+        S zin[UPW], xl[UPW], Ql[UPW], e[UPW];
+        {
+          S a = 0;
+          int c2 = 0;
+          for (; c2 < chx[0]; c2++) {
+            const int u = rgx[0] * Ls.CHx + c2;
+            a = xfa[u * 32 + lane] + xfb[u * 32 + lane] * a;
+          }
+          zin[0] = a;
+          if (!xchain) {
+            a = 0;
+            c2 = 0;
+          }
+          for (; c2 < chx[1]; c2++) {
+            const int u = rgx[1] * Ls.CHx + c2;
+            a = xfa[u * 32 + lane] + xfb[u * 32 + lane] * a;
+          }
+          zin[1] = a;
+        }
+#pragma unroll
+        for (int q = 0; q < UPW; q++) {
+          xl[q] = 0;
+          Ql[q] = 1;
+          e[q] = (S)tb[jl[q] * 8 + kSlotE];
+        }
+#pragma unroll
+        for (int p = K / 2 - 1; p >= 0; p--) {
+#pragma unroll
+          for (int q = 0; q < UPW; q++) {
+            const int i = chx[q] * K + 2 * p;
+            const auto rb = V::ld(B + jl[q] * LD + i);
+            const auto w2 = V::ld(sW2 + i);
+            {  // column i + 1
+              const S zz = z[q][2 * p + 1] + PQ[q][2 * p + 1] * zin[q];
+              const S aR = e[q] * w2.y;
+              xl[q] = rb.y * (zz + aR * xl[q]);  // x_i = (z_i - c_i x_{i+1}) / b'_i
+              Ql[q] = (aR * rb.y) * Ql[q];
+              z[q][2 * p + 1] = xl[q];
+              PQ[q][2 * p + 1] = Ql[q];
+            }
+            {  // column i
+              const S zz = z[q][2 * p] + PQ[q][2 * p] * zin[q];
+              const S aR = e[q] * w2.x;
+              xl[q] = rb.x * (zz + aR * xl[q]);
+              Ql[q] = (aR * rb.x) * Ql[q];
+              z[q][2 * p] = xl[q];
+              PQ[q][2 * p] = Ql[q];
+            }
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < UPW; q++) {
+          const int u = warp + q * NW;
+          xba[u * 32 + lane] = xl[q];
+          xbb[u * 32 + lane] = Ql[q];
+        }
+      }
+      __syncthreads();
+      // -------- pass 3: backward fix-up; dtInv * u goes to B (:205) --------
+      {
+        S xin[UPW];
+        {
+          S a = 0;
+          int c2 = Ls.CHx - 1;
+          for (; c2 > chx[1]; c2--) {
+            const int u = rgx[1] * Ls.CHx + c2;
+            a = xba[u * 32 + lane] + xbb[u * 32 + lane] * a;
+          }
+          xin[1] = a;
+          if (!xchain) {
+            a = 0;
+            c2 = Ls.CHx - 1;
+          }
+          for (; c2 > chx[0]; c2--) {
+            const int u = rgx[0] * Ls.CHx + c2;
+            a = xba[u * 32 + lane] + xbb[u * 32 + lane] * a;
+          }
+          xin[0] = a;
+        }
+#pragma unroll
+        for (int p = 0; p < K / 2; p++) {
+#pragma unroll
+          for (int q = 0; q < UPW; q++) {
+            const int i = chx[q] * K + 2 * p;
+            V::st(B + jl[q] * LD + i, dt * (z[q][2 * p] + PQ[q][2 * p] * xin[q]),
+                  dt * (z[q][2 * p + 1] + PQ[q][2 * p + 1] * xin[q]));
+          }
+        }
+      }
+      __syncthreads();
+
+      // -------- Y sweep: lane = columns col0, col0 + 1 --------
+      S y[2][K];
+      {
+        S zz0 = 0, zz1 = 0;
+        const int j0 = chy * K;
+        auto Ru = V::ld(A + j0 * LD + col0);        // row j0 - 1 (halo row at the block edge)
+        auto Rm = V::ld(A + (j0 + 1) * LD + col0);  // row j0
+#pragma unroll
+        for (int m = 0; m < K; m++) {
+          const int j = j0 + m;
+          const auto Rd = V::ld(A + (j + 2) * LD + col0);  // row j + 1
+          const auto g01 = V::ld(sG + 4 * j);
+          const S g2 = sG[4 * j + 2];
+          const S my = (S)tb[j * 8 + kSlotMY];
+          const auto bx = V::ld(B + j * LD + col0);
+          const S v0 = g01.x * Ru.x + g01.y * Rm.x + g2 * Rd.x;  // explicitY (:199)
+          const S v1 = g01.x * Ru.y + g01.y * Rm.y + g2 * Rd.y;
+          zz0 = (bx.x - (S)0.5 * v0) + my * zz0;                   // :205, forward recurrence
+          zz1 = (bx.y - (S)0.5 * v1) + my * zz1;
+          y[0][m] = zz0;
+          y[1][m] = zz1;
+          Ru = Rm;
+          Rm = Rd;
+        }
+        V::st(yf + warp * 64 + 2 * lane, zz0, zz1);
+      }
+      __syncthreads();
+      if (s + 1 < steps) issue_copies(k - 1, ((sc + 1) & 1) ? sT1 : sT0);
+      if (clustered) {
+        for (int col = tid; col < X; col += NT) {
+          const int g = col >> 6, w = col & 63;
+          S a = 0;
+          for (int c2 = 0; c2 < Ls.CHy; c2++)
+            a = yf[(g * Ls.CHy + c2) * 64 + w] + (S)tb[(c2 * K + K - 1) * 8 + kSlotCP] * a;
+          blkF[col] = a;
+        }
+        if (tid == 0) {
+          S b = 1;
+          for (int c2 = 0; c2 < Ls.CHy; c2++) b = (S)tb[(c2 * K + K - 1) * 8 + kSlotCP] * b;
+          s_tot[0] = b;
+        }
+        cg::cluster_group cl = cg::this_cluster();
+        cl.sync();
+        for (int col = tid; col < X; col += NT) {
+          S zv = 0;
+          for (int r = 0; r < rank; r++) {
+            const S* rf = cl.map_shared_rank(blkF, r);
+            const S* rt = cl.map_shared_rank(s_tot, r);
+            zv = rf[col] + rt[0] * zv;
+          }
+          s_zin[col] = zv;
+        }
+        __syncthreads();
+      }
+      {
+        S zin0 = 0, zin1 = 0;
+        if (clustered) {
+          const auto zi = V::ld(s_zin + col0);
+          zin0 = zi.x;
+          zin1 = zi.y;
+        }
+        for (int c2 = 0; c2 < chy; c2++) {
+          const auto a = V::ld(yf + (cg2 * Ls.CHy + c2) * 64 + 2 * lane);
+          const S cp = (S)tb[(c2 * K + K - 1) * 8 + kSlotCP];
+          zin0 = a.x + cp * zin0;
+          zin1 = a.y + cp * zin1;
+        }
+        S xx0 = 0, xx1 = 0;
+#pragma unroll
+        for (int m = K - 1; m >= 0; m--) {
+          const int j = chy * K + m;
+          const double2 nr = *reinterpret_cast<const double2*>(tb + j * 8 + kSlotNY);  // nY, 1/b'
+          const S cp = (S)tb[j * 8 + kSlotCP];
+          const S zv0 = y[0][m] + cp * zin0;
+          const S zv1 = y[1][m] + cp * zin1;
+          xx0 = (S)nr.y * zv0 + (S)nr.x * xx0;
+          xx1 = (S)nr.y * zv1 + (S)nr.x * xx1;
+          y[0][m] = xx0;
+          y[1][m] = xx1;
+        }
+        V::st(yb + warp * 64 + 2 * lane, xx0, xx1);
+      }
+      __syncthreads();
+      if (clustered) {
+        for (int col = tid; col < X; col += NT) {
+          const int g = col >> 6, w = col & 63;
+          S a = 0;
+          for (int c2 = Ls.CHy - 1; c2 >= 0; c2--)
+            a = yb[(g * Ls.CHy + c2) * 64 + w] + (S)tb[(c2 * K) * 8 + kSlotCQ] * a;
+          blkB[col] = a;
+        }
+        if (tid == 0) {
+          S b = 1;
+          for (int c2 = Ls.CHy - 1; c2 >= 0; c2--) b = (S)tb[(c2 * K) * 8 + kSlotCQ] * b;
+          s_tot[1] = b;
+        }
+        cg::cluster_group cl = cg::this_cluster();
+        cl.sync();
+        for (int col = tid; col < X; col += NT) {
+          S xv = 0;
+          for (int r = C - 1; r > rank; r--) {
+            const S* rb_ = cl.map_shared_rank(blkB, r);
+            const S* rt = cl.map_shared_rank(s_tot, r);
+            xv = rb_[col] + rt[1] * xv;
+          }
+          s_xin[col] = xv;
+        }
+        __syncthreads();
+      }
+      {
+        S xin0 = 0, xin1 = 0;
+        if (clustered) {
+          const auto xi = V::ld(s_xin + col0);
+          xin0 = xi.x;
+          xin1 = xi.y;
+        }
+        for (int c2 = Ls.CHy - 1; c2 > chy; c2--) {
+          const auto b = V::ld(yb + (cg2 * Ls.CHy + c2) * 64 + 2 * lane);
+          const S cq = (S)tb[(c2 * K) * 8 + kSlotCQ];
+          xin0 = b.x + cq * xin0;
+          xin1 = b.y + cq * xin1;
+        }
+#pragma unroll
+        for (int m = 0; m < K; m++) {
+          const int j = chy * K + m;
+          const S cq = (S)tb[j * 8 + kSlotCQ];
+          const S xv0 = y[0][m] + cq * xin0;
+          const S xv1 = y[1][m] + cq * xin1;
+          y[0][m] = xv0;
+          y[1][m] = xv1;
+          V::st(A + (j + 1) * LD + col0, xv0, xv1);
+        }
+        // halo rows of the cluster neighbours, and the price on the last step
+        if (halo_prev && chy == 0) V::st(halo_prev + col0, y[0][0], y[1][0]);
+        if (halo_next && chy == Ls.CHy - 1) V::st(halo_next + col0, y[0][K - 1], y[1][K - 1]);
+        if (s == steps - 1 && out_h >= 0) {
+          S pv = 0;
+#pragma unroll
+          for (int m = 0; m < K; m++)
+            if (m == out_m) pv = out_h ? y[1][m] : y[0][m];
+          args.out[c.out + item.strike] = (double)pv;  // myResult[myYindex, myXindex]
+        }
+      }
+    }
+  }
+  if (clustered) cg::this_cluster().sync();
+}
+
+}  // namespace lvc

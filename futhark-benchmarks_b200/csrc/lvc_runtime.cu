@@ -33,6 +33,7 @@
 #include "LocVolCalib.h"
 #include "lvc_kernels.cuh"
 #include "lvc_line.cuh"
+#include "lvc_pair.cuh"
 #include "lvc_probe.cuh"
 
 using namespace lvc;
@@ -173,6 +174,8 @@ struct Config {
   int kind, NT, KX, C;
   bool gstate;
   bool full = false;
+  bool pair = false;  // paired line kernel
+  int ld = 0;         // line family: row stride of the pivot rows and the on-chip grid
   int Ycs;
   size_t smem_bytes;
   int64_t grid_elems;
@@ -189,6 +192,7 @@ struct Launch {
   int kind, NT, KX, C;
   bool gstate;
   bool full = false;
+  bool pair = false;
   int item_off, n_items, grid;
   size_t smem_bytes;
   int64_t gstate_per_cta;  // elements of the state type
@@ -314,7 +318,13 @@ template <typename S, typename PV>
 using RbFn = void (*)(RollbackArgs<S, PV>);
 
 template <typename S, typename PV>
-RbFn<S, PV> rollback_fn(int kind, int NT, int KX, bool gs, bool full = false) {
+RbFn<S, PV> rollback_fn(int kind, int NT, int KX, bool gs, bool full = false, bool pair = false) {
+  if (kind == kKindLine && pair) {
+    if (NT == 64) return lvc_line_pair_kernel<S, PV, 64>;
+    if (NT == 128) return lvc_line_pair_kernel<S, PV, 128>;
+    if (NT == 256) return lvc_line_pair_kernel<S, PV, 256>;
+    return nullptr;
+  }
   if (kind == kKindLine && full) {
     if (NT == 32) return lvc_line_full_kernel<S, PV, 32, 2>;
     if (NT == 64) return lvc_line_full_kernel<S, PV, 64, 2>;
@@ -361,7 +371,34 @@ bool line_full_cfg(int X, int Y, int C, int max_smem, Config& cf) {
   if (F.Ux != units || F.Uy != units || F.total > max_smem) return false;
   cf.kind = kKindLine;
   cf.full = true;
+  cf.pair = false;
+  cf.ld = line_ld(X);
   cf.NT = 16 * units;  // 32 lanes x units / 2 units per warp
+  cf.KX = kLineK;
+  cf.C = C;
+  cf.gstate = false;
+  cf.Ycs = Ycs;
+  cf.smem_bytes = (size_t)F.total;
+  cf.grid_elems = 0;
+  return true;
+}
+
+// Paired line kernel: full tiles with numX % 64 == 0; two X units and one Y
+// unit (64 columns) per warp.
+template <typename S>
+bool line_pair_cfg(int X, int Y, int C, int max_smem, Config& cf) {
+  if (X > 256 || X % 64 || Y % C || (Y / C) % 32) return false;
+  const int Ycs = Y / C;
+  const int units = X * Ycs / 512;  // X units of 32 rows x 16 columns
+  if (units != 4 && units != 8 && units != 16) return false;  // NT = 16 * units instantiated
+  const int NW = units / 2;
+  const PairLayout F = pair_layout<S>(X, Ycs);
+  if (F.Ux != units || F.Uy != NW || F.total > max_smem) return false;
+  cf.kind = kKindLine;
+  cf.full = false;
+  cf.pair = true;
+  cf.ld = pair_ld(X);
+  cf.NT = 32 * NW;
   cf.KX = kLineK;
   cf.C = C;
   cf.gstate = false;
@@ -386,6 +423,8 @@ bool line_generic_cfg(int X, int Y, int C, int max_smem, Config& cf) {
   if (L.total > max_smem) return false;
   cf.kind = kKindLine;
   cf.full = false;
+  cf.pair = false;
+  cf.ld = line_ld(X);
   cf.NT = NT;
   cf.KX = kLineK;
   cf.C = C;
@@ -407,6 +446,8 @@ bool chunk_cfg(int X, int Y, int C, int max_smem, bool gstate, Config& cf) {
   if ((size_t)L.total * sizeof(S) > (size_t)max_smem) return false;
   cf.kind = kKindChunk;
   cf.full = false;
+  cf.pair = false;
+  cf.ld = 0;
   cf.KX = Xp <= 256 ? 8 : 16;
   cf.gstate = gstate;
   cf.C = C;
@@ -419,12 +460,14 @@ bool chunk_cfg(int X, int Y, int C, int max_smem, bool gstate, Config& cf) {
   return true;
 }
 
-// Built-in choice: the smallest cluster the line family fits in (full tiles
-// first), else the chunk family on chip, else the chunk family on HBM.
+// Built-in choice: the smallest cluster the line family fits in (paired
+// kernel, then full tiles, then any sizes), else the chunk family on chip,
+// else the chunk family on HBM.
 template <typename S>
 Config default_config(int X, int Y, int max_smem) {
   Config cf;
   for (int C = 1; C <= kMaxCluster; C *= 2) {
+    if (line_pair_cfg<S>(X, Y, C, max_smem, cf)) return cf;
     if (line_full_cfg<S>(X, Y, C, max_smem, cf)) return cf;
     if (line_generic_cfg<S>(X, Y, C, max_smem, cf)) return cf;
   }
@@ -443,6 +486,7 @@ std::vector<Config> enum_configs(int X, int Y, int max_smem) {
   std::vector<Config> v;
   Config cf;
   for (int C = 1; C <= kMaxCluster; C *= 2) {
+    if (line_pair_cfg<S>(X, Y, C, max_smem, cf)) v.push_back(cf);
     if (line_full_cfg<S>(X, Y, C, max_smem, cf)) v.push_back(cf);
     if (line_generic_cfg<S>(X, Y, C, max_smem, cf) && (C == 1 || cf.Ycs >= 16)) v.push_back(cf);
   }
@@ -454,7 +498,8 @@ std::vector<Config> enum_configs(int X, int Y, int max_smem) {
 }
 
 int family_of(const Config& c) {
-  return c.kind == kKindChunk ? LVC_FAMILY_CHUNK : (c.full ? LVC_FAMILY_LINE_FULL : LVC_FAMILY_LINE);
+  if (c.kind == kKindChunk) return LVC_FAMILY_CHUNK;
+  return c.pair ? LVC_FAMILY_LINE_PAIR : c.full ? LVC_FAMILY_LINE_FULL : LVC_FAMILY_LINE;
 }
 
 bool same_shape(const Config& a, const Config& b) {
@@ -477,7 +522,7 @@ Config choose_config(const futhark_context* ctx, int X, int Y) {
 
 template <typename S, typename PV>
 int prepare_launch(futhark_context* ctx, Launch& L, int max_sms = 0) {
-  RbFn<S, PV> fn = rollback_fn<S, PV>(L.kind, L.NT, L.KX, L.gstate, L.full);
+  RbFn<S, PV> fn = rollback_fn<S, PV>(L.kind, L.NT, L.KX, L.gstate, L.full, L.pair);
   if (!fn) return set_error(ctx, FUTHARK_PROGRAM_ERROR, "no rollback kernel for this configuration");
   // Several launch classes may share one kernel instantiation with different
   // shared-memory sizes: allow the device maximum once for all of them.
@@ -548,7 +593,7 @@ cudaError_t launch_rollback(lvc_plan* P, const Launch& L, cudaStream_t s) {
     cfg.attrs = &attr;
     cfg.numAttrs = 1;
   }
-  return cudaLaunchKernelEx(&cfg, rollback_fn<S, PV>(L.kind, L.NT, L.KX, L.gstate, L.full), a);
+  return cudaLaunchKernelEx(&cfg, rollback_fn<S, PV>(L.kind, L.NT, L.KX, L.gstate, L.full, L.pair), a);
 }
 
 // Enqueue one run of a plan.  `ev` (optional) receives a start/stop event
@@ -634,8 +679,8 @@ int plan_build(futhark_context* ctx, const lvc_calibration* cs, int n, lvc_plan*
   P->params.assign(cs, cs + n);
   P->calibs.resize(n);
   P->row_start.assign(n + 1, 0);
-  std::map<std::tuple<int, int, int, int, bool, bool>, std::vector<std::pair<int64_t, Item>>> classes;
-  std::map<std::tuple<int, int, int, int, bool, bool>, Config> class_cfg;
+  std::map<std::tuple<int, int, int, int, bool, bool, bool>, std::vector<std::pair<int64_t, Item>>> classes;
+  std::map<std::tuple<int, int, int, int, bool, bool, bool>, Config> class_cfg;
   int64_t tab_off = 0, piv_off = 0, out_off = 0;
   for (int i = 0; i < n; i++) {
     const lvc_calibration& c = cs[i];
@@ -650,16 +695,17 @@ int plan_build(futhark_context* ctx, const lvc_calibration* cs, int n, lvc_plan*
     d.C = cf.C;
     d.kind = cf.kind;
     d.Ycs = cf.Ycs;
-    d.pad0 = d.pad1 = 0;
+    d.ld = cf.ld;
+    d.pad1 = 0;
     fill_scalars(d, c);
     d.tab = tab_off;
     tab_off += al2(tab_layout(c.numX, c.numY, c.numT, d.Xp, d.kind).total);
     d.piv = piv_off;
-    piv_off += (piv_elems(c.numX, c.numY, c.numT, d.Xp, d.kind) + 3) & ~int64_t(3);
+    piv_off += (piv_elems(c.numX, c.numY, c.numT, d.Xp, d.kind, d.ld) + 3) & ~int64_t(3);
     d.out = out_off;
     out_off += c.outer;
     P->row_start[i + 1] = P->row_start[i] + (int64_t)(c.numT > 1 ? c.numT - 1 : 0) * c.numY;
-    const auto key = std::make_tuple(cf.kind, cf.NT, cf.KX, cf.C, cf.gstate, cf.full);
+    const auto key = std::make_tuple(cf.kind, cf.NT, cf.KX, cf.C, cf.gstate, cf.full, cf.pair);
     auto& cls = classes[key];
     auto it = class_cfg.find(key);
     if (it == class_cfg.end()) {
@@ -687,6 +733,7 @@ int plan_build(futhark_context* ctx, const lvc_calibration* cs, int n, lvc_plan*
     Launch L;
     L.kind = cf.kind;
     L.full = cf.full;
+    L.pair = cf.pair;
     L.NT = cf.NT;
     L.KX = cf.KX;
     L.C = cf.C;
@@ -1248,6 +1295,7 @@ int lvc_context_set_tuning_param(struct futhark_context* ctx, const char* param_
 namespace {
 
 const char* family_name(int fam, bool gstate) {
+  if (fam == LVC_FAMILY_LINE_PAIR) return "line_pair";
   if (fam == LVC_FAMILY_LINE_FULL) return "line_full";
   if (fam == LVC_FAMILY_LINE) return "line";
   return gstate ? "chunk_hbm" : "chunk";
@@ -1498,9 +1546,12 @@ int lvc_tuning_load(struct futhark_context* ctx, const char* path) {
       lvc_shape sh{};
       sh.cluster = C;
       const std::string fs(fam);
-      sh.family = fs == "line_full" ? LVC_FAMILY_LINE_FULL : fs == "line" ? LVC_FAMILY_LINE : LVC_FAMILY_CHUNK;
+      sh.family = fs == "line_pair"   ? LVC_FAMILY_LINE_PAIR
+                  : fs == "line_full" ? LVC_FAMILY_LINE_FULL
+                  : fs == "line"      ? LVC_FAMILY_LINE
+                                      : LVC_FAMILY_CHUNK;
       sh.hbm_state = fs == "chunk_hbm" ? 1 : 0;
-      const bool known = fs == "line_full" || fs == "line" || fs == "chunk" || fs == "chunk_hbm";
+      const bool known = fs == "line_pair" || fs == "line_full" || fs == "line" || fs == "chunk" || fs == "chunk_hbm";
       const int p = !strcmp(prec, "f64") ? LVC_F64 : !strcmp(prec, "f32state") ? LVC_F32_STATE : -1;
       if (!known || p < 0) rc = 1;
       else rc = lvc_tuning_set(ctx, X, Y, p, &sh);
@@ -1641,12 +1692,13 @@ extern "C" int lvc_entry_main_f64_noalloc(struct futhark_context* ctx, double* p
   d.C = cf.C;
   d.kind = cf.kind;
   d.Ycs = cf.Ycs;
+  d.ld = cf.ld;
   fill_scalars(d, c);
   d.tab = 0;
   d.piv = 0;
   d.out = 0;
   const int64_t tab_elems = al2(tab_layout(numX, numY, numT, d.Xp, d.kind).total);
-  const int64_t piv_n = (piv_elems(numX, numY, numT, d.Xp, d.kind) + 3) & ~int64_t(3);
+  const int64_t piv_n = (piv_elems(numX, numY, numT, d.Xp, d.kind, d.ld) + 3) & ~int64_t(3);
   // scratch carve-up
   const size_t o_calib = 0;
   const size_t o_err = up256(o_calib + sizeof(CalibDev));
@@ -1691,6 +1743,7 @@ extern "C" int lvc_entry_main_f64_noalloc(struct futhark_context* ctx, double* p
     Launch L;
     L.kind = cf.kind;
     L.full = cf.full;
+    L.pair = cf.pair;
     L.NT = cf.NT;
     L.KX = cf.KX;
     L.C = cf.C;
@@ -1727,7 +1780,7 @@ extern "C" int lvc_entry_main_f64_noalloc(struct futhark_context* ctx, double* p
       cfg.attrs = &attr;
       cfg.numAttrs = 1;
     }
-    LVC_CUDA(ctx, cudaLaunchKernelEx(&cfg, rollback_fn<double, double>(L.kind, L.NT, L.KX, false, L.full), a));
+    LVC_CUDA(ctx, cudaLaunchKernelEx(&cfg, rollback_fn<double, double>(L.kind, L.NT, L.KX, false, L.full, L.pair), a));
   }
   int h = 0;
   LVC_CUDA(ctx, cudaMemcpyAsync(&h, d_err, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -1855,7 +1908,7 @@ size_t request_bytes(const futhark_context* ctx, const lvc_calibration& c, int p
   const int Xp = std::max(8, pow2ceil(c.numX));
   const size_t ps = f64 ? 8 : 4;
   size_t b = 8 * (size_t)al2(tab_layout(c.numX, c.numY, c.numT, Xp, cf.kind).total);
-  b += ps * (size_t)(piv_elems(c.numX, c.numY, c.numT, Xp, cf.kind) + 4);
+  b += ps * (size_t)(piv_elems(c.numX, c.numY, c.numT, Xp, cf.kind, cf.ld) + 4);
   b += 16 * (size_t)c.outer + 4096;
   if (cf.gstate) b += ps * (size_t)cf.grid_elems * 148 * 4;
   return b + 8 * 256;  // allocation rounding
