@@ -176,68 +176,102 @@ __global__ void __launch_bounds__(256) lvc_setup_kernel(const CalibDev* __restri
 }
 
 // ---------------------------------------------------------------------------
-// pivot kernel: one thread per (calibration, step, row); the sequential pivot
-// recurrence of one X-direction system, written as 1/b'_i.
+// pivot kernel: one lane per (calibration, step, row) runs the sequential pivot
+// recurrence of one X-direction system, written as 1/b'_i.  A warp owns 32
+// consecutive rows and goes through them 32 columns at a time: every lane
+// puts its 32 pivots in a shared tile, then the warp writes the tile out one
+// row at a time, 32 consecutive columns per store, so every row leaves in
+// whole 32-byte sectors (a store per lane per column would touch 32 rows per
+// instruction and leave partly written sectors to the L2).
 // ---------------------------------------------------------------------------
+constexpr int kPivotWarps = 4;  // warps per CTA (128 threads)
+
 template <typename PV>
 __global__ void __launch_bounds__(128) lvc_pivot_kernel(const CalibDev* __restrict__ calibs,
                                                         const int64_t* __restrict__ row_start,
                                                         int ncal, const double* __restrict__ tabs,
                                                         PV* __restrict__ piv) {
+  __shared__ double tile[kPivotWarps][32][33];
+  __shared__ PV* rowp[kPivotWarps][32];
+  __shared__ int rowx[kPivotWarps][32], rowld[kPivotWarps][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int64_t total = row_start[ncal];
-  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < total;
-       r += (int64_t)gridDim.x * blockDim.x) {
-    int lo = 0, hi = ncal - 1;  // last c with row_start[c] <= r
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (row_start[mid] <= r) lo = mid; else hi = mid - 1;
-    }
-    const CalibDev c = calibs[lo];
-    const int X = c.numX, Y = c.numY, Xp = c.Xp;
-    const TabLayout L = tab_layout(X, Y, c.numT, Xp, c.kind);
-    const int64_t local = r - row_start[lo];
-    const int k = (int)(local / Y), j = (int)(local % Y);
-    const double* tab = tabs + c.tab;
-    const double dt = tab[L.dtinv + k];
-    double rb_prev = 0.0, c_prev = 0.0;
-    if (c.kind == kKindLine) {
-      // b'_i = (dt - e W1_i) - (e W0_i)(e W2_{i-1}) / b'_{i-1}, stored as rows of
-      // stride LD (the line kernel's shared-memory image)
-      const double e = tab[L.stab + ((int64_t)k * Y + j) * 8];
-      const int LDl = c.ld;
-      PV* o = piv + c.piv + ((int64_t)k * round4(Y) + j) * LDl;
-      for (int i = X; i < LDl; i++) o[i] = (PV)0;
-      const double* W0 = tab + L.wcol;
-      const double* W1 = W0 + L.xa;
-      const double* W2 = W1 + L.xa;
-      for (int i = 0; i < X; i++) {
-        const double a = -(e * W0[i]);
-        const double b = dt - e * W1[i];
-        const double cc = -(e * W2[i]);
-        const double bp = (i == 0) ? b : b - a * c_prev * rb_prev;
-        const double rb = 1.0 / bp;
-        o[i] = (PV)rb;
-        rb_prev = rb;
-        c_prev = cc;
+  const int64_t ngroups = (total + 31) / 32;
+  for (int64_t g = (int64_t)blockIdx.x * kPivotWarps + w; g < ngroups; g += (int64_t)gridDim.x * kPivotWarps) {
+    const int64_t r = g * 32 + lane;
+    int X = 0, LDr = 0;
+    PV* o = nullptr;
+    bool line = false;
+    double e = 0.0, dt = 0.0;
+    const double* tab = tabs;
+    TabLayout L{};
+    if (r < total) {
+      int lo = 0, hi = ncal - 1;  // last c with row_start[c] <= r
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (row_start[mid] <= r) lo = mid; else hi = mid - 1;
       }
-      continue;
+      const CalibDev c = calibs[lo];
+      const int Y = c.numY;
+      X = c.numX;
+      L = tab_layout(X, Y, c.numT, c.Xp, c.kind);
+      const int64_t local = r - row_start[lo];
+      const int k = (int)(local / Y), j = (int)(local % Y);
+      tab = tabs + c.tab;
+      dt = tab[L.dtinv + k];
+      line = c.kind == kKindLine;
+      if (line) {
+        // rows of stride ld: the line kernels' shared-memory image
+        e = tab[L.stab + ((int64_t)k * Y + j) * 8];
+        LDr = c.ld;
+        o = piv + c.piv + ((int64_t)k * round4(Y) + j) * LDr;
+      } else {
+        e = tab[L.eyt + (int64_t)k * L.eyt_ld + j];
+        LDr = c.Xp;
+        o = piv + c.piv + ((int64_t)k * Y + j) * LDr;
+      }
     }
-    const double e = tab[L.eyt + (int64_t)k * L.eyt_ld + j];
-    PV* o = piv + c.piv + ((int64_t)k * Y + j) * Xp;
-    for (int i = 0; i < X; i++) {
-      const double2 c01 = *reinterpret_cast<const double2*>(tab + L.colc + 4LL * i);
-      const double2 c23 = *reinterpret_cast<const double2*>(tab + L.colc + 4LL * i + 2);
-      const double var = c01.x * e;
-      const double a = -(0.5 * (var * c01.y));
-      const double b = dt - 0.5 * (var * c23.x);
-      const double cc = -(0.5 * (var * c23.y));
-      const double bp = (i == 0) ? b : b - a * c_prev * rb_prev;
-      const double rb = 1.0 / bp;
-      o[i] = (PV)rb;
-      rb_prev = rb;
-      c_prev = cc;
+    rowp[w][lane] = o;
+    rowx[w][lane] = X;
+    rowld[w][lane] = LDr;
+    const int maxld = __reduce_max_sync(0xffffffffu, (unsigned)LDr);
+    __syncwarp();
+    double rb_prev = 0.0, c_prev = 0.0;
+    for (int c0 = 0; c0 < maxld; c0 += 32) {
+      for (int m = 0; m < 32; m++) {
+        const int i = c0 + m;
+        double rb = 0.0;
+        if (i < X) {
+          double a, b, cc;
+          if (line) {
+            // b'_i = (dt - e W1_i) - (e W0_i)(e W2_{i-1}) / b'_{i-1}
+            const double* W0 = tab + L.wcol;
+            a = -(e * W0[i]);
+            b = dt - e * W0[L.xa + i];
+            cc = -(e * W0[2 * L.xa + i]);
+          } else {
+            const double2 c01 = *reinterpret_cast<const double2*>(tab + L.colc + 4LL * i);
+            const double2 c23 = *reinterpret_cast<const double2*>(tab + L.colc + 4LL * i + 2);
+            const double var = c01.x * e;
+            a = -(0.5 * (var * c01.y));
+            b = dt - 0.5 * (var * c23.x);
+            cc = -(0.5 * (var * c23.y));
+          }
+          const double bp = (i == 0) ? b : b - a * c_prev * rb_prev;
+          rb = 1.0 / bp;
+          rb_prev = rb;
+          c_prev = cc;
+        }
+        tile[w][lane][m] = rb;
+      }
+      __syncwarp();
+      for (int rr = 0; rr < 32; rr++) {
+        PV* orow = rowp[w][rr];
+        const int i = c0 + lane;
+        if (orow && i < rowld[w][rr]) orow[i] = (PV)(i < rowx[w][rr] ? tile[w][rr][lane] : 0.0);
+      }
+      __syncwarp();
     }
-    for (int i = X; i < Xp; i++) o[i] = (PV)0;
   }
 }
 

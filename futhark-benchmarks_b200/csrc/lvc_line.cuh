@@ -94,10 +94,14 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
       : "memory");
   return done != 0;
 }
-// Bounded wait: gives up after ~2^22 polls (each poll may suspend the thread
-// for a while); the caller flags an error instead of hanging the GPU.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
-  for (int i = 0; i < (1 << 22); i++)
+// Bounded wait: gives up after `limit` polls (each poll may suspend the
+// thread for a while); the caller flags an error instead of hanging the GPU.
+// After a first timeout the kernels pass a short limit for the rest of the
+// item, so a copy that never lands costs one long wait, not one per step.
+constexpr int kWaitPolls = 1 << 22;
+constexpr int kWaitPollsAfterTimeout = 64;
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, int limit = kWaitPolls) {
+  for (int i = 0; i < limit; i++)
     if (mbar_try_wait(bar, parity)) return true;
   return false;
 }
@@ -231,9 +235,13 @@ __global__ void __launch_bounds__(NT, (NT >= 512 ? 1 : 512 / NT)) lvc_line_kerne
       return g0 * up + g1 * Rc + g2 * dn;
     };
 
+    bool timed_out = false;  // a bulk-copy wait of this item gave up
     for (int s = 0; s < steps; s++, sc++) {
       const int k = steps - 1 - s;  // reverse (zip (init tl) (tail tl))  (:217)
-      if (!mbar_wait(bar, phase)) atomicExch(args.err, 3);
+      if (!mbar_wait(bar, phase, timed_out ? kWaitPollsAfterTimeout : kWaitPolls)) {
+        timed_out = true;
+        atomicExch(args.err, 3);
+      }
       phase ^= 1u;
       if (clustered) cg::this_cluster().sync(); else __syncthreads();
       const double* tb = sT[sc & 1];
@@ -627,9 +635,13 @@ __global__ void __launch_bounds__(NT, (FullMinBlocks<NT>::v)) lvc_line_full_kern
       }
     }
 
+    bool timed_out = false;  // a bulk-copy wait of this item gave up
     for (int s = 0; s < steps; s++, sc++) {
       const int k = steps - 1 - s;
-      if (!mbar_wait(bar, phase)) atomicExch(args.err, 3);
+      if (!mbar_wait(bar, phase, timed_out ? kWaitPollsAfterTimeout : kWaitPolls)) {
+        timed_out = true;
+        atomicExch(args.err, 3);
+      }
       phase ^= 1u;
       if (clustered) cg::this_cluster().sync(); else __syncthreads();
       const double* tb = sT[sc & 1];

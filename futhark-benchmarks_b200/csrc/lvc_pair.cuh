@@ -25,7 +25,7 @@ namespace lvc {
 
 struct PairLayout {
   int LD, Ycs, CHx, Ux, CG2, CHy, Uy;
-  int bar, A, B, w0, w1, w2, grow, tab0, tab1, xfa, xfb, xba, xbb, yf, yb, blkF, blkB, zin, xin, tot, total;
+  int bar, A, B, w0, w1, w2, grow, gx, ex, tab0, tab1, xfa, xfb, xba, xbb, yf, yb, blkF, blkB, zin, xin, tot, total;
 };
 
 // Byte offsets of the shared-memory buffers.
@@ -48,7 +48,9 @@ LVC_HD PairLayout pair_layout(int X, int Ycs) {
   L.w0 = o; o += up(X * s);               // W_k(i), planar
   L.w1 = o; o += up(X * s);
   L.w2 = o; o += up(X * s);
-  L.grow = o; o += up(4 * Ycs * s);
+  L.grow = o; o += up(4 * Ycs * s);        // [Ycs][4] g0..g2 of a row: Y-sweep broadcasts
+  L.gx = o; o += up(3 * Ycs * s);          // [3][Ycs] the same, planar: X sweep (lane = row)
+  L.ex = o; o += up(Ycs * s);              // [Ycs] e_j of the current step, planar
   L.tab0 = o; o += up(8 * Ycs * 8);
   L.tab1 = o; o += up(8 * Ycs * 8);
   L.xfa = o; o += up(L.Ux * 32 * s);
@@ -126,6 +128,8 @@ __global__ void __launch_bounds__(NT, (FullMinBlocks<NT>::v)) lvc_line_pair_kern
     S* sW1 = reinterpret_cast<S*>(smem + Ls.w1);
     S* sW2 = reinterpret_cast<S*>(smem + Ls.w2);
     S* sG = reinterpret_cast<S*>(smem + Ls.grow);
+    S* sGx = reinterpret_cast<S*>(smem + Ls.gx);
+    S* sE = reinterpret_cast<S*>(smem + Ls.ex);
     double* const sT0 = reinterpret_cast<double*>(smem + Ls.tab0);
     double* const sT1 = reinterpret_cast<double*>(smem + Ls.tab1);
     S* xfa = reinterpret_cast<S*>(smem + Ls.xfa);
@@ -169,6 +173,13 @@ __global__ void __launch_bounds__(NT, (FullMinBlocks<NT>::v)) lvc_line_pair_kern
       (k == 0 ? sW0 : k == 1 ? sW1 : sW2)[i] = (S)tabc[Lt.wcol + k * (int64_t)((X + 1) & ~1) + i];
     }
     for (int e = tid; e < 4 * Ycs; e += NT) sG[e] = (S)tabc[Lt.rowc + 4LL * r0 + e];
+    // Row constants read with lane = row are planar, so that 32 rows fall in
+    // distinct banks (the [row][4] and [row][8] layouts would conflict 8- and
+    // 16-way).
+    for (int e = tid; e < 3 * Ycs; e += NT) {
+      const int k = e / Ycs, j = e - k * Ycs;
+      sGx[e] = (S)tabc[Lt.rowc + 4LL * (r0 + j) + k];
+    }
 
     if (steps == 0) {
       if (tid == 0 && c.yindex >= r0 && c.yindex < r0 + Ycs)
@@ -212,12 +223,19 @@ __global__ void __launch_bounds__(NT, (FullMinBlocks<NT>::v)) lvc_line_pair_kern
       }
     }
 
+    bool timed_out = false;  // a bulk-copy wait of this item gave up
     for (int s = 0; s < steps; s++, sc++) {
       const int k = steps - 1 - s;
-      if (!mbar_wait(bar, phase)) atomicExch(args.err, 3);
+      if (!mbar_wait(bar, phase, timed_out ? kWaitPollsAfterTimeout : kWaitPolls)) {
+        timed_out = true;
+        atomicExch(args.err, 3);
+      }
       phase ^= 1u;
-      if (clustered) cg::this_cluster().sync(); else __syncthreads();
       const double* tb = (sc & 1) ? sT1 : sT0;
+      // e_j of this step, planar (the barrier below orders it before the X
+      // sweep; its last readers were the previous step's passes 1 and 2)
+      for (int j = tid; j < Ycs; j += NT) sE[j] = (S)tb[j * 8 + kSlotE];
+      if (clustered) cg::this_cluster().sync(); else __syncthreads();
       const S dt = (S)tabc[Lt.dtinv + k];
 
       // -------- X sweep pass 1: explicitX + explicitY, forward recurrence (chunk-local) --------
@@ -229,10 +247,10 @@ __global__ void __launch_bounds__(NT, (FullMinBlocks<NT>::v)) lvc_line_pair_kern
         for (int q = 0; q < UPW; q++) {
           const int ib = chx[q] * K;
           const S* Arow = A + (jl[q] + 1) * LD;
-          e[q] = (S)tb[jl[q] * 8 + kSlotE];
-          g0[q] = sG[4 * jl[q]];
-          g1[q] = sG[4 * jl[q] + 1];
-          g2[q] = sG[4 * jl[q] + 2];
+          e[q] = sE[jl[q]];
+          g0[q] = sGx[jl[q]];
+          g1[q] = sGx[Ycs + jl[q]];
+          g2[q] = sGx[2 * Ycs + jl[q]];
           Rl[q] = ib > 0 ? Arow[ib - 1] : (S)0;
           Rc[q] = V::ld(Arow + ib);
           rbp[q] = ib > 0 ? B[jl[q] * LD + ib - 1] : (S)0;
@@ -310,7 +328,7 @@ __global__ void __launch_bounds__(NT, (FullMinBlocks<NT>::v)) lvc_line_pair_kern
         for (int q = 0; q < UPW; q++) {
           xl[q] = 0;
           Ql[q] = 1;
-          e[q] = (S)tb[jl[q] * 8 + kSlotE];
+          e[q] = sE[jl[q]];
         }
 #pragma unroll
         for (int p = K / 2 - 1; p >= 0; p--) {

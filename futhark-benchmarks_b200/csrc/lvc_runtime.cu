@@ -2062,11 +2062,8 @@ int lvc_server_new(struct futhark_context* ctx, const struct lvc_server_config* 
   S->sctx.device = ctx->device;
   S->sctx.num_sms = ctx->num_sms;
   S->sctx.max_smem = ctx->max_smem;
-  {
-    std::lock_guard<std::mutex> g(ctx->mu);
-    S->sctx.shapes = ctx->shapes;  // the server prices with the shapes tuned so far
-    S->sctx.tuning = ctx->tuning;
-  }
+  S->sctx.shapes = ctx->shapes;  // the server prices with the shapes tuned so far (ctx->mu is held)
+  S->sctx.tuning = ctx->tuning;
   S->sctx.ok = true;
   S->pool.budget = (size_t)c.hbm_budget_bytes;
   cudaError_t e = cudaStreamCreateWithFlags(&S->sctx.stream, cudaStreamNonBlocking);
