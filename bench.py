@@ -43,6 +43,11 @@ UNIT = "options/s"
 # implicit-X coefficients 12, tridiagonal X 10, combine 3, implicit-Y
 # coefficients 12, tridiagonal Y 10.
 F_ALG = 77
+# DRAM bytes (read + write) of the rollback launches of one run of the default
+# workload (uneven mix, 512 calibrations, seed 0, f64), from the ncu launch list
+# of `python bench.py --steps 2 --warmup 3 --no-plain --no-serving --cpu-seconds 3`
+# (dram__bytes_read.sum + dram__bytes_write.sum over the 13 plan runs / 13).
+ROLLBACK_DRAM_BYTES_DEFAULT = 355.982e9 / 13
 CALIB_DEV_BYTES = 112  # sizeof(lvc::CalibDev) (static_assert in lvc_layout.h), uploaded per calibration per step
 
 
@@ -73,6 +78,26 @@ def dist_env():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     return rank, world, local
+
+
+def rank_reduce(x: float, op: str, world: int, device: str) -> float:
+    """Max or sum of a per-rank number over all ranks (any process-group backend)."""
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def job_throughput(ms_rank: float, options_rank: float, steps: int, world: int, device: str):
+    """Whole-job options/s: the options of all ranks over the slowest rank's
+    device time (weak scaling: every rank prices its own shard).  Returns
+    (options/s, max ms over ranks)."""
+    ms_max = rank_reduce(ms_rank, "max", world, device)
+    total = rank_reduce(options_rank, "sum", world, device)
+    return total * steps / (ms_max * 1e-3), ms_max
 
 
 def workload(args, rank):
@@ -270,21 +295,13 @@ def run_ours(args):
             import torch.distributed as dist
             dist.barrier(device_ids=[local])
 
+    dev = f"cuda:{local}"
+
     def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        import torch.distributed as dist
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return rank_reduce(x, "max", world, dev)
 
     def sum_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        import torch.distributed as dist
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        return float(t.item())
+        return rank_reduce(x, "sum", world, dev)
 
     calibs, desc = workload(args, rank)
     precision = pkg.F64 if args.precision == "f64" else pkg.F32_STATE
@@ -313,8 +330,7 @@ def run_ours(args):
     barrier()
     ms = ev0.elapsed_time(ev1)
     clk = clocks.stop()
-    ms_max = max_over_ranks(ms)
-    value = sum_over_ranks(n_opts) * args.steps / (ms_max * 1e-3)
+    value, ms_max = job_throughput(ms, n_opts, args.steps, world, dev)
 
     # ---- the rollback kernel alone (events around each rollback launch) ----
     plan.time(max(1, args.steps))
@@ -364,6 +380,12 @@ def run_ours(args):
     if rank == 0 and world == 1:
         cpu = cpu_baseline(calibs, args.cpu_seconds)
 
+    default_workload = (args.workload == "uneven" and args.calibs == 512 and args.seed == 0
+                        and args.precision == "f64")
+    traffic = ROLLBACK_DRAM_BYTES_DEFAULT if default_workload else None
+    traffic_src = ("ncu launch list of the default workload: DRAM bytes of the rollback launches per step "
+                   "(the per-step pivot rows come from L2; the grids stay in shared memory)"
+                   if default_workload else "not measured for this workload")
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -379,8 +401,10 @@ def run_ours(args):
                     "path": "lvc_plan_set_params + lvc_plan_run + lvc_plan_copy_prices"},
             "gpu_launches": args.steps * plan.num_launches,
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
-                         "frac": achieved / fp64_peak, "traffic": None,
-                         "kernel": "lvc_rollback_kernel (sum of its launches)",
+                         "frac": achieved / fp64_peak, "traffic": traffic,
+                         "traffic_source": traffic_src,
+                         "kernel": "rollback launches (lvc_line_pair_kernel for numX % 64 == 0, "
+                                   "lvc_line_full_kernel for numX == 32), summed per step",
                          "flops_per_unit": F_ALG, "unit_of_work": "option-cell-step",
                          "units_per_step": work, "kernel_ms_per_step": roll_ms,
                          "peak_source": "measured live: lvc_probe_dfma_kernel on this GPU "
