@@ -25,7 +25,7 @@ namespace lvc {
 
 struct PairLayout {
   int LD, Ycs, CHx, Ux, CG2, CHy, Uy;
-  int bar, A, B, w0, w1, w2, grow, gx, ex, tab0, tab1, xfa, xfb, xba, xbb, yf, yb, blkF, blkB, zin, xin, tot, total;
+  int bar, A, B, w0, w1, w2, grow, gx, ex, tab0, tab1, xf, xb, yf, yb, blkF, blkB, zin, xin, tot, total;
 };
 
 // Byte offsets of the shared-memory buffers.
@@ -53,10 +53,8 @@ LVC_HD PairLayout pair_layout(int X, int Ycs) {
   L.ex = o; o += up(Ycs * s);              // [Ycs] e_j of the current step, planar
   L.tab0 = o; o += up(8 * Ycs * 8);
   L.tab1 = o; o += up(8 * Ycs * 8);
-  L.xfa = o; o += up(L.Ux * 32 * s);
-  L.xfb = o; o += up(L.Ux * 32 * s);
-  L.xba = o; o += up(L.Ux * 32 * s);
-  L.xbb = o; o += up(L.Ux * 32 * s);
+  L.xf = o; o += up(L.Ux * 64 * s);        // [unit][lane] (a, b) of the forward chunk maps
+  L.xb = o; o += up(L.Ux * 64 * s);        // the same, backward
   L.yf = o; o += up(L.Uy * 64 * s);
   L.yb = o; o += up(L.Uy * 64 * s);
   L.blkF = o; o += up(X * s);
@@ -132,10 +130,8 @@ __global__ void __launch_bounds__(NT, (FullMinBlocks<NT>::v)) lvc_line_pair_kern
     S* sE = reinterpret_cast<S*>(smem + Ls.ex);
     double* const sT0 = reinterpret_cast<double*>(smem + Ls.tab0);
     double* const sT1 = reinterpret_cast<double*>(smem + Ls.tab1);
-    S* xfa = reinterpret_cast<S*>(smem + Ls.xfa);
-    S* xfb = reinterpret_cast<S*>(smem + Ls.xfb);
-    S* xba = reinterpret_cast<S*>(smem + Ls.xba);
-    S* xbb = reinterpret_cast<S*>(smem + Ls.xbb);
+    S* xf = reinterpret_cast<S*>(smem + Ls.xf);
+    S* xb = reinterpret_cast<S*>(smem + Ls.xb);
     S* yf = reinterpret_cast<S*>(smem + Ls.yf);
     S* yb = reinterpret_cast<S*>(smem + Ls.yb);
     S* blkF = reinterpret_cast<S*>(smem + Ls.blkF);
@@ -198,17 +194,19 @@ __global__ void __launch_bounds__(NT, (FullMinBlocks<NT>::v)) lvc_line_pair_kern
     };
     issue_copies(steps - 1, (sc & 1) ? sT1 : sT0);
 
-    // X units u = warp + q * NW: rows rgx*32 + lane, columns chx*16 ..
+    // X units u = 2 * warp + q: rows rgx*32 + lane, columns chx*16 .. -- a
+    // warp's two units are neighbouring chunks of the same rows (the number of
+    // chunks per row, numX / 16, is even), so the second unit's chunk prefix
+    // is the first one's plus one chunk
     int rgx[UPW], chx[UPW], jl[UPW];
 #pragma unroll
     for (int q = 0; q < UPW; q++) {
-      const int u = warp + q * NW;
+      const int u = UPW * warp + q;
       rgx[q] = u / Ls.CHx;
       chx[q] = u - rgx[q] * Ls.CHx;
       jl[q] = rgx[q] * 32 + lane;
     }
-    // the two units of a warp fold their chunk prefixes in one pass when
-    // they lie on the same rows
+    // the two units of a warp fold their chunk prefixes in one pass
     const bool xchain = rgx[1] == rgx[0] && chx[1] > chx[0];
     // Y unit u = warp: columns cg2*64 + 2*lane (+1), rows chy*16 ..
     const int cg2 = warp / Ls.CHy, chy = warp - cg2 * Ls.CHy;
@@ -297,9 +295,8 @@ __global__ void __launch_bounds__(NT, (FullMinBlocks<NT>::v)) lvc_line_pair_kern
         }
 #pragma unroll
         for (int q = 0; q < UPW; q++) {
-          const int u = warp + q * NW;
-          xfa[u * 32 + lane] = zl[q];
-          xfb[u * 32 + lane] = Pl[q];
+          const int u = UPW * warp + q;
+          V::st(xf + (u * 32 + lane) * 2, zl[q], Pl[q]);
         }
       }
       __syncthreads();
@@ -310,8 +307,8 @@ __global__ void __launch_bounds__(NT, (FullMinBlocks<NT>::v)) lvc_line_pair_kern
           S a = 0;
           int c2 = 0;
           for (; c2 < chx[0]; c2++) {
-            const int u = rgx[0] * Ls.CHx + c2;
-            a = xfa[u * 32 + lane] + xfb[u * 32 + lane] * a;
+            const auto f = V::ld(xf + ((rgx[0] * Ls.CHx + c2) * 32 + lane) * 2);
+            a = f.x + f.y * a;
           }
           zin[0] = a;
           if (!xchain) {
@@ -319,8 +316,8 @@ __global__ void __launch_bounds__(NT, (FullMinBlocks<NT>::v)) lvc_line_pair_kern
             c2 = 0;
           }
           for (; c2 < chx[1]; c2++) {
-            const int u = rgx[1] * Ls.CHx + c2;
-            a = xfa[u * 32 + lane] + xfb[u * 32 + lane] * a;
+            const auto f = V::ld(xf + ((rgx[1] * Ls.CHx + c2) * 32 + lane) * 2);
+            a = f.x + f.y * a;
           }
           zin[1] = a;
         }
@@ -357,9 +354,8 @@ __global__ void __launch_bounds__(NT, (FullMinBlocks<NT>::v)) lvc_line_pair_kern
         }
 #pragma unroll
         for (int q = 0; q < UPW; q++) {
-          const int u = warp + q * NW;
-          xba[u * 32 + lane] = xl[q];
-          xbb[u * 32 + lane] = Ql[q];
+          const int u = UPW * warp + q;
+          V::st(xb + (u * 32 + lane) * 2, xl[q], Ql[q]);
         }
       }
       __syncthreads();
@@ -370,8 +366,8 @@ __global__ void __launch_bounds__(NT, (FullMinBlocks<NT>::v)) lvc_line_pair_kern
           S a = 0;
           int c2 = Ls.CHx - 1;
           for (; c2 > chx[1]; c2--) {
-            const int u = rgx[1] * Ls.CHx + c2;
-            a = xba[u * 32 + lane] + xbb[u * 32 + lane] * a;
+            const auto f = V::ld(xb + ((rgx[1] * Ls.CHx + c2) * 32 + lane) * 2);
+            a = f.x + f.y * a;
           }
           xin[1] = a;
           if (!xchain) {
@@ -379,8 +375,8 @@ __global__ void __launch_bounds__(NT, (FullMinBlocks<NT>::v)) lvc_line_pair_kern
             c2 = Ls.CHx - 1;
           }
           for (; c2 > chx[0]; c2--) {
-            const int u = rgx[0] * Ls.CHx + c2;
-            a = xba[u * 32 + lane] + xbb[u * 32 + lane] * a;
+            const auto f = V::ld(xb + ((rgx[0] * Ls.CHx + c2) * 32 + lane) * 2);
+            a = f.x + f.y * a;
           }
           xin[0] = a;
         }
