@@ -82,8 +82,14 @@ template <> struct P2<float> {
   }
 };
 
+// f32 state: a CTA's shared memory is half that of f64, so two CTAs can share
+// an SM when the registers allow it as well.
+template <typename S, int NT> struct PairMinBlocks {
+  static constexpr int v = FullMinBlocks<NT>::v * (sizeof(S) == 4 ? 2 : 1);
+};
+
 template <typename S, typename PV, int NT>
-__global__ void __launch_bounds__(NT, (FullMinBlocks<NT>::v)) lvc_line_pair_kernel(RollbackArgs<S, PV> args) {
+__global__ void __launch_bounds__(NT, (PairMinBlocks<S, NT>::v)) lvc_line_pair_kernel(RollbackArgs<S, PV> args) {
   constexpr int K = kLineK;
   constexpr int NW = NT / 32;
   constexpr int UPW = 2;        // X units per warp
