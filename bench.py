@@ -65,6 +65,7 @@ def parse():
                     help="time the plain per-call form on the first N calibrations (0 = all)")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="built-in shapes instead of the autotuner's")
     ap.add_argument("--serving-rates", default="100,1000,5000,20000",
                     help="Poisson arrival rates (requests/s) of the serving sweep")
     ap.add_argument("--serving-requests", type=int, default=300)
@@ -307,6 +308,16 @@ def run_ours(args):
     precision = pkg.F64 if args.precision == "f64" else pkg.F32_STATE
     ctx = pkg.Context(f"#{local}")
     fp64_peak, smem_peak = ctx.probe_peaks()
+    # shape autotuner: every candidate (kernel family x cluster size) of every
+    # grid class, timed on the class's own instances; before the timed region
+    tune = None
+    if not args.no_autotune:
+        t0 = time.perf_counter()
+        entries = ctx.autotune(calibs, precision=precision, probe_steps=8)
+        tune = {"seconds": time.perf_counter() - t0, "classes": len(entries),
+                "changed_from_builtin": [f"{e.numX}x{e.numY}: {e.shape}" for e in entries
+                                         if e.us_per_step_default > 0
+                                         and e.us_per_step_best < e.us_per_step_default * 0.999]}
     plan = ctx.plan(calibs, precision=precision)
     ext = torch.cuda.ExternalStream(ctx.stream, device=f"cuda:{local}")
     n_opts = wl.total_options(calibs)
@@ -393,7 +404,7 @@ def run_ours(args):
             "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if precision == pkg.F64 else "f32-state (f64 pivots)",
             "data": "synthetic (seeded calibration parameters; no dataset)",
-            "config": dict(desc, precision=args.precision, options_per_rank=n_opts,
+            "config": dict(desc, precision=args.precision, options_per_rank=n_opts, autotune=tune,
                            option_cell_steps_per_rank=work,
                            l2="inputs larger than L2: the per-step pivot tables of the mix exceed 126 MB"),
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": CALIB_DEV_BYTES * len(calibs),

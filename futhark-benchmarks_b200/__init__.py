@@ -74,7 +74,7 @@ class Shape(ctypes.Structure):
     _fields_ = [("family", ctypes.c_int32), ("cluster", ctypes.c_int32), ("threads", ctypes.c_int32),
                 ("rows_per_cta", ctypes.c_int32), ("smem_bytes", ctypes.c_int32), ("hbm_state", ctypes.c_int32)]
 
-    FAMILIES = {0: "chunk", 1: "line", 2: "line_full", 3: "line_pair"}
+    FAMILIES = {0: "chunk", 1: "line", 2: "line_full", 3: "line_pair", 4: "line_pair1"}
 
     def __repr__(self):
         fam = self.FAMILIES.get(self.family, "?") + ("_hbm" if self.hbm_state else "")

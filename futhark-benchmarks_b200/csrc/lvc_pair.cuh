@@ -15,8 +15,15 @@
 // reading one 16-byte pair from 32 consecutive rows fall into 4 conflict-free
 // wavefronts (8 lanes cover the 32 banks), and rows start 16-byte aligned for
 // the pair accesses of the Y sweep.  Columns numX and numX + 1 are zero.
-// Needs numX % 64 == 0 (whole 64-column Y units), rows per CTA % 32 == 0 and
+// Needs numX % (32 * UPW) == 0 (whole Y units), rows per CTA % 32 == 0 and
 // numY = cluster size x rows per CTA.
+//
+// UPW (units per warp) = 2: each warp owns two X units (two independent
+// recurrence chains per lane) and one 64-column Y unit (two columns per lane);
+// with UPW = 1 a warp owns one X unit and one 32-column Y unit (one column per
+// lane), so the same block runs on twice the warps at half the registers per
+// thread -- more warps to hide shared-memory and FP64 latency when the grid's
+// shared memory leaves room for only one CTA per SM.
 #pragma once
 
 #include "lvc_line.cuh"
@@ -30,7 +37,7 @@ struct PairLayout {
 
 // Byte offsets of the shared-memory buffers.
 template <typename S>
-LVC_HD PairLayout pair_layout(int X, int Ycs) {
+LVC_HD PairLayout pair_layout(int X, int Ycs, int upw) {
   PairLayout L;
   auto up = [](int n) { return (n + 15) / 16 * 16; };
   const int s = (int)sizeof(S);
@@ -38,7 +45,7 @@ LVC_HD PairLayout pair_layout(int X, int Ycs) {
   L.Ycs = Ycs;
   L.CHx = X / kLineK;
   L.Ux = (Ycs / 32) * L.CHx;  // X units: 2 per warp
-  L.CG2 = X / 64;
+  L.CG2 = X / (32 * upw);    // column groups of a Y unit (32 * upw columns)
   L.CHy = Ycs / kLineK;
   L.Uy = L.CG2 * L.CHy;       // Y units: 1 per warp
   int o = 0;
@@ -55,8 +62,8 @@ LVC_HD PairLayout pair_layout(int X, int Ycs) {
   L.tab1 = o; o += up(8 * Ycs * 8);
   L.xf = o; o += up(L.Ux * 64 * s);        // [unit][lane] (a, b) of the forward chunk maps
   L.xb = o; o += up(L.Ux * 64 * s);        // the same, backward
-  L.yf = o; o += up(L.Uy * 64 * s);
-  L.yb = o; o += up(L.Uy * 64 * s);
+  L.yf = o; o += up(L.Uy * 32 * upw * s);
+  L.yb = o; o += up(L.Uy * 32 * upw * s);
   L.blkF = o; o += up(X * s);
   L.blkB = o; o += up(X * s);
   L.zin = o; o += up(X * s);
@@ -82,18 +89,36 @@ template <> struct P2<float> {
   }
 };
 
-// f32 state: a CTA's shared memory is half that of f64, so two CTAs can share
-// an SM when the registers allow it as well.
-template <typename S, int NT> struct PairMinBlocks {
-  static constexpr int v = FullMinBlocks<NT>::v * (sizeof(S) == 4 ? 2 : 1);
+// N adjacent columns of a row (N = 1 or 2) to and from registers.
+template <typename S, int N>
+__device__ __forceinline__ void ld_cols(const S* p, S (&v)[N]) {
+  if constexpr (N == 2) {
+    const auto t = P2<S>::ld(p);
+    v[0] = t.x;
+    v[1] = t.y;
+  } else {
+    v[0] = *p;
+  }
+}
+template <typename S, int N>
+__device__ __forceinline__ void st_cols(S* p, const S (&v)[N]) {
+  if constexpr (N == 2) P2<S>::st(p, v[0], v[1]); else *p = v[0];
+}
+
+// Resident CTAs per SM the launch bounds ask for: 256 threads' worth of
+// warps, twice that with f32 state (half the shared memory per CTA).
+template <typename S, int NT, int UPW> struct PairMinBlocks {
+  static constexpr int base = UPW == 2 ? FullMinBlocks<NT>::v : (NT >= 512 ? 1 : 512 / NT);
+  static constexpr int v = UPW == 2 && sizeof(S) == 4 ? 2 * base : base;
 };
 
-template <typename S, typename PV, int NT>
-__global__ void __launch_bounds__(NT, (PairMinBlocks<S, NT>::v)) lvc_line_pair_kernel(RollbackArgs<S, PV> args) {
+template <typename S, typename PV, int NT, int UPW>
+__global__ void __launch_bounds__(NT, (PairMinBlocks<S, NT, UPW>::v)) lvc_line_pair_kernel(RollbackArgs<S, PV> args) {
   constexpr int K = kLineK;
   constexpr int NW = NT / 32;
-  constexpr int UPW = 2;        // X units per warp
   constexpr int NU = NW * UPW;  // X units per sweep
+  constexpr int UW = 32 * UPW;  // columns per Y unit
+  static_assert(UPW == 1 || UPW == 2, "one or two units per warp");
   static_assert(sizeof(S) == sizeof(PV), "pivots are copied verbatim into the state buffer");
   static_assert(K % 2 == 0, "columns are walked in pairs");
   using V = P2<S>;
@@ -118,10 +143,10 @@ __global__ void __launch_bounds__(NT, (PairMinBlocks<S, NT>::v)) lvc_line_pair_k
     const int X = c.numX, Y = c.numY, T = c.numT;
     const int Ycs = c.Ycs;
     const int r0 = rank * Ycs;
-    const PairLayout Ls = pair_layout<S>(X, Ycs);
+    const PairLayout Ls = pair_layout<S>(X, Ycs, UPW);
     // uniform over the cluster (every CTA of a cluster sees the same item)
     if (c.kind != kKindLine || c.C != C || c.ld != Ls.LD || Ls.total > args.smem_elems * (int)sizeof(S) ||
-        Ls.Ux != NU || Ls.Uy != NW || (X % 64) || (Ycs % 32) || Ycs * C != Y) {
+        Ls.Ux != NU || Ls.Uy != NW || (X % UW) || (Ycs % 32) || Ycs * C != Y) {
       if (tid == 0) atomicExch(args.err, 5);
       continue;
     }
@@ -200,7 +225,7 @@ __global__ void __launch_bounds__(NT, (PairMinBlocks<S, NT>::v)) lvc_line_pair_k
     };
     issue_copies(steps - 1, (sc & 1) ? sT1 : sT0);
 
-    // X units u = 2 * warp + q: rows rgx*32 + lane, columns chx*16 .. -- a
+    // X units u = UPW * warp + q: rows rgx*32 + lane, columns chx*16 .. -- a
     // warp's two units are neighbouring chunks of the same rows (the number of
     // chunks per row, numX / 16, is even), so the second unit's chunk prefix
     // is the first one's plus one chunk
@@ -213,16 +238,16 @@ __global__ void __launch_bounds__(NT, (PairMinBlocks<S, NT>::v)) lvc_line_pair_k
       jl[q] = rgx[q] * 32 + lane;
     }
     // the two units of a warp fold their chunk prefixes in one pass
-    const bool xchain = rgx[1] == rgx[0] && chx[1] > chx[0];
-    // Y unit u = warp: columns cg2*64 + 2*lane (+1), rows chy*16 ..
-    const int cg2 = warp / Ls.CHy, chy = warp - cg2 * Ls.CHy;
-    const int col0 = cg2 * 64 + 2 * lane;
-    // output lane: the column half and element holding myResult[myYindex, myXindex]
+    const bool xchain = UPW == 2 && rgx[UPW - 1] == rgx[0] && chx[UPW - 1] > chx[0];
+    // Y unit u = warp: columns cgy*UW + UPW*lane (+ h < UPW), rows chy*16 ..
+    const int cgy = warp / Ls.CHy, chy = warp - cgy * Ls.CHy;
+    const int col0 = cgy * UW + UPW * lane;
+    // output lane: the column and element holding myResult[myYindex, myXindex]
     int out_h = -1, out_m = 0;
     {
       const int jy = c.yindex - r0 - chy * K;
-      if ((c.xindex & ~1) == col0 && jy >= 0 && jy < K) {
-        out_h = c.xindex & 1;
+      if (c.xindex >= col0 && c.xindex < col0 + UPW && jy >= 0 && jy < K) {
+        out_h = c.xindex - col0;
         out_m = jy;
       }
     }
@@ -317,15 +342,17 @@ __global__ void __launch_bounds__(NT, (PairMinBlocks<S, NT>::v)) lvc_line_pair_k
             a = f.x + f.y * a;
           }
           zin[0] = a;
-          if (!xchain) {
-            a = 0;
-            c2 = 0;
+          if constexpr (UPW == 2) {
+            if (!xchain) {
+              a = 0;
+              c2 = 0;
+            }
+            for (; c2 < chx[UPW - 1]; c2++) {
+              const auto f = V::ld(xf + ((rgx[UPW - 1] * Ls.CHx + c2) * 32 + lane) * 2);
+              a = f.x + f.y * a;
+            }
+            zin[UPW - 1] = a;
           }
-          for (; c2 < chx[1]; c2++) {
-            const auto f = V::ld(xf + ((rgx[1] * Ls.CHx + c2) * 32 + lane) * 2);
-            a = f.x + f.y * a;
-          }
-          zin[1] = a;
         }
 #pragma unroll
         for (int q = 0; q < UPW; q++) {
@@ -371,14 +398,16 @@ __global__ void __launch_bounds__(NT, (PairMinBlocks<S, NT>::v)) lvc_line_pair_k
         {
           S a = 0;
           int c2 = Ls.CHx - 1;
-          for (; c2 > chx[1]; c2--) {
-            const auto f = V::ld(xb + ((rgx[1] * Ls.CHx + c2) * 32 + lane) * 2);
-            a = f.x + f.y * a;
-          }
-          xin[1] = a;
-          if (!xchain) {
-            a = 0;
-            c2 = Ls.CHx - 1;
+          if constexpr (UPW == 2) {
+            for (; c2 > chx[UPW - 1]; c2--) {
+              const auto f = V::ld(xb + ((rgx[UPW - 1] * Ls.CHx + c2) * 32 + lane) * 2);
+              a = f.x + f.y * a;
+            }
+            xin[UPW - 1] = a;
+            if (!xchain) {
+              a = 0;
+              c2 = Ls.CHx - 1;
+            }
           }
           for (; c2 > chx[0]; c2--) {
             const auto f = V::ld(xb + ((rgx[0] * Ls.CHx + c2) * 32 + lane) * 2);
@@ -398,40 +427,43 @@ __global__ void __launch_bounds__(NT, (PairMinBlocks<S, NT>::v)) lvc_line_pair_k
       }
       __syncthreads();
 
-      // -------- Y sweep: lane = columns col0, col0 + 1 --------
-      S y[2][K];
+      // -------- Y sweep: lane = columns col0 .. col0 + UPW - 1 --------
+      S y[UPW][K];
       {
-        S zz0 = 0, zz1 = 0;
+        S zz[UPW], Ru[UPW], Rm[UPW];
         const int j0 = chy * K;
-        auto Ru = V::ld(A + j0 * LD + col0);        // row j0 - 1 (halo row at the block edge)
-        auto Rm = V::ld(A + (j0 + 1) * LD + col0);  // row j0
+        ld_cols<S, UPW>(A + j0 * LD + col0, Ru);        // row j0 - 1 (halo row at the block edge)
+        ld_cols<S, UPW>(A + (j0 + 1) * LD + col0, Rm);  // row j0
+#pragma unroll
+        for (int h = 0; h < UPW; h++) zz[h] = 0;
 #pragma unroll
         for (int m = 0; m < K; m++) {
           const int j = j0 + m;
-          const auto Rd = V::ld(A + (j + 2) * LD + col0);  // row j + 1
+          S Rd[UPW], bx[UPW];
+          ld_cols<S, UPW>(A + (j + 2) * LD + col0, Rd);  // row j + 1
+          ld_cols<S, UPW>(B + j * LD + col0, bx);
           const auto g01 = V::ld(sG + 4 * j);
           const S g2 = sG[4 * j + 2];
           const S my = (S)tb[j * 8 + kSlotMY];
-          const auto bx = V::ld(B + j * LD + col0);
-          const S v0 = g01.x * Ru.x + g01.y * Rm.x + g2 * Rd.x;  // explicitY (:199)
-          const S v1 = g01.x * Ru.y + g01.y * Rm.y + g2 * Rd.y;
-          zz0 = (bx.x - (S)0.5 * v0) + my * zz0;                   // :205, forward recurrence
-          zz1 = (bx.y - (S)0.5 * v1) + my * zz1;
-          y[0][m] = zz0;
-          y[1][m] = zz1;
-          Ru = Rm;
-          Rm = Rd;
+#pragma unroll
+          for (int h = 0; h < UPW; h++) {
+            const S v = g01.x * Ru[h] + g01.y * Rm[h] + g2 * Rd[h];  // explicitY (:199)
+            zz[h] = (bx[h] - (S)0.5 * v) + my * zz[h];              // :205, forward recurrence
+            y[h][m] = zz[h];
+            Ru[h] = Rm[h];
+            Rm[h] = Rd[h];
+          }
         }
-        V::st(yf + warp * 64 + 2 * lane, zz0, zz1);
+        st_cols<S, UPW>(yf + warp * UW + UPW * lane, zz);
       }
       __syncthreads();
       if (s + 1 < steps) issue_copies(k - 1, ((sc + 1) & 1) ? sT1 : sT0);
       if (clustered) {
         for (int col = tid; col < X; col += NT) {
-          const int g = col >> 6, w = col & 63;
+          const int g = col / UW, w = col - g * UW;
           S a = 0;
           for (int c2 = 0; c2 < Ls.CHy; c2++)
-            a = yf[(g * Ls.CHy + c2) * 64 + w] + (S)tb[(c2 * K + K - 1) * 8 + kSlotCP] * a;
+            a = yf[(g * Ls.CHy + c2) * UW + w] + (S)tb[(c2 * K + K - 1) * 8 + kSlotCP] * a;
           blkF[col] = a;
         }
         if (tid == 0) {
@@ -453,40 +485,41 @@ __global__ void __launch_bounds__(NT, (PairMinBlocks<S, NT>::v)) lvc_line_pair_k
         __syncthreads();
       }
       {
-        S zin0 = 0, zin1 = 0;
-        if (clustered) {
-          const auto zi = V::ld(s_zin + col0);
-          zin0 = zi.x;
-          zin1 = zi.y;
+        S zin[UPW], xx[UPW];
+#pragma unroll
+        for (int h = 0; h < UPW; h++) {
+          zin[h] = 0;
+          xx[h] = 0;
         }
+        if (clustered) ld_cols<S, UPW>(s_zin + col0, zin);
         for (int c2 = 0; c2 < chy; c2++) {
-          const auto a = V::ld(yf + (cg2 * Ls.CHy + c2) * 64 + 2 * lane);
+          S a[UPW];
+          ld_cols<S, UPW>(yf + (cgy * Ls.CHy + c2) * UW + UPW * lane, a);
           const S cp = (S)tb[(c2 * K + K - 1) * 8 + kSlotCP];
-          zin0 = a.x + cp * zin0;
-          zin1 = a.y + cp * zin1;
+#pragma unroll
+          for (int h = 0; h < UPW; h++) zin[h] = a[h] + cp * zin[h];
         }
-        S xx0 = 0, xx1 = 0;
 #pragma unroll
         for (int m = K - 1; m >= 0; m--) {
           const int j = chy * K + m;
           const double2 nr = *reinterpret_cast<const double2*>(tb + j * 8 + kSlotNY);  // nY, 1/b'
           const S cp = (S)tb[j * 8 + kSlotCP];
-          const S zv0 = y[0][m] + cp * zin0;
-          const S zv1 = y[1][m] + cp * zin1;
-          xx0 = (S)nr.y * zv0 + (S)nr.x * xx0;
-          xx1 = (S)nr.y * zv1 + (S)nr.x * xx1;
-          y[0][m] = xx0;
-          y[1][m] = xx1;
+#pragma unroll
+          for (int h = 0; h < UPW; h++) {
+            const S zv = y[h][m] + cp * zin[h];
+            xx[h] = (S)nr.y * zv + (S)nr.x * xx[h];
+            y[h][m] = xx[h];
+          }
         }
-        V::st(yb + warp * 64 + 2 * lane, xx0, xx1);
+        st_cols<S, UPW>(yb + warp * UW + UPW * lane, xx);
       }
       __syncthreads();
       if (clustered) {
         for (int col = tid; col < X; col += NT) {
-          const int g = col >> 6, w = col & 63;
+          const int g = col / UW, w = col - g * UW;
           S a = 0;
           for (int c2 = Ls.CHy - 1; c2 >= 0; c2--)
-            a = yb[(g * Ls.CHy + c2) * 64 + w] + (S)tb[(c2 * K) * 8 + kSlotCQ] * a;
+            a = yb[(g * Ls.CHy + c2) * UW + w] + (S)tb[(c2 * K) * 8 + kSlotCQ] * a;
           blkB[col] = a;
         }
         if (tid == 0) {
@@ -508,36 +541,49 @@ __global__ void __launch_bounds__(NT, (PairMinBlocks<S, NT>::v)) lvc_line_pair_k
         __syncthreads();
       }
       {
-        S xin0 = 0, xin1 = 0;
-        if (clustered) {
-          const auto xi = V::ld(s_xin + col0);
-          xin0 = xi.x;
-          xin1 = xi.y;
-        }
+        S xin[UPW];
+#pragma unroll
+        for (int h = 0; h < UPW; h++) xin[h] = 0;
+        if (clustered) ld_cols<S, UPW>(s_xin + col0, xin);
         for (int c2 = Ls.CHy - 1; c2 > chy; c2--) {
-          const auto b = V::ld(yb + (cg2 * Ls.CHy + c2) * 64 + 2 * lane);
+          S b[UPW];
+          ld_cols<S, UPW>(yb + (cgy * Ls.CHy + c2) * UW + UPW * lane, b);
           const S cq = (S)tb[(c2 * K) * 8 + kSlotCQ];
-          xin0 = b.x + cq * xin0;
-          xin1 = b.y + cq * xin1;
+#pragma unroll
+          for (int h = 0; h < UPW; h++) xin[h] = b[h] + cq * xin[h];
         }
 #pragma unroll
         for (int m = 0; m < K; m++) {
           const int j = chy * K + m;
           const S cq = (S)tb[j * 8 + kSlotCQ];
-          const S xv0 = y[0][m] + cq * xin0;
-          const S xv1 = y[1][m] + cq * xin1;
-          y[0][m] = xv0;
-          y[1][m] = xv1;
-          V::st(A + (j + 1) * LD + col0, xv0, xv1);
+          S xv[UPW];
+#pragma unroll
+          for (int h = 0; h < UPW; h++) {
+            xv[h] = y[h][m] + cq * xin[h];
+            y[h][m] = xv[h];
+          }
+          st_cols<S, UPW>(A + (j + 1) * LD + col0, xv);
         }
         // halo rows of the cluster neighbours, and the price on the last step
-        if (halo_prev && chy == 0) V::st(halo_prev + col0, y[0][0], y[1][0]);
-        if (halo_next && chy == Ls.CHy - 1) V::st(halo_next + col0, y[0][K - 1], y[1][K - 1]);
+        if (halo_prev && chy == 0) {
+          S t[UPW];
+#pragma unroll
+          for (int h = 0; h < UPW; h++) t[h] = y[h][0];
+          st_cols<S, UPW>(halo_prev + col0, t);
+        }
+        if (halo_next && chy == Ls.CHy - 1) {
+          S t[UPW];
+#pragma unroll
+          for (int h = 0; h < UPW; h++) t[h] = y[h][K - 1];
+          st_cols<S, UPW>(halo_next + col0, t);
+        }
         if (s == steps - 1 && out_h >= 0) {
           S pv = 0;
 #pragma unroll
-          for (int m = 0; m < K; m++)
-            if (m == out_m) pv = out_h ? y[1][m] : y[0][m];
+          for (int h = 0; h < UPW; h++)
+#pragma unroll
+            for (int m = 0; m < K; m++)
+              if (h == out_h && m == out_m) pv = y[h][m];
           args.out[c.out + item.strike] = (double)pv;  // myResult[myYindex, myXindex]
         }
       }

@@ -175,6 +175,7 @@ struct Config {
   bool gstate;
   bool full = false;
   bool pair = false;  // paired line kernel
+  int upw = 2;        // paired kernel: units per warp
   int ld = 0;         // line family: row stride of the pivot rows and the on-chip grid
   int Ycs;
   size_t smem_bytes;
@@ -193,6 +194,7 @@ struct Launch {
   bool gstate;
   bool full = false;
   bool pair = false;
+  int upw = 2;
   int item_off, n_items, grid;
   size_t smem_bytes;
   int64_t gstate_per_cta;  // elements of the state type
@@ -318,11 +320,19 @@ template <typename S, typename PV>
 using RbFn = void (*)(RollbackArgs<S, PV>);
 
 template <typename S, typename PV>
-RbFn<S, PV> rollback_fn(int kind, int NT, int KX, bool gs, bool full = false, bool pair = false) {
+RbFn<S, PV> rollback_fn(int kind, int NT, int KX, bool gs, bool full = false, bool pair = false,
+                        int upw = 2) {
+  if (kind == kKindLine && pair && upw == 1) {
+    if (NT == 64) return lvc_line_pair_kernel<S, PV, 64, 1>;
+    if (NT == 128) return lvc_line_pair_kernel<S, PV, 128, 1>;
+    if (NT == 256) return lvc_line_pair_kernel<S, PV, 256, 1>;
+    if (NT == 512) return lvc_line_pair_kernel<S, PV, 512, 1>;
+    return nullptr;
+  }
   if (kind == kKindLine && pair) {
-    if (NT == 64) return lvc_line_pair_kernel<S, PV, 64>;
-    if (NT == 128) return lvc_line_pair_kernel<S, PV, 128>;
-    if (NT == 256) return lvc_line_pair_kernel<S, PV, 256>;
+    if (NT == 64) return lvc_line_pair_kernel<S, PV, 64, 2>;
+    if (NT == 128) return lvc_line_pair_kernel<S, PV, 128, 2>;
+    if (NT == 256) return lvc_line_pair_kernel<S, PV, 256, 2>;
     return nullptr;
   }
   if (kind == kKindLine && full) {
@@ -383,20 +393,22 @@ bool line_full_cfg(int X, int Y, int C, int max_smem, Config& cf) {
   return true;
 }
 
-// Paired line kernel: full tiles with numX % 64 == 0; two X units and one Y
-// unit (64 columns) per warp.
+// Paired line kernel on full tiles: upw = 2 (two X units and one 64-column
+// Y unit per warp, numX % 64 == 0) or upw = 1 (one X unit and one 32-column
+// Y unit per warp, twice the warps).
 template <typename S>
-bool line_pair_cfg(int X, int Y, int C, int max_smem, Config& cf) {
-  if (X > 256 || X % 64 || Y % C || (Y / C) % 32) return false;
+bool line_pair_cfg(int X, int Y, int C, int max_smem, Config& cf, int upw = 2) {
+  if (X > 256 || X % (32 * upw) || Y % C || (Y / C) % 32) return false;
   const int Ycs = Y / C;
   const int units = X * Ycs / 512;  // X units of 32 rows x 16 columns
-  if (units != 4 && units != 8 && units != 16) return false;  // NT = 16 * units instantiated
-  const int NW = units / 2;
-  const PairLayout F = pair_layout<S>(X, Ycs);
+  const int NW = units / upw;
+  if (NW * upw != units || NW < 2 || NW > (upw == 2 ? 8 : 16) || (NW & (NW - 1))) return false;
+  const PairLayout F = pair_layout<S>(X, Ycs, upw);
   if (F.Ux != units || F.Uy != NW || F.total > max_smem) return false;
   cf.kind = kKindLine;
   cf.full = false;
   cf.pair = true;
+  cf.upw = upw;
   cf.ld = pair_ld(X);
   cf.NT = 32 * NW;
   cf.KX = kLineK;
@@ -461,13 +473,15 @@ bool chunk_cfg(int X, int Y, int C, int max_smem, bool gstate, Config& cf) {
 }
 
 // Built-in choice: the smallest cluster the line family fits in (paired
-// kernel, then full tiles, then any sizes), else the chunk family on chip,
-// else the chunk family on HBM.
+// kernel with two units per warp, then with one unit per warp -- numX == 32
+// --, then full tiles, then any sizes), else the chunk family on chip, else
+// the chunk family on HBM.
 template <typename S>
 Config default_config(int X, int Y, int max_smem) {
   Config cf;
   for (int C = 1; C <= kMaxCluster; C *= 2) {
     if (line_pair_cfg<S>(X, Y, C, max_smem, cf)) return cf;
+    if (line_pair_cfg<S>(X, Y, C, max_smem, cf, 1)) return cf;  // numX == 32
     if (line_full_cfg<S>(X, Y, C, max_smem, cf)) return cf;
     if (line_generic_cfg<S>(X, Y, C, max_smem, cf)) return cf;
   }
@@ -487,6 +501,7 @@ std::vector<Config> enum_configs(int X, int Y, int max_smem) {
   Config cf;
   for (int C = 1; C <= kMaxCluster; C *= 2) {
     if (line_pair_cfg<S>(X, Y, C, max_smem, cf)) v.push_back(cf);
+    if (line_pair_cfg<S>(X, Y, C, max_smem, cf, 1)) v.push_back(cf);
     if (line_full_cfg<S>(X, Y, C, max_smem, cf)) v.push_back(cf);
     if (line_generic_cfg<S>(X, Y, C, max_smem, cf) && (C == 1 || cf.Ycs >= 16)) v.push_back(cf);
   }
@@ -499,7 +514,8 @@ std::vector<Config> enum_configs(int X, int Y, int max_smem) {
 
 int family_of(const Config& c) {
   if (c.kind == kKindChunk) return LVC_FAMILY_CHUNK;
-  return c.pair ? LVC_FAMILY_LINE_PAIR : c.full ? LVC_FAMILY_LINE_FULL : LVC_FAMILY_LINE;
+  if (c.pair) return c.upw == 1 ? LVC_FAMILY_LINE_PAIR1 : LVC_FAMILY_LINE_PAIR;
+  return c.full ? LVC_FAMILY_LINE_FULL : LVC_FAMILY_LINE;
 }
 
 bool same_shape(const Config& a, const Config& b) {
@@ -522,7 +538,7 @@ Config choose_config(const futhark_context* ctx, int X, int Y) {
 
 template <typename S, typename PV>
 int prepare_launch(futhark_context* ctx, Launch& L, int max_sms = 0) {
-  RbFn<S, PV> fn = rollback_fn<S, PV>(L.kind, L.NT, L.KX, L.gstate, L.full, L.pair);
+  RbFn<S, PV> fn = rollback_fn<S, PV>(L.kind, L.NT, L.KX, L.gstate, L.full, L.pair, L.upw);
   if (!fn) return set_error(ctx, FUTHARK_PROGRAM_ERROR, "no rollback kernel for this configuration");
   // Several launch classes may share one kernel instantiation with different
   // shared-memory sizes: allow the device maximum once for all of them.
@@ -593,7 +609,7 @@ cudaError_t launch_rollback(lvc_plan* P, const Launch& L, cudaStream_t s) {
     cfg.attrs = &attr;
     cfg.numAttrs = 1;
   }
-  return cudaLaunchKernelEx(&cfg, rollback_fn<S, PV>(L.kind, L.NT, L.KX, L.gstate, L.full, L.pair), a);
+  return cudaLaunchKernelEx(&cfg, rollback_fn<S, PV>(L.kind, L.NT, L.KX, L.gstate, L.full, L.pair, L.upw), a);
 }
 
 // Enqueue one run of a plan.  `ev` (optional) receives a start/stop event
@@ -679,8 +695,8 @@ int plan_build(futhark_context* ctx, const lvc_calibration* cs, int n, lvc_plan*
   P->params.assign(cs, cs + n);
   P->calibs.resize(n);
   P->row_start.assign(n + 1, 0);
-  std::map<std::tuple<int, int, int, int, bool, bool, bool>, std::vector<std::pair<int64_t, Item>>> classes;
-  std::map<std::tuple<int, int, int, int, bool, bool, bool>, Config> class_cfg;
+  std::map<std::tuple<int, int, int, int, bool, bool, bool, int>, std::vector<std::pair<int64_t, Item>>> classes;
+  std::map<std::tuple<int, int, int, int, bool, bool, bool, int>, Config> class_cfg;
   int64_t tab_off = 0, piv_off = 0, out_off = 0;
   for (int i = 0; i < n; i++) {
     const lvc_calibration& c = cs[i];
@@ -705,7 +721,7 @@ int plan_build(futhark_context* ctx, const lvc_calibration* cs, int n, lvc_plan*
     d.out = out_off;
     out_off += c.outer;
     P->row_start[i + 1] = P->row_start[i] + (int64_t)(c.numT > 1 ? c.numT - 1 : 0) * c.numY;
-    const auto key = std::make_tuple(cf.kind, cf.NT, cf.KX, cf.C, cf.gstate, cf.full, cf.pair);
+    const auto key = std::make_tuple(cf.kind, cf.NT, cf.KX, cf.C, cf.gstate, cf.full, cf.pair, cf.upw);
     auto& cls = classes[key];
     auto it = class_cfg.find(key);
     if (it == class_cfg.end()) {
@@ -734,6 +750,7 @@ int plan_build(futhark_context* ctx, const lvc_calibration* cs, int n, lvc_plan*
     L.kind = cf.kind;
     L.full = cf.full;
     L.pair = cf.pair;
+    L.upw = cf.upw;
     L.NT = cf.NT;
     L.KX = cf.KX;
     L.C = cf.C;
@@ -1295,6 +1312,7 @@ int lvc_context_set_tuning_param(struct futhark_context* ctx, const char* param_
 namespace {
 
 const char* family_name(int fam, bool gstate) {
+  if (fam == LVC_FAMILY_LINE_PAIR1) return "line_pair1";
   if (fam == LVC_FAMILY_LINE_PAIR) return "line_pair";
   if (fam == LVC_FAMILY_LINE_FULL) return "line_full";
   if (fam == LVC_FAMILY_LINE) return "line";
@@ -1542,16 +1560,17 @@ int lvc_tuning_load(struct futhark_context* ctx, const char* path) {
     int X = 0, Y = 0, C = 0;
     unsigned long v = 0;
     char name[128];
-    if (sscanf(line, "lvc.shape.%15[a-z0-9].%dx%d=%15[a-z_],%d", prec, &X, &Y, fam, &C) == 5) {
+    if (sscanf(line, "lvc.shape.%15[a-z0-9].%dx%d=%15[a-z_0-9],%d", prec, &X, &Y, fam, &C) == 5) {
       lvc_shape sh{};
       sh.cluster = C;
       const std::string fs(fam);
-      sh.family = fs == "line_pair"   ? LVC_FAMILY_LINE_PAIR
+      sh.family = fs == "line_pair1"  ? LVC_FAMILY_LINE_PAIR1
+                  : fs == "line_pair" ? LVC_FAMILY_LINE_PAIR
                   : fs == "line_full" ? LVC_FAMILY_LINE_FULL
                   : fs == "line"      ? LVC_FAMILY_LINE
                                       : LVC_FAMILY_CHUNK;
       sh.hbm_state = fs == "chunk_hbm" ? 1 : 0;
-      const bool known = fs == "line_pair" || fs == "line_full" || fs == "line" || fs == "chunk" || fs == "chunk_hbm";
+      const bool known = fs == "line_pair1" || fs == "line_pair" || fs == "line_full" || fs == "line" || fs == "chunk" || fs == "chunk_hbm";
       const int p = !strcmp(prec, "f64") ? LVC_F64 : !strcmp(prec, "f32state") ? LVC_F32_STATE : -1;
       if (!known || p < 0) rc = 1;
       else rc = lvc_tuning_set(ctx, X, Y, p, &sh);
@@ -1744,6 +1763,7 @@ extern "C" int lvc_entry_main_f64_noalloc(struct futhark_context* ctx, double* p
     L.kind = cf.kind;
     L.full = cf.full;
     L.pair = cf.pair;
+    L.upw = cf.upw;
     L.NT = cf.NT;
     L.KX = cf.KX;
     L.C = cf.C;
@@ -1780,7 +1800,7 @@ extern "C" int lvc_entry_main_f64_noalloc(struct futhark_context* ctx, double* p
       cfg.attrs = &attr;
       cfg.numAttrs = 1;
     }
-    LVC_CUDA(ctx, cudaLaunchKernelEx(&cfg, rollback_fn<double, double>(L.kind, L.NT, L.KX, false, L.full, L.pair), a));
+    LVC_CUDA(ctx, cudaLaunchKernelEx(&cfg, rollback_fn<double, double>(L.kind, L.NT, L.KX, false, L.full, L.pair, L.upw), a));
   }
   int h = 0;
   LVC_CUDA(ctx, cudaMemcpyAsync(&h, d_err, sizeof(int), cudaMemcpyDeviceToHost, s));

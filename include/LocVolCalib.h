@@ -254,6 +254,7 @@ LVC_API int lvc_context_set_tuning_param(struct futhark_context *ctx, const char
 #define LVC_FAMILY_LINE 1      /* one lane per grid line, any sizes with numX <= 256 */
 #define LVC_FAMILY_LINE_FULL 2 /* line family on full 32 x 32 tiles (numX, rows per CTA multiples of 32) */
 #define LVC_FAMILY_LINE_PAIR 3 /* full tiles walked two columns at a time (numX % 64 == 0) */
+#define LVC_FAMILY_LINE_PAIR1 4 /* the same with one unit per warp: twice the warps (numX % 32 == 0) */
 
 struct lvc_shape {
   int32_t family;       /* LVC_FAMILY_* */
@@ -294,7 +295,7 @@ LVC_API int lvc_autotune(struct futhark_context *ctx, const struct lvc_calibrati
                          int32_t n, int32_t precision, int32_t probe_steps);
 /* The tuning parameters and the table as a tuning file of name=value lines:
  *   lvc.streams=4
- *   lvc.shape.f64.256x256=line_pair,8      (family: line_pair|line_full|line|chunk|chunk_hbm, cluster) */
+ *   lvc.shape.f64.256x256=line_pair,8      (family: line_pair|line_pair1|line_full|line|chunk|chunk_hbm, cluster) */
 LVC_API int lvc_tuning_save(struct futhark_context *ctx, const char *path);
 LVC_API int lvc_tuning_load(struct futhark_context *ctx, const char *path);
 
