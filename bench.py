@@ -191,17 +191,39 @@ def pick_sample(calibs, target_s):
 
 
 def cpu_baseline(calibs, target_s):
-    """Time the oracle (CPU restatement of the reference) on a bounded sample."""
+    """Time the oracle (CPU restatement of the reference) on a bounded sample.
+    Returns the baseline record and the oracle's prices of the sample (the
+    leading calibrations of the workload)."""
     from oracle import oracle
     sample, threads = pick_sample(calibs, target_s)
     t0 = time.perf_counter()
-    oracle.batch_f64(sample, threads=threads)
+    ref = oracle.batch_f64(sample, threads=threads)
     dt = time.perf_counter() - t0
     opts = sum(c.outer for c in sample)
     work = sum(c.work() for c in sample)
     return {"value": opts / dt, "unit": UNIT, "cores": threads, "kind": "port",
             "sample": f"first {len(sample)} calibrations of the workload ({opts} options, "
-                      f"{work:.3e} option-cell-steps), f64 oracle, {dt:.1f} s"}
+                      f"{work:.3e} option-cell-steps), f64 oracle, {dt:.1f} s"}, ref, sample
+
+
+def error_vs_oracle(got, ref, sample):
+    """Relative error of the engine's prices against the FP64 oracle: over all
+    prices, and over the prices above 1e-3 of their calibration's largest
+    (the FP32-state contract: 1e-4 there, 1e-7 absolute below)."""
+    import numpy as np
+    got = np.asarray(got[: len(ref)], dtype=np.float64)
+    rel = np.abs(got - ref) / np.maximum(np.abs(ref), 1e-300)
+    sig = np.zeros(len(ref), dtype=bool)
+    o = 0
+    for c in sample:
+        if c.outer:
+            blk = np.abs(ref[o:o + c.outer])
+            sig[o:o + c.outer] = blk > 1e-3 * blk.max()
+        o += c.outer
+    return {"max_rel": float(rel.max()) if rel.size else 0.0,
+            "max_rel_significant": float(rel[sig].max()) if sig.any() else 0.0,
+            "max_abs_below_significance": float(np.abs(got - ref)[~sig].max()) if (~sig).any() else 0.0,
+            "prices": int(len(ref)), "sample": "the cpu_baseline sample (leading calibrations of the workload)"}
 
 
 def run_reference(args):
@@ -387,9 +409,10 @@ def run_ours(args):
     if not args.no_serving:
         serving = run_serving(pkg, wl, ctx, args, rank, precision)
 
-    cpu = None
+    cpu = err = None
     if rank == 0 and world == 1:
-        cpu = cpu_baseline(calibs, args.cpu_seconds)
+        cpu, ref, sample = cpu_baseline(calibs, args.cpu_seconds)
+        err = error_vs_oracle(prices, ref, sample)
 
     default_workload = (args.workload == "uneven" and args.calibs == 512 and args.seed == 0
                         and args.precision == "f64")
@@ -425,6 +448,7 @@ def run_ours(args):
             "serving": serving,
             "batched_vs_plain": (value / plain["value"]) if plain else None,
             "cpu_baseline": cpu,
+            "error_vs_fp64_oracle": err,
             "clocks": clk,
         }
         print(json.dumps(line), flush=True)

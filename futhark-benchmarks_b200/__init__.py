@@ -131,6 +131,7 @@ def load_library(path: str = LIB_PATH):
         "lvc_shape_candidates": (ctypes.c_int, [vp, i32, i32, i32, ctypes.POINTER(Shape), i32, ctypes.POINTER(i32)]),
         "lvc_tuning_set": (ctypes.c_int, [vp, i32, i32, i32, ctypes.POINTER(Shape)]),
         "lvc_tuning_get": (ctypes.c_int, [vp, i32, i32, i32, ctypes.POINTER(TuningEntry)]),
+        "lvc_plan_shape": (ctypes.c_int, [vp, i32, ctypes.POINTER(Shape)]),
         "lvc_tuning_entries": (i32, [vp, ctypes.POINTER(TuningEntry), i32]),
         "lvc_autotune": (ctypes.c_int, [vp, ctypes.POINTER(_Calib), i32, i32, i32]),
         "lvc_tuning_save": (ctypes.c_int, [vp, ctypes.c_char_p]),
@@ -384,6 +385,13 @@ class Plan:
     @property
     def device_prices(self) -> int:
         return int(self.ctx.lib.lvc_plan_device_prices(self._p) or 0)
+
+    def shape(self, calib: int = 0) -> "Shape":
+        """The shape (kernel family, cluster size, ...) calibration `calib` runs under."""
+        sh = Shape()
+        if self.ctx.lib.lvc_plan_shape(self._p, calib, ctypes.byref(sh)):
+            raise FutharkError(FUTHARK_PROGRAM_ERROR, f"no calibration {calib} in this plan")
+        return sh
 
     def free(self):
         if self._p:

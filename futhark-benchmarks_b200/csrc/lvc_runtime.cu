@@ -210,6 +210,7 @@ struct lvc_plan {
   int64_t nprices = 0;
   std::vector<lvc_calibration> params;
   std::vector<CalibDev> calibs;
+  std::vector<Config> cfgs;  // the shape each calibration runs under
   std::vector<Launch> launches;
   std::vector<Item> items;
   std::vector<int64_t> row_start;
@@ -231,6 +232,7 @@ struct lvc_plan {
   int max_sms = 0;             // cap on the SMs a launch may occupy (0: all, <0: one CTA per item)
   double sms = 0.0;            // SMs the widest launch occupies
   int n_streams = 1;           // streams the launch classes fork over
+  uint64_t shapes_gen = 0;     // the context's tuning-table generation the plan was built under
   cudaStream_t aux[kMaxAux] = {};
   cudaEvent_t ev_fork = nullptr;
   cudaEvent_t ev_join[kMaxAux] = {};
@@ -250,6 +252,7 @@ struct futhark_context {
   TuningParams tuning;
   cudaStream_t aux[kMaxAux] = {};  // fork streams of the batch plans
   std::map<std::tuple<int, int, int>, TunedShape> shapes;  // (numX, numY, precision) -> tuned shape
+  uint64_t shapes_gen = 0;  // bumped on every change of `shapes`
 };
 
 namespace {
@@ -694,6 +697,7 @@ int plan_build(futhark_context* ctx, const lvc_calibration* cs, int n, lvc_plan*
   P->ncal = n;
   P->params.assign(cs, cs + n);
   P->calibs.resize(n);
+  P->cfgs.resize(n);
   P->row_start.assign(n + 1, 0);
   std::map<std::tuple<int, int, int, int, bool, bool, bool, int>, std::vector<std::pair<int64_t, Item>>> classes;
   std::map<std::tuple<int, int, int, int, bool, bool, bool, int>, Config> class_cfg;
@@ -702,6 +706,7 @@ int plan_build(futhark_context* ctx, const lvc_calibration* cs, int n, lvc_plan*
     const lvc_calibration& c = cs[i];
     if (int rc = validate(ctx, c, i)) return rc;
     const Config cf = choose_config<S>(ctx, c.numX, c.numY);
+    P->cfgs[i] = cf;
     CalibDev& d = P->calibs[i];
     d.numX = c.numX;
     d.numY = c.numY;
@@ -847,6 +852,7 @@ int plan_new_locked(futhark_context* ctx, const lvc_calibration* cs, int n, int 
   P->pool = pool;
   P->use_graph = use_graph;
   P->max_sms = max_sms;
+  P->shapes_gen = ctx->shapes_gen;
   if (use_graph && max_sms == 0) {  // batch plans follow the context's tuning
     P->max_sms = ctx->tuning.grid == 1 ? -1 : 0;
     P->n_streams = ctx->tuning.streams;
@@ -902,7 +908,9 @@ int entry_run(futhark_context* ctx, const lvc_calibration& c) {
   lvc_plan* P = ctx->entry_plan;
   if (P) {
     const lvc_calibration& o = P->params[0];
-    if (o.outer != c.outer || o.numX != c.numX || o.numY != c.numY || o.numT != c.numT) {
+    // rebuilt when the sizes change, or the tuning table (the shape) did
+    if (o.outer != c.outer || o.numX != c.numX || o.numY != c.numY || o.numT != c.numT ||
+        P->shapes_gen != ctx->shapes_gen) {
       LVC_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
       plan_release(P);
       P = ctx->entry_plan = nullptr;
@@ -1413,6 +1421,7 @@ int lvc_tuning_set(struct futhark_context* ctx, int32_t numX, int32_t numY, int3
   const TuneKey key{numX, numY, precision};
   if (!shape) {
     ctx->shapes.erase(key);
+    ctx->shapes_gen++;
     return 0;
   }
   for (const Config& c : candidates(ctx, numX, numY, precision)) {
@@ -1421,6 +1430,7 @@ int lvc_tuning_set(struct futhark_context* ctx, int32_t numX, int32_t numY, int3
       t.cf = c;
       t.tuned = true;
       ctx->shapes[key] = t;
+      ctx->shapes_gen++;
       return 0;
     }
   }
@@ -1444,6 +1454,12 @@ int lvc_tuning_get(struct futhark_context* ctx, int32_t numX, int32_t numY, int3
   } else {
     to_shape(builtin(ctx, numX, numY, precision), &out->shape);
   }
+  return 0;
+}
+
+int lvc_plan_shape(const struct lvc_plan* plan, int32_t calib, struct lvc_shape* out) {
+  if (!plan || !out || calib < 0 || calib >= plan->ncal) return FUTHARK_PROGRAM_ERROR;
+  to_shape(plan->cfgs[calib], out);
   return 0;
 }
 
@@ -1521,12 +1537,14 @@ int lvc_autotune(struct futhark_context* ctx, const struct lvc_calibration* cali
     if (any && same_shape(best.cf, def) && def_us > 0.0) best_us = def_us;
     if (!any) {
       ctx->shapes.erase(key);
+      ctx->shapes_gen++;
       return set_error(ctx, FUTHARK_PROGRAM_ERROR, "autotune: no shape ran for a grid class");
     }
     best.us_best = best_us;
     best.us_default = def_us;
     ctx->shapes[key] = best;
   }
+  ctx->shapes_gen++;
   return 0;
 }
 

@@ -282,6 +282,9 @@ LVC_API int lvc_shape_candidates(struct futhark_context *ctx, int32_t numX, int3
  * NULL returns the class to the built-in choice. */
 LVC_API int lvc_tuning_set(struct futhark_context *ctx, int32_t numX, int32_t numY,
                            int32_t precision, const struct lvc_shape *shape);
+/* The shape calibration `calib` of a plan runs under (FUTHARK_PROGRAM_ERROR
+ * for an index out of range). */
+LVC_API int lvc_plan_shape(const struct lvc_plan *plan, int32_t calib, struct lvc_shape *out);
 /* The shape the class runs under now (tuned or built-in). */
 LVC_API int lvc_tuning_get(struct futhark_context *ctx, int32_t numX, int32_t numY,
                            int32_t precision, struct lvc_tuning_entry *out);

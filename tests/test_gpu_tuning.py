@@ -36,6 +36,14 @@ def test_every_candidate_shape_matches_oracle(ctx, oracle, grid):
         for sh in cands:
             ctx.tuning_set(X, Y, 0, sh)
             assert ctx.tuning_get(X, Y, 0).shape.key() == sh.key()
+            # a fresh plan takes the pinned shape ...
+            plan = ctx.plan([c])
+            assert plan.shape(0).key() == sh.key()
+            plan.run()
+            assert rel_err(plan.prices(), exp) <= 1e-9, sh
+            plan.free()
+            # ... and so does the entry point, whose cached plan (same sizes on
+            # every pass of this loop) is rebuilt when the tuning table changes
             got = ctx.main_f64(*[getattr(c, k) for k in FIELDS])
             assert rel_err(got, exp) <= 1e-9, sh
     finally:
@@ -51,6 +59,9 @@ def test_every_candidate_shape_f32_state(ctx, oracle, grid):
     try:
         for sh in ctx.shape_candidates(X, Y, 1):
             ctx.tuning_set(X, Y, 1, sh)
+            plan = ctx.plan([c], precision=1)
+            assert plan.shape(0).key() == sh.key()
+            plan.free()
             got = ctx.batch([c], precision=1)
             assert rel_err(got[big], exp[big]) <= 1e-4, sh
             assert np.max(np.abs(got[~big] - exp[~big]), initial=0.0) <= 1e-7, sh
