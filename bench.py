@@ -47,7 +47,7 @@ F_ALG = 77
 # workload (uneven mix, 512 calibrations, seed 0, f64), from the ncu launch list
 # of `python bench.py --steps 2 --warmup 3 --no-plain --no-serving --cpu-seconds 3`
 # (dram__bytes_read.sum + dram__bytes_write.sum over the 13 plan runs / 13).
-ROLLBACK_DRAM_BYTES_DEFAULT = 355.982e9 / 13
+ROLLBACK_DRAM_BYTES_DEFAULT = 382.956e9 / 13
 CALIB_DEV_BYTES = 112  # sizeof(lvc::CalibDev) (static_assert in lvc_layout.h), uploaded per calibration per step
 
 
