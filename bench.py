@@ -425,7 +425,7 @@ def run_ours(args):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64" if precision == pkg.F64 else "f32-state (f64 pivots)",
+            "dtype": "f64" if precision == pkg.F64 else "f32-state (pivot divisions in f64)",
             "data": "synthetic (seeded calibration parameters; no dataset)",
             "config": dict(desc, precision=args.precision, options_per_rank=n_opts, autotune=tune,
                            option_cell_steps_per_rank=work,
