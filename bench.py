@@ -65,6 +65,7 @@ def parse():
                     help="time the plain per-call form on the first N calibrations (0 = all)")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--no-tridiag", action="store_true", help="skip the batched tridiagonal solver section")
     ap.add_argument("--no-autotune", action="store_true", help="built-in shapes instead of the autotuner's")
     ap.add_argument("--serving-rates", default="100,1000,5000,20000",
                     help="Poisson arrival rates (requests/s) of the serving sweep")
@@ -259,6 +260,81 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def hbm_peak():
+    """Measured HBM copy bandwidth (GB/s) of this pool's B200s, else the fallback."""
+    try:
+        with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback 6.65 TB/s"
+
+
+def run_tridiag(pkg, wl, ctx, args):
+    """The batched tridiagonal solvers (misc/ocean-sim/tridiag-test.fut) on the
+    benchmark stanza's [57600][115] f32 systems: device-resident time per launch
+    (L2 flushed between launches), end to end through the generated API with
+    host arrays, bit-exactness against the oracle on a sample, CPU baseline."""
+    import numpy as np
+    import torch
+    from oracle import oracle
+    rows, m = wl.TRIDIAG_BENCH
+    host = wl.tridiag_inputs(rows, m, seed=args.seed)
+    dev = [torch.from_numpy(v).cuda() for v in host]
+    out = torch.empty_like(dev[0])
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
+    ext = torch.cuda.ExternalStream(ctx.stream)
+    peak, peak_src = hbm_peak()
+    alg_bytes = 5 * rows * m * 4  # four inputs read, one output written
+    res = {"workload": f"[{rows}][{m}] f32 systems x 4 arrays, seeded uniform on the reference's "
+                       "dataset-script bounds (synthetic)", "algorithmic_bytes_per_launch": alg_bytes,
+           "peak_gbs": peak, "peak_source": peak_src}
+    sample = 2048
+    for form, oform in (("seq", "seq"), ("par", "par4")):
+        torch.cuda.synchronize()
+        for _ in range(max(3, args.warmup)):
+            ctx.tridag_device(form, rows, m, *[t.data_ptr() for t in dev], out.data_ptr())
+        ctx.sync()
+        times = []
+        for _ in range(max(5, args.steps)):
+            flush.zero_()
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(ext)
+            ctx.tridag_device(form, rows, m, *[t.data_ptr() for t in dev], out.data_ptr())
+            e1.record(ext)
+            ctx.sync()
+            times.append(e0.elapsed_time(e1))
+        ctx.tridag_check()
+        ms = float(np.median(times))
+        got = out[:sample].cpu().numpy()
+        exact = bool(np.array_equal(got, oracle.tridag(*[v[:sample] for v in host], form=oform)))
+        # end to end: host arrays in, host array out, through futhark_entry_tridagNested*
+        ctx.tridag(*host, form=form)
+        t0 = time.perf_counter()
+        reps = 3
+        for _ in range(reps):
+            ctx.tridag(*host, form=form)
+        e2e_ms = 1e3 * (time.perf_counter() - t0) / reps
+        gbs = alg_bytes / (ms * 1e-3) / 1e9
+        res[form] = {"entry": "tridagNested" if form == "par" else "tridagNestedSeq",
+                     "device_ms": ms, "systems_per_s": rows / (ms * 1e-3),
+                     "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s",
+                                  "frac": gbs / peak},
+                     "e2e_ms": e2e_ms, "e2e_systems_per_s": rows / (e2e_ms * 1e-3),
+                     "e2e_h2d_bytes": 4 * rows * m * 4, "e2e_d2h_bytes": rows * m * 4,
+                     "bit_exact_vs_oracle": exact, "oracle_sample_rows": sample}
+    # CPU baseline: the oracle (one thread) on a bounded sample of the systems
+    cpu_rows = rows
+    t0 = time.perf_counter()
+    oracle.tridag(*[v[:cpu_rows] for v in host], form="seq")
+    dt = time.perf_counter() - t0
+    res["cpu_baseline"] = {"value": cpu_rows / dt, "unit": "systems/s", "cores": 1, "kind": "port",
+                           "sample": f"all {cpu_rows} systems, tridagSeq oracle"}
+    del flush
+    return res
+
+
 def run_serving(pkg, wl, ctx, args, rank, precision):
     """Poisson request streams through the serving runtime (continuous batching)."""
     import numpy as np
@@ -405,6 +481,10 @@ def run_ours(args):
         plain = {"value": sum(c.outer for c in sub) / dt, "unit": UNIT,
                  "calls": len(sub), "form": "futhark_entry_main_f64 once per calibration"}
 
+    tridiag = None
+    if not args.no_tridiag and rank == 0:
+        tridiag = run_tridiag(pkg, wl, ctx, args)
+
     serving = None
     if not args.no_serving:
         serving = run_serving(pkg, wl, ctx, args, rank, precision)
@@ -446,6 +526,7 @@ def run_ours(args):
                          "smem_peak_gbs": smem_peak},
             "plain_per_call": plain,
             "serving": serving,
+            "tridiag": tridiag,
             "batched_vs_plain": (value / plain["value"]) if plain else None,
             "cpu_baseline": cpu,
             "error_vs_fp64_oracle": err,

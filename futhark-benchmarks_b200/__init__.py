@@ -163,6 +163,16 @@ def load_library(path: str = LIB_PATH):
         "lvc_plan_num_launches": (i32, [vp]),
         "lvc_batch": (ctypes.c_int, [vp, ctypes.POINTER(_Calib), i32, i32, vp]),
         "lvc_context_stream": (vp, [vp]),
+        "futhark_new_f32_2d": (vp, [vp, vp, i64, i64]),
+        "futhark_free_f32_2d": (ctypes.c_int, [vp, vp]),
+        "futhark_values_f32_2d": (ctypes.c_int, [vp, vp, vp]),
+        "futhark_shape_f32_2d": (ctypes.POINTER(i64), [vp, vp]),
+        "futhark_entry_tridagNested": (ctypes.c_int, [vp, ctypes.POINTER(vp), vp, vp, vp, vp]),
+        "futhark_entry_tridagNestedConst": (ctypes.c_int, [vp, ctypes.POINTER(vp), vp, vp, vp, vp]),
+        "futhark_entry_tridagNestedSeq": (ctypes.c_int, [vp, ctypes.POINTER(vp), vp, vp, vp, vp]),
+        "futhark_entry_tridagNestedSeqConst": (ctypes.c_int, [vp, ctypes.POINTER(vp), vp, vp, vp, vp]),
+        "lvc_tridag_f32": (ctypes.c_int, [vp, i32, i64, i64, vp, vp, vp, vp, vp]),
+        "lvc_tridag_check": (ctypes.c_int, [vp]),
         "lvc_probe_peaks": (ctypes.c_int, [vp, ctypes.POINTER(f64), ctypes.POINTER(f64)]),
         "lvc_server_new": (ctypes.c_int, [vp, ctypes.POINTER(_ServerConfig), ctypes.POINTER(vp)]),
         "lvc_server_submit": (ctypes.c_int, [vp, ctypes.POINTER(_Calib), ctypes.POINTER(ctypes.c_uint64)]),
@@ -287,6 +297,45 @@ class Context:
 
     def tuning_load(self, path: str):
         self._check(self.lib.lvc_tuning_load(self._ctx, str(path).encode()))
+
+    # -- batched tridiagonal solvers (misc/ocean-sim/tridiag-test.fut) ---------
+    TRIDAG_ENTRIES = {("par", False): "tridagNested", ("par", True): "tridagNestedConst",
+                      ("seq", False): "tridagNestedSeq", ("seq", True): "tridagNestedSeqConst"}
+
+    def tridag(self, a, b, c, y, form: str = "par", const: bool = False) -> np.ndarray:
+        """One of the four tridagNested* entry points on host [n][m] f32 arrays:
+        form "par" (tridagPar) or "seq" (tridagSeq); const requires m == 115."""
+        arrs = [np.ascontiguousarray(v, dtype=np.float32) for v in (a, b, c, y)]
+        if arrs[0].ndim != 2:
+            raise ValueError("tridag: 2-D arrays expected")
+        ins = []
+        try:
+            for v in arrs:
+                h = self.lib.futhark_new_f32_2d(self._ctx, v.ctypes.data, v.shape[0], v.shape[1])
+                if not h:
+                    raise FutharkError(FUTHARK_OUT_OF_MEMORY, self._take_error() or "futhark_new_f32_2d failed")
+                ins.append(h)
+            out = ctypes.c_void_p()
+            entry = getattr(self.lib, "futhark_entry_" + self.TRIDAG_ENTRIES[(form, bool(const))])
+            self._check(entry(self._ctx, ctypes.byref(out), *ins))
+            try:
+                shape = self.lib.futhark_shape_f32_2d(self._ctx, out)
+                res = np.empty((shape[0], shape[1]), dtype=np.float32)
+                self._check(self.lib.futhark_values_f32_2d(self._ctx, out, res.ctypes.data))
+            finally:
+                self.lib.futhark_free_f32_2d(self._ctx, out)
+            return res
+        finally:
+            for h in ins:
+                self.lib.futhark_free_f32_2d(self._ctx, h)
+
+    def tridag_device(self, form: str, rows: int, m: int, a: int, b: int, c: int, y: int, out: int):
+        """lvc_tridag_f32 on device pointers, asynchronous on this context's stream."""
+        self._check(self.lib.lvc_tridag_f32(self._ctx, 0 if form == "seq" else 1, rows, m, a, b, c, y, out))
+
+    def tridag_check(self):
+        """Raises if a device-pointer solve since the last check had a copy time out."""
+        self._check(self.lib.lvc_tridag_check(self._ctx))
 
     @property
     def stream(self) -> int:

@@ -25,7 +25,7 @@ ORACLE_DIR = os.path.join(REPO, "oracle")
 ORACLE_LIB = os.path.join(ORACLE_DIR, "liblvc_oracle.so")
 
 SOURCES = ["lvc_runtime.cu"]
-HEADERS = ["lvc_kernels.cuh", "lvc_layout.h", "lvc_probe.cuh", "lvc_line.cuh", "lvc_pair.cuh"]
+HEADERS = ["lvc_kernels.cuh", "lvc_layout.h", "lvc_probe.cuh", "lvc_line.cuh", "lvc_pair.cuh", "lvc_tridiag.cuh"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",
@@ -51,6 +51,7 @@ def _stale(target: str, deps) -> bool:
 def build_lib(force: bool = False, verbose: bool = False, extra=()) -> str:
     deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS]
     deps.append(os.path.join(REPO, "include", "LocVolCalib.h"))
+    deps.append(os.path.join(REPO, "include", "tridiag.h"))
     deps.append(os.path.abspath(__file__))
     if not force and not _stale(LIB, deps):
         return LIB

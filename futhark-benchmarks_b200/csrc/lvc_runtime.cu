@@ -34,6 +34,8 @@
 #include "lvc_kernels.cuh"
 #include "lvc_line.cuh"
 #include "lvc_pair.cuh"
+#include "lvc_tridiag.cuh"
+#include "tridiag.h"
 #include "lvc_probe.cuh"
 
 using namespace lvc;
@@ -85,6 +87,11 @@ struct futhark_f32_1d {
 struct futhark_f64_1d {
   double* data;
   int64_t shape[1];
+  size_t bytes;
+};
+struct futhark_f32_2d {
+  float* data;
+  int64_t shape[2];
   size_t bytes;
 };
 
@@ -2239,6 +2246,201 @@ int lvc_server_free(struct lvc_server* S) {
   cudaStreamDestroy(S->sctx.capture);
   delete S;
   return 0;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Batched tridiagonal solvers: the entry points of the tridiagonal test
+// program (misc/ocean-sim/tridiag-test.fut:14-26) on the same contexts.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int64_t kTridagInnerDim = 115;  // INNER_DIM of tridiag-test.fut:4
+
+// Enqueues one batched solve on ctx->stream (device pointers).  Called with
+// ctx->mu held.  m <= 400: the block kernel (no scratch); larger m: scratch
+// from the context's device pool (stream-ordered: every user of that pool
+// runs on ctx->stream).
+int tridag_check_locked(futhark_context* ctx) {
+  int flag = 0;  // a bulk copy that never landed (its systems are NaN)
+  LVC_CUDA(ctx, cudaMemcpyFromSymbolAsync(&flag, lvc_tridag_err, sizeof flag, 0, cudaMemcpyDeviceToHost, ctx->stream));
+  LVC_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if (flag) {
+    const int zero = 0;
+    cudaMemcpyToSymbol(lvc_tridag_err, &zero, sizeof zero);
+    return set_error(ctx, FUTHARK_PROGRAM_ERROR, "tridiagonal solve: a bulk copy timed out");
+  }
+  return 0;
+}
+
+int tridag_launch(futhark_context* ctx, int form, int64_t rows, int64_t m, const float* a, const float* b,
+                  const float* c, const float* y, float* out) {
+  if (rows < 0 || m < 0 || m > INT32_MAX) return set_error(ctx, FUTHARK_PROGRAM_ERROR, "bad tridiagonal batch shape");
+  if (rows == 0 || m == 0) return 0;
+  if (m <= kTriBlockMaxM) {  // one warp per 32 systems, staged through shared memory
+    const int64_t nblk = (rows + kTriBlockRows - 1) / kTriBlockRows;
+    if (nblk > INT32_MAX) return set_error(ctx, FUTHARK_PROGRAM_ERROR, "tridiagonal batch too large");
+    auto aligned = [](const void* p) { return ((uintptr_t)p & 15) == 0; };
+    const int vec = aligned(a) && aligned(b) && aligned(c) && aligned(y) && aligned(out);
+    const size_t bs = (size_t)((kTriBlockRows * m + 3) & ~int64_t(3));
+    const size_t smem_blk = 16 + 4 * bs * sizeof(float);  // mbarrier + four blocks
+    auto fb = form == 0 ? lvc_tridag_block_kernel<0> : lvc_tridag_block_kernel<1>;
+    const size_t smem_max = 16 + 4 * (size_t)((kTriBlockRows * kTriBlockMaxM + 3) & ~3) * sizeof(float);
+    LVC_CUDA(ctx, cudaFuncSetAttribute((const void*)fb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max));
+    fb<<<(unsigned)nblk, kTriBlockRows, smem_blk, ctx->stream>>>(rows, (int)m, a, b, c, y, out, vec);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "tridiagonal launch");
+    return 0;
+  }
+  const int64_t blocks = (rows + kTriThreads - 1) / kTriThreads;
+  if (blocks > INT32_MAX) return set_error(ctx, FUTHARK_PROGRAM_ERROR, "tridiagonal batch too large");
+  if (!ctx->pool) ctx->pool = new DevicePool();
+  float* gscratch = static_cast<float*>(ctx->pool->alloc(sizeof(float) * (size_t)m * (size_t)rows));
+  if (!gscratch) return set_error(ctx, FUTHARK_OUT_OF_MEMORY, "out of device memory for tridiagonal scratch");
+  auto fn = form == 0 ? lvc_tridag_kernel<0> : lvc_tridag_kernel<1>;
+  fn<<<(unsigned)blocks, kTriThreads, 0, ctx->stream>>>(rows, (int)m, a, b, c, y, out, gscratch);
+  const cudaError_t e = cudaGetLastError();
+  ctx->pool->release(gscratch);  // later users of the pool are ordered after this launch
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "tridiagonal launch");
+  return 0;
+}
+
+int tridag_entry(futhark_context* ctx, futhark_f32_2d** out0, const futhark_f32_2d* a, const futhark_f32_2d* b,
+                 const futhark_f32_2d* c, const futhark_f32_2d* y, int form, int64_t need_m) {
+  std::lock_guard<std::mutex> g(ctx->mu);
+  if (!ctx->ok) return set_error(ctx, FUTHARK_PROGRAM_ERROR, "context has no usable CUDA device");
+  if (!out0 || !a || !b || !c || !y) return set_error(ctx, FUTHARK_PROGRAM_ERROR, "null array");
+  const int64_t rows = a->shape[0], m = a->shape[1];
+  for (const futhark_f32_2d* v : {b, c, y})
+    if (v->shape[0] != rows || v->shape[1] != m)
+      return set_error(ctx, FUTHARK_PROGRAM_ERROR, "tridiagonal entry: the four input arrays differ in shape");
+  if (need_m >= 0 && m != need_m) {
+    char buf[160];
+    snprintf(buf, sizeof buf, "tridiagonal entry: inner dimension %lld does not match the required %lld",
+             (long long)m, (long long)need_m);
+    return set_error(ctx, FUTHARK_PROGRAM_ERROR, buf);
+  }
+  LVC_CUDA(ctx, cudaSetDevice(ctx->device));
+  auto* o = new (std::nothrow) futhark_f32_2d();
+  if (!o) return set_error(ctx, FUTHARK_OUT_OF_MEMORY, "out of host memory");
+  o->shape[0] = rows;
+  o->shape[1] = m;
+  o->bytes = sizeof(float) * (size_t)std::max<int64_t>(1, rows * m);
+  if (cudaMalloc(&o->data, o->bytes) != cudaSuccess) {
+    delete o;
+    cudaGetLastError();
+    return set_error(ctx, FUTHARK_OUT_OF_MEMORY, "out of device memory");
+  }
+  int rc = tridag_launch(ctx, form, rows, m, a->data, b->data, c->data, y->data, o->data);
+  if (!rc) rc = tridag_check_locked(ctx);
+  if (rc) {
+    cudaFree(o->data);
+    delete o;
+    return rc;
+  }
+  *out0 = o;
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+struct futhark_f32_2d* futhark_new_f32_2d(struct futhark_context* ctx, const float* data, int64_t dim0,
+                                          int64_t dim1) {
+  std::lock_guard<std::mutex> g(ctx->mu);
+  if (!ctx->ok || dim0 < 0 || dim1 < 0) {
+    ctx->error = "cannot create array";
+    return nullptr;
+  }
+  cudaSetDevice(ctx->device);
+  auto* a = new (std::nothrow) futhark_f32_2d();
+  if (!a) return nullptr;
+  a->shape[0] = dim0;
+  a->shape[1] = dim1;
+  const int64_t n = dim0 * dim1;
+  a->bytes = sizeof(float) * (size_t)std::max<int64_t>(1, n);
+  if (cudaMalloc(&a->data, a->bytes) != cudaSuccess) {
+    cudaGetLastError();
+    ctx->error = "out of device memory";
+    delete a;
+    return nullptr;
+  }
+  if (n > 0 && data &&
+      cudaMemcpyAsync(a->data, data, sizeof(float) * n, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess) {
+    cudaFree(a->data);
+    delete a;
+    ctx->error = "host to device copy failed";
+    return nullptr;
+  }
+  cudaStreamSynchronize(ctx->stream);
+  return a;
+}
+
+int futhark_free_f32_2d(struct futhark_context* ctx, struct futhark_f32_2d* arr) {
+  if (!arr) return 0;
+  std::lock_guard<std::mutex> g(ctx->mu);
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  cudaFree(arr->data);
+  delete arr;
+  return 0;
+}
+
+int futhark_values_f32_2d(struct futhark_context* ctx, struct futhark_f32_2d* arr, float* data) {
+  std::lock_guard<std::mutex> g(ctx->mu);
+  if (!arr) return set_error(ctx, FUTHARK_PROGRAM_ERROR, "null array");
+  LVC_CUDA(ctx, cudaSetDevice(ctx->device));
+  const int64_t n = arr->shape[0] * arr->shape[1];
+  if (n > 0)
+    LVC_CUDA(ctx, cudaMemcpyAsync(data, arr->data, sizeof(float) * n, cudaMemcpyDeviceToHost, ctx->stream));
+  LVC_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return 0;
+}
+
+const int64_t* futhark_shape_f32_2d(struct futhark_context* ctx, struct futhark_f32_2d* arr) {
+  (void)ctx;
+  return arr ? arr->shape : nullptr;
+}
+
+int futhark_entry_tridagNested(struct futhark_context* ctx, struct futhark_f32_2d** out0,
+                               const struct futhark_f32_2d* in0, const struct futhark_f32_2d* in1,
+                               const struct futhark_f32_2d* in2, const struct futhark_f32_2d* in3) {
+  return tridag_entry(ctx, out0, in0, in1, in2, in3, 1, -1);
+}
+int futhark_entry_tridagNestedConst(struct futhark_context* ctx, struct futhark_f32_2d** out0,
+                                    const struct futhark_f32_2d* in0, const struct futhark_f32_2d* in1,
+                                    const struct futhark_f32_2d* in2, const struct futhark_f32_2d* in3) {
+  return tridag_entry(ctx, out0, in0, in1, in2, in3, 1, kTridagInnerDim);
+}
+int futhark_entry_tridagNestedSeq(struct futhark_context* ctx, struct futhark_f32_2d** out0,
+                                  const struct futhark_f32_2d* in0, const struct futhark_f32_2d* in1,
+                                  const struct futhark_f32_2d* in2, const struct futhark_f32_2d* in3) {
+  return tridag_entry(ctx, out0, in0, in1, in2, in3, 0, -1);
+}
+int futhark_entry_tridagNestedSeqConst(struct futhark_context* ctx, struct futhark_f32_2d** out0,
+                                       const struct futhark_f32_2d* in0, const struct futhark_f32_2d* in1,
+                                       const struct futhark_f32_2d* in2, const struct futhark_f32_2d* in3) {
+  return tridag_entry(ctx, out0, in0, in1, in2, in3, 0, kTridagInnerDim);
+}
+
+int lvc_tridag_f32(struct futhark_context* ctx, int32_t form, int64_t rows, int64_t m, const float* a,
+                   const float* b, const float* c, const float* y, float* out) {
+  std::lock_guard<std::mutex> g(ctx->mu);
+  if (!ctx->ok) return set_error(ctx, FUTHARK_PROGRAM_ERROR, "context has no usable CUDA device");
+  if (form != LVC_TRIDAG_SEQ && form != LVC_TRIDAG_PAR)
+    return set_error(ctx, FUTHARK_PROGRAM_ERROR, "unknown tridiagonal form");
+  if (rows * m > 0 && (!a || !b || !c || !y || !out)) return set_error(ctx, FUTHARK_PROGRAM_ERROR, "null pointer");
+  LVC_CUDA(ctx, cudaSetDevice(ctx->device));
+  return tridag_launch(ctx, form == LVC_TRIDAG_SEQ ? 0 : 1, rows, m, a, b, c, y, out);
+}
+
+int lvc_tridag_check(struct futhark_context* ctx) {
+  std::lock_guard<std::mutex> g(ctx->mu);
+  if (!ctx->ok) return set_error(ctx, FUTHARK_PROGRAM_ERROR, "context has no usable CUDA device");
+  LVC_CUDA(ctx, cudaSetDevice(ctx->device));
+  return tridag_check_locked(ctx);
 }
 
 }  // extern "C"

@@ -1,0 +1,327 @@
+// Batched tridiagonal solvers: the tridagNested* entry points of
+// misc/ocean-sim/tridiag-test.fut:14-26 (f32, one system per row of
+// [rows][m] arrays).
+//
+//   FORM 0  tridagSeq (misc/ocean-sim/tridiag.fut:81-95): normalised Thomas.
+//   FORM 1  tridagPar (misc/ocean-sim/tridiag.fut:4-79): the three scans --
+//           4-tuple matrix scan for the pivots, two linear-function scans --
+//           folded left to right.
+//
+// Two kernels, one thread per system in both: lvc_tridag_block_kernel (m up
+// to 400, the common case) stages a warp's 32 systems through shared memory
+// with coalesced copies; lvc_tridag_kernel (any m) reads rows in place.
+// Each recurrence runs in the reference's operation
+// order with every product, sum and quotient explicitly rounded (no fused
+// multiply-add), so a system's solution is bit for bit the one the CPU
+// restatement of the same fold gives.  The work is a handful of operations per
+// element against 20 bytes of HBM traffic (four inputs, one output): the kernel
+// is bound by HBM and by the latency of the sequential recurrence, which the
+// many independent systems of a batch hide.  lvc_tridag_kernel keeps its
+// per-row scratch (the pivots of FORM 1, the normalised super-diagonal of
+// FORM 0) in a global [element][row] buffer -- consecutive threads at
+// consecutive addresses -- and the right-hand side of the backward pass in the
+// output row itself.
+#pragma once
+
+#include <cstdint>
+
+#include "lvc_line.cuh"  // mbarrier and bulk-copy helpers
+
+namespace lvc {
+
+// Set by lvc_tridag_block_kernel when a bulk-copy wait gave up (its systems
+// then come out as NaN); reset and read by the host around each launch.
+__device__ int lvc_tridag_err;
+
+constexpr int kTriThreads = 128;  // threads (systems) per CTA of lvc_tridag_kernel
+
+__device__ __forceinline__ float tri_mul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float tri_add(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float tri_sub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float tri_div(float a, float b) { return __fdiv_rn(a, b); }
+// 1 / x correctly rounded: the same value as tri_div(1.0f, x), cheaper
+__device__ __forceinline__ float tri_rcp(float x) { return __frcp_rn(x); }
+
+template <int FORM>
+__global__ void __launch_bounds__(kTriThreads) lvc_tridag_kernel(int64_t rows, int m, const float* __restrict__ a,
+                                                                const float* __restrict__ b,
+                                                                const float* __restrict__ c,
+                                                                const float* __restrict__ y,
+                                                                float* __restrict__ out,
+                                                                float* __restrict__ gscratch) {
+  const int64_t r = (int64_t)blockIdx.x * kTriThreads + threadIdx.x;
+  if (r >= rows) return;  // no barrier below: threads are independent
+  const float* ar = a + r * m;
+  const float* br = b + r * m;
+  const float* cr = c + r * m;
+  const float* yr = y + r * m;
+  float* o = out + r * m;
+  float* scr = gscratch + r;
+  const int64_t sstride = rows;  // element i of this row's scratch at scr[i * sstride]
+
+  if constexpr (FORM == 0) {
+    // forward: cp_i = c_i / (b_i - a_i cp_{i-1}), yp_i = (y_i - a_i yp_{i-1}) / (...)  (:82-91)
+    float cp = tri_div(cr[0], br[0]);
+    float yp = tri_div(yr[0], br[0]);
+    scr[0] = cp;
+    o[0] = yp;
+    for (int i = 1; i < m; i++) {
+      const float ai = ar[i];
+      const float nf = tri_rcp(tri_sub(br[i], tri_mul(ai, cp)));
+      cp = tri_mul(cr[i], nf);
+      yp = tri_mul(tri_sub(yr[i], tri_mul(ai, yp)), nf);
+      scr[i * sstride] = cp;
+      o[i] = yp;
+    }
+    // backward: x_i = yp_i - cp_i x_{i+1}  (:92-95)
+    float x = yp;
+    for (int i = m - 2; i >= 0; i--) {
+      x = tri_sub(o[i], tri_mul(scr[i * sstride], x));
+      o[i] = x;
+    }
+  } else {
+    // Recurrence 1 (:9-33): b'_i from the scan of (b_i, -a_i c_{i-1}, 1, 0)
+    const float b0 = br[0];
+    float s0 = 1.0f, s1 = 0.0f, s2 = 0.0f, s3 = 1.0f;
+    for (int i = 0; i < m; i++) {
+      float m0 = 1.0f, m1 = 0.0f, m2 = 0.0f, m3 = 1.0f;
+      if (0 < i) {
+        m0 = br[i];
+        m1 = tri_sub(0.0f, tri_mul(ar[i], cr[i - 1]));
+        m2 = 1.0f;
+        m3 = 0.0f;
+      }
+      const float value = tri_rcp(tri_mul(s0, m0));
+      const float n0 = tri_mul(tri_add(tri_mul(m0, s0), tri_mul(m1, s2)), value);
+      const float n1 = tri_mul(tri_add(tri_mul(m0, s1), tri_mul(m1, s3)), value);
+      const float n2 = tri_mul(tri_add(tri_mul(m2, s0), tri_mul(m3, s2)), value);
+      const float n3 = tri_mul(tri_add(tri_mul(m2, s1), tri_mul(m3, s3)), value);
+      s0 = n0;
+      s1 = n1;
+      s2 = n2;
+      s3 = n3;
+      scr[i * sstride] = tri_div(tri_add(tri_mul(s0, b0), s1), tri_add(tri_mul(s2, b0), s3));
+    }
+    // Recurrence 2 (:38-56): y'_i = y_i - (a_i / b'_{i-1}) y'_{i-1}, into the output row
+    const float y0 = yr[0];
+    float c0 = 0.0f, c1 = 1.0f;
+    for (int i = 0; i < m; i++) {
+      float l0 = 0.0f, l1 = 1.0f;
+      if (0 < i) {
+        l0 = yr[i];
+        l1 = tri_sub(0.0f, tri_div(ar[i], scr[(i - 1) * sstride]));
+      }
+      const float n0 = tri_add(l0, tri_mul(l1, c0));
+      const float n1 = tri_mul(c1, l1);
+      c0 = n0;
+      c1 = n1;
+      o[i] = tri_add(c0, tri_mul(c1, y0));
+    }
+    // Recurrence 3 (:61-79): backward, over the reversed index
+    const float yn = tri_div(o[m - 1], scr[(int64_t)(m - 1) * sstride]);
+    c0 = 0.0f;
+    c1 = 1.0f;
+    for (int k = 0; k < m; k++) {
+      const int i = m - k - 1;
+      float l0 = 0.0f, l1 = 1.0f;
+      if (0 < k) {
+        const float bi = scr[i * sstride];
+        l0 = tri_div(o[i], bi);
+        l1 = tri_sub(0.0f, tri_div(cr[i], bi));
+      }
+      const float n0 = tri_add(l0, tri_mul(l1, c0));
+      const float n1 = tri_mul(c1, l1);
+      c0 = n0;
+      c1 = n1;
+      o[i] = tri_add(c0, tri_mul(c1, yn));
+    }
+  }
+}
+
+// Block kernel: one warp per 32 consecutive systems.  In row-major [rows][m]
+// arrays those systems are one contiguous block of 32*m floats per array, so
+// the warp copies the four input blocks into shared memory with coalesced
+// 16-byte loads, each lane then runs its system's recurrences out of shared
+// memory (row stride m: for odd m the 32 lanes hit 32 different banks), and
+// the solution block goes back with coalesced stores.  Every intermediate
+// overwrites an input element that is no longer needed -- FORM 0: cp_i over
+// c_i, yp_i and then x_i over y_i; FORM 1: b'_i over b_i, y'_i and then x_i
+// over y_i -- so the shared memory is exactly the four input blocks.  The
+// arithmetic and its order are those of lvc_tridag_kernel.
+// When the arrays are 16-byte aligned and a block's bytes a multiple of 16
+// (every full block: 32 * m * 4 bytes), one thread moves the blocks with TMA
+// bulk copies (four in, one out) -- tens of kilobytes in flight per CTA,
+// which a warp's own loads cannot keep up; otherwise the warp copies.
+constexpr int kTriBlockRows = 32;
+constexpr int kTriBlockMaxM = 400;  // 4 x 32 x 400 floats = 200 KB of shared memory
+
+__device__ __forceinline__ void tri_copy_in(float* dst, const float* __restrict__ src, int64_t n, bool vec, int lane) {
+  if (vec) {
+    const int64_t n4 = n >> 2;
+    const float4* s4 = reinterpret_cast<const float4*>(src);
+    float4* d4 = reinterpret_cast<float4*>(dst);
+    for (int64_t k = lane; k < n4; k += 32) d4[k] = __ldcs(s4 + k);  // read once: streaming
+    for (int64_t k = (n4 << 2) + lane; k < n; k += 32) dst[k] = __ldcs(src + k);
+  } else {
+    for (int64_t k = lane; k < n; k += 32) dst[k] = __ldcs(src + k);
+  }
+}
+
+__device__ __forceinline__ void tri_bulk_s2g(void* dst, const void* src, unsigned bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;\n" ::"l"(dst), "r"(smem_u32(src)),
+               "r"(bytes)
+               : "memory");
+}
+
+template <int FORM>
+__global__ void __launch_bounds__(32) lvc_tridag_block_kernel(int64_t rows, int m, const float* __restrict__ a,
+                                                             const float* __restrict__ b,
+                                                             const float* __restrict__ c,
+                                                             const float* __restrict__ y,
+                                                             float* __restrict__ out, int vec) {
+  extern __shared__ __align__(16) unsigned char tri_raw[];
+  uint64_t* bar = reinterpret_cast<uint64_t*>(tri_raw);
+  float* tri_blk = reinterpret_cast<float*>(tri_raw + 16);
+  const int lane = threadIdx.x;
+  const int64_t r0 = (int64_t)blockIdx.x * kTriBlockRows;
+  const int nr = (int)(rows - r0 < kTriBlockRows ? rows - r0 : kTriBlockRows);
+  const int64_t n = (int64_t)nr * m;
+  const int64_t bs = (int64_t)kTriBlockRows * m + 3 & ~int64_t(3);  // per-array block, 16-byte aligned
+  float* sa = tri_blk;
+  float* sb = sa + bs;
+  float* scc = sb + bs;
+  float* sy = scc + bs;
+  const int64_t off = r0 * m;
+  const unsigned bytes = (unsigned)(n * sizeof(float));
+  const bool bulk = vec && (bytes % 16) == 0;
+  if (bulk) {
+    if (lane == 0) {
+      mbar_init(bar, 1);
+      asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+      mbar_expect_tx(bar, 4 * bytes);
+      bulk_g2s(sa, a + off, bytes, bar);
+      bulk_g2s(sb, b + off, bytes, bar);
+      bulk_g2s(scc, c + off, bytes, bar);
+      bulk_g2s(sy, y + off, bytes, bar);
+    }
+    __syncwarp();
+    if (!mbar_wait(bar, 0)) {
+      // the copies did not land: flag it, give them one more bounded wait,
+      // and leave NaN where these systems' solutions go
+      if (lane == 0) atomicExch(&lvc_tridag_err, 1);
+      mbar_wait(bar, 0);
+      for (int64_t k = lane; k < n; k += 32) out[off + k] = __int_as_float(0x7fc00000);
+      return;
+    }
+  } else {
+    tri_copy_in(sa, a + off, n, vec, lane);
+    tri_copy_in(sb, b + off, n, vec, lane);
+    tri_copy_in(scc, c + off, n, vec, lane);
+    tri_copy_in(sy, y + off, n, vec, lane);
+  }
+  __syncwarp();
+  if (lane < nr) {
+    const float* ar = sa + (int64_t)lane * m;
+    float* br = sb + (int64_t)lane * m;
+    float* cr = scc + (int64_t)lane * m;
+    float* yr = sy + (int64_t)lane * m;
+    if constexpr (FORM == 0) {
+      float cp = tri_div(cr[0], br[0]);
+      float yp = tri_div(yr[0], br[0]);
+      cr[0] = cp;
+      yr[0] = yp;
+      for (int i = 1; i < m; i++) {
+        const float ai = ar[i];
+        const float nf = tri_rcp(tri_sub(br[i], tri_mul(ai, cp)));
+        cp = tri_mul(cr[i], nf);
+        yp = tri_mul(tri_sub(yr[i], tri_mul(ai, yp)), nf);
+        cr[i] = cp;
+        yr[i] = yp;
+      }
+      float x = yp;
+      for (int i = m - 2; i >= 0; i--) {
+        x = tri_sub(yr[i], tri_mul(cr[i], x));
+        yr[i] = x;
+      }
+    } else {
+      const float b0 = br[0];
+      float s0 = 1.0f, s1 = 0.0f, s2 = 0.0f, s3 = 1.0f;
+      float cprev = 0.0f;  // c_{i-1}, read before b'_{i-1} replaced b_{i-1} (c is not overwritten)
+      for (int i = 0; i < m; i++) {
+        float m0 = 1.0f, m1 = 0.0f, m2 = 0.0f, m3 = 1.0f;
+        if (0 < i) {
+          m0 = br[i];
+          m1 = tri_sub(0.0f, tri_mul(ar[i], cprev));
+          m2 = 1.0f;
+          m3 = 0.0f;
+        }
+        cprev = cr[i];
+        const float value = tri_rcp(tri_mul(s0, m0));
+        const float n0 = tri_mul(tri_add(tri_mul(m0, s0), tri_mul(m1, s2)), value);
+        const float n1 = tri_mul(tri_add(tri_mul(m0, s1), tri_mul(m1, s3)), value);
+        const float n2 = tri_mul(tri_add(tri_mul(m2, s0), tri_mul(m3, s2)), value);
+        const float n3 = tri_mul(tri_add(tri_mul(m2, s1), tri_mul(m3, s3)), value);
+        s0 = n0;
+        s1 = n1;
+        s2 = n2;
+        s3 = n3;
+        br[i] = tri_div(tri_add(tri_mul(s0, b0), s1), tri_add(tri_mul(s2, b0), s3));  // b'_i
+      }
+      const float y0 = yr[0];
+      float c0 = 0.0f, c1 = 1.0f;
+      for (int i = 0; i < m; i++) {
+        float l0 = 0.0f, l1 = 1.0f;
+        if (0 < i) {
+          l0 = yr[i];
+          l1 = tri_sub(0.0f, tri_div(ar[i], br[i - 1]));
+        }
+        const float n0 = tri_add(l0, tri_mul(l1, c0));
+        const float n1 = tri_mul(c1, l1);
+        c0 = n0;
+        c1 = n1;
+        yr[i] = tri_add(c0, tri_mul(c1, y0));  // y'_i over y_i (y_i already read)
+      }
+      const float yn = tri_div(yr[m - 1], br[m - 1]);
+      c0 = 0.0f;
+      c1 = 1.0f;
+      for (int k = 0; k < m; k++) {
+        const int i = m - k - 1;
+        float l0 = 0.0f, l1 = 1.0f;
+        if (0 < k) {
+          const float bi = br[i];
+          l0 = tri_div(yr[i], bi);
+          l1 = tri_sub(0.0f, tri_div(cr[i], bi));
+        }
+        const float n0 = tri_add(l0, tri_mul(l1, c0));
+        const float n1 = tri_mul(c1, l1);
+        c0 = n0;
+        c1 = n1;
+        yr[i] = tri_add(c0, tri_mul(c1, yn));
+      }
+    }
+  }
+  float* dst = out + off;
+  if (bulk) {
+    // the lanes' shared-memory writes, then one thread's bulk store
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    __syncwarp();
+    if (lane == 0) {
+      tri_bulk_s2g(dst, sy, bytes);
+      asm volatile("cp.async.bulk.commit_group;\n" ::: "memory");
+      asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory");  // sy read before the CTA exits
+    }
+    return;
+  }
+  __syncwarp();
+  if (vec) {
+    const int64_t n4 = n >> 2;
+    const float4* s4 = reinterpret_cast<const float4*>(sy);
+    float4* d4 = reinterpret_cast<float4*>(dst);
+    for (int64_t k = lane; k < n4; k += 32) __stcs(d4 + k, s4[k]);
+    for (int64_t k = (n4 << 2) + lane; k < n; k += 32) __stcs(dst + k, sy[k]);
+  } else {
+    for (int64_t k = lane; k < n; k += 32) __stcs(dst + k, sy[k]);
+  }
+}
+
+}  // namespace lvc

@@ -58,3 +58,17 @@ def poisson_arrivals(rate: float, n: int, seed: int = 0) -> np.ndarray:
     """Arrival times (seconds) of n requests of a Poisson process of `rate` per second."""
     rng = np.random.default_rng(seed)
     return np.cumsum(rng.exponential(1.0 / rate, size=n))
+
+
+# Batched tridiagonal systems of misc/ocean-sim/tridiag-test.fut: [rows][m] f32
+# arrays a, b, c, y drawn uniformly from the bounds the reference's dataset
+# script gives futhark dataset (misc/ocean-sim/data/rand-dataset-tridiag.sh:
+# a 0.3:1.3, b 0.4:1.4, c 0.5:1.5, y 0.2:1.2), here from a seeded numpy
+# generator.  The benchmark stanza's size is [57600][115] (tridiag-test.fut:12).
+TRIDIAG_BOUNDS = ((0.3, 1.3), (0.4, 1.4), (0.5, 1.5), (0.2, 1.2))
+TRIDIAG_BENCH = (57600, 115)
+
+
+def tridiag_inputs(rows: int, m: int, seed: int = 0):
+    rng = np.random.default_rng(seed)
+    return tuple(rng.uniform(lo, hi, size=(rows, m)).astype(np.float32) for lo, hi in TRIDIAG_BOUNDS)

@@ -22,7 +22,8 @@
 //   lvc_oracle_main_f32 / _f64           : the reference `main` (:238-252)
 //   lvc_oracle_value_f32 / _f64          : the reference `value` (:211-236)
 //   lvc_oracle_batch_f64                 : many calibrations, prices concatenated
-//   lvc_oracle_tridag_{par,seq}_{f32,f64}: row-batched tridiagonal solvers
+//   lvc_oracle_tridag_{par,par4,seq}_{f32,f64}: row-batched tridiagonal solvers
+//     (par: LocVolCalib.fut's tridagPar; par4: misc/ocean-sim/tridiag.fut's)
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -194,6 +195,77 @@ void tridag_par(int64_t n, const T* a, const T* b, const T* c, const T* y, T* ou
     c0 = n0;
     c1 = n1;
     out[i] = c0 + c1 * yn;  // the reverse of :122-123
+  }
+}
+
+// misc/ocean-sim/tridiag.fut:4-79 (the tridagPar of the tridiagonal test
+// program): recurrence 1 as a scan of 4-tuple matrices normalised by
+// 1/(a0*b0) (:9-33), recurrences 2 and 3 as in tridag_par above (:38-79); the
+// scans folded left to right, accumulator as the operator's first argument.
+template <typename T>
+void tridag_par4(int64_t n, const T* a, const T* b, const T* c, const T* y, T* out,
+                 T* bp, T* yp) {
+  const T b0 = b[0];
+  T s0 = (T)1.0, s1 = (T)0.0, s2 = (T)0.0, s3 = (T)1.0;  // neutral element (1,0,0,1)
+  for (int64_t i = 0; i < n; i++) {
+    T m0, m1, m2, m3;
+    if (0 < i) {
+      m0 = b[i];
+      m1 = (T)0.0 - a[i] * c[i - 1];
+      m2 = (T)1.0;
+      m3 = (T)0.0;
+    } else {
+      m0 = (T)1.0;
+      m1 = (T)0.0;
+      m2 = (T)0.0;
+      m3 = (T)1.0;
+    }
+    const T value = (T)1.0 / (s0 * m0);
+    const T n0 = (m0 * s0 + m1 * s2) * value;
+    const T n1 = (m0 * s1 + m1 * s3) * value;
+    const T n2 = (m2 * s0 + m3 * s2) * value;
+    const T n3 = (m2 * s1 + m3 * s3) * value;
+    s0 = n0;
+    s1 = n1;
+    s2 = n2;
+    s3 = n3;
+    bp[i] = (s0 * b0 + s1) / (s2 * b0 + s3);
+  }
+  const T y0 = y[0];
+  T c0 = (T)0.0, c1 = (T)1.0;
+  for (int64_t i = 0; i < n; i++) {
+    T l0, l1;
+    if (0 < i) {
+      l0 = y[i];
+      l1 = (T)0.0 - a[i] / bp[i - 1];
+    } else {
+      l0 = (T)0.0;
+      l1 = (T)1.0;
+    }
+    const T n0 = l0 + l1 * c0;
+    const T n1 = c1 * l1;
+    c0 = n0;
+    c1 = n1;
+    yp[i] = c0 + c1 * y0;
+  }
+  const T yn = yp[n - 1] / bp[n - 1];
+  c0 = (T)0.0;
+  c1 = (T)1.0;
+  for (int64_t k = 0; k < n; k++) {
+    const int64_t i = n - k - 1;
+    T l0, l1;
+    if (0 < k) {
+      l0 = yp[i] / bp[i];
+      l1 = (T)0.0 - c[i] / bp[i];
+    } else {
+      l0 = (T)0.0;
+      l1 = (T)1.0;
+    }
+    const T n0 = l0 + l1 * c0;
+    const T n1 = c1 * l1;
+    c0 = n0;
+    c1 = n1;
+    out[i] = c0 + c1 * yn;
   }
 }
 
@@ -423,6 +495,8 @@ LVC_TRIDAG_BATCH(lvc_oracle_tridag_par_f32, float, tridag_par)
 LVC_TRIDAG_BATCH(lvc_oracle_tridag_par_f64, double, tridag_par)
 LVC_TRIDAG_BATCH(lvc_oracle_tridag_seq_f32, float, tridag_seq)
 LVC_TRIDAG_BATCH(lvc_oracle_tridag_seq_f64, double, tridag_seq)
+LVC_TRIDAG_BATCH(lvc_oracle_tridag_par4_f32, float, tridag_par4)
+LVC_TRIDAG_BATCH(lvc_oracle_tridag_par4_f64, double, tridag_par4)
 
 int lvc_oracle_max_threads(void) { return (int)std::thread::hardware_concurrency(); }
 

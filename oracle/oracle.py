@@ -42,7 +42,8 @@ def load():
     L.lvc_oracle_batch_f64.argtypes = [i32] + [vp] * 9 + [vp, vp, ctypes.c_int]
     L.lvc_oracle_batch_f64.restype = ctypes.c_int
     for name in ("lvc_oracle_tridag_par_f32", "lvc_oracle_tridag_par_f64",
-                 "lvc_oracle_tridag_seq_f32", "lvc_oracle_tridag_seq_f64"):
+                 "lvc_oracle_tridag_seq_f32", "lvc_oracle_tridag_seq_f64",
+                 "lvc_oracle_tridag_par4_f32", "lvc_oracle_tridag_par4_f64"):
         fn = getattr(L, name)
         fn.argtypes = [i64, i64] + [vp] * 5
         fn.restype = None

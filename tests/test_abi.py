@@ -11,7 +11,7 @@ import pytest
 from conftest import REPO
 
 HEADERS = sorted(glob.glob(os.path.join(REPO, "include", "*.h")))
-DECL = re.compile(r"^LVC_API\s+[^(]*?\b([a-z_][a-z_0-9]*)\s*\(", re.M)
+DECL = re.compile(r"^LVC_API\s+[^(]*?\b([A-Za-z_][A-Za-z_0-9]*)\s*\(", re.M)
 
 
 def declared_functions():

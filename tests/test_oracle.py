@@ -110,3 +110,16 @@ def test_batch_equals_per_calibration(oracle, pkg):
                                            ("outer", "numX", "numY", "numT", "s0", "t", "alpha", "nu", "beta")])
                           for c in calibs])
     assert np.array_equal(got, exp)
+
+
+def test_tridag_par4_agrees_with_thomas_f64(oracle):
+    # misc/ocean-sim/tridiag.fut's tridagPar (4-tuple matrix scan) is the same
+    # solution as tridagSeq in exact arithmetic: at f64 on the reference's own
+    # test inputs the two agree to ~4e-11 (the f32 runs differ by up to 6e-2
+    # on the worst element of these ill-conditioned random systems, median 2e-6)
+    z = np.load(os.path.join(GOLDEN, "tridiag32_small.npz"))
+    a, b, c, y = (z[k].astype(np.float64) for k in "abcy")
+    xs = oracle.tridag(a, b, c, y, form="seq")
+    for form in ("par", "par4"):
+        xp = oracle.tridag(a, b, c, y, form=form)
+        assert np.max(np.abs(xp - xs) / np.abs(xs)) <= 1e-9
