@@ -73,6 +73,12 @@ LVC_HD PairLayout pair_layout(int X, int Ycs, int upw) {
   return L;
 }
 
+// cluster ranks whose block maps are loaded at once (f64; f32 state, whose
+// registers are capped at 128, folds one rank at a time)
+template <typename S> struct FoldBatch {
+  static constexpr int v = sizeof(S) == 8 ? 4 : 1;
+};
+
 template <typename S> struct P2;
 template <> struct P2<double> {
   using T = double2;
@@ -121,6 +127,7 @@ __global__ void __launch_bounds__(NT, (PairMinBlocks<S, NT, UPW>::v)) lvc_line_p
   static_assert(UPW == 1 || UPW == 2, "one or two units per warp");
   static_assert(sizeof(S) == sizeof(PV), "pivots are copied verbatim into the state buffer");
   static_assert(K % 2 == 0, "columns are walked in pairs");
+  constexpr int FB = FoldBatch<S>::v;
   using V = P2<S>;
   extern __shared__ __align__(16) unsigned char smem[];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -264,7 +271,12 @@ __global__ void __launch_bounds__(NT, (PairMinBlocks<S, NT, UPW>::v)) lvc_line_p
       // e_j of this step, planar (the barrier below orders it before the X
       // sweep; its last readers were the previous step's passes 1 and 2)
       for (int j = tid; j < Ycs; j += NT) sE[j] = (S)tb[j * 8 + kSlotE];
-      if (clustered) cg::this_cluster().sync(); else __syncthreads();
+      // Cluster: the neighbours' halo rows of the previous step have landed
+      // (they arrived after pushing them; the arrive/wait pair is split so its
+      // latency overlaps the bulk-copy wait above).  Step 0 reads only the
+      // halo rows this CTA initialised itself.
+      if (clustered && s > 0) asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
+      __syncthreads();
       const S dt = (S)tabc[Lt.dtinv + k];
 
       // -------- X sweep pass 1: explicitX + explicitY, forward recurrence (chunk-local) --------
@@ -473,12 +485,23 @@ __global__ void __launch_bounds__(NT, (PairMinBlocks<S, NT, UPW>::v)) lvc_line_p
         }
         cg::cluster_group cl = cg::this_cluster();
         cl.sync();
+        // fold of the lower ranks' block maps, in rank order; the remote
+        // loads of a batch are independent, so they overlap (one distributed
+        // shared-memory round trip per batch instead of one per rank)
         for (int col = tid; col < X; col += NT) {
           S zv = 0;
-          for (int r = 0; r < rank; r++) {
-            const S* rf = cl.map_shared_rank(blkF, r);
-            const S* rt = cl.map_shared_rank(s_tot, r);
-            zv = rf[col] + rt[0] * zv;
+          for (int rb0 = 0; rb0 < rank; rb0 += FB) {
+            S f[FB], t[FB];
+#pragma unroll
+            for (int q = 0; q < FB; q++) {
+              if (rb0 + q < rank) {
+                f[q] = cl.map_shared_rank(blkF, rb0 + q)[col];
+                t[q] = cl.map_shared_rank(s_tot, rb0 + q)[0];
+              }
+            }
+#pragma unroll
+            for (int q = 0; q < FB; q++)
+              if (rb0 + q < rank) zv = f[q] + t[q] * zv;
           }
           s_zin[col] = zv;
         }
@@ -531,10 +554,18 @@ __global__ void __launch_bounds__(NT, (PairMinBlocks<S, NT, UPW>::v)) lvc_line_p
         cl.sync();
         for (int col = tid; col < X; col += NT) {
           S xv = 0;
-          for (int r = C - 1; r > rank; r--) {
-            const S* rb_ = cl.map_shared_rank(blkB, r);
-            const S* rt = cl.map_shared_rank(s_tot, r);
-            xv = rb_[col] + rt[1] * xv;
+          for (int rb0 = C - 1; rb0 > rank; rb0 -= FB) {
+            S f[FB], t[FB];
+#pragma unroll
+            for (int q = 0; q < FB; q++) {
+              if (rb0 - q > rank) {
+                f[q] = cl.map_shared_rank(blkB, rb0 - q)[col];
+                t[q] = cl.map_shared_rank(s_tot, rb0 - q)[1];
+              }
+            }
+#pragma unroll
+            for (int q = 0; q < FB; q++)
+              if (rb0 - q > rank) xv = f[q] + t[q] * xv;
           }
           s_xin[col] = xv;
         }
@@ -587,6 +618,9 @@ __global__ void __launch_bounds__(NT, (PairMinBlocks<S, NT, UPW>::v)) lvc_line_p
           args.out[c.out + item.strike] = (double)pv;  // myResult[myYindex, myXindex]
         }
       }
+      // halo rows pushed: release them to the neighbours' next step (the last
+      // step has no next step; the next item starts with a full cluster sync)
+      if (clustered && s + 1 < steps) asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory");
     }
   }
   if (clustered) cg::this_cluster().sync();
