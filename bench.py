@@ -412,10 +412,12 @@ def run_ours(args):
     if not args.no_autotune:
         t0 = time.perf_counter()
         entries = ctx.autotune(calibs, precision=precision, probe_steps=8)
+        plan_params = ctx.autotune_plan(calibs, precision=precision)
         tune = {"seconds": time.perf_counter() - t0, "classes": len(entries),
                 "changed_from_builtin": [f"{e.numX}x{e.numY}: {e.shape}" for e in entries
                                          if e.us_per_step_default > 0
-                                         and e.us_per_step_best < e.us_per_step_default * 0.999]}
+                                         and e.us_per_step_best < e.us_per_step_default * 0.999],
+                "plan_params": plan_params}
     plan = ctx.plan(calibs, precision=precision)
     ext = torch.cuda.ExternalStream(ctx.stream, device=f"cuda:{local}")
     n_opts = wl.total_options(calibs)

@@ -134,6 +134,8 @@ def load_library(path: str = LIB_PATH):
         "lvc_plan_shape": (ctypes.c_int, [vp, i32, ctypes.POINTER(Shape)]),
         "lvc_tuning_entries": (i32, [vp, ctypes.POINTER(TuningEntry), i32]),
         "lvc_autotune": (ctypes.c_int, [vp, ctypes.POINTER(_Calib), i32, i32, i32]),
+        "lvc_autotune_plan": (ctypes.c_int, [vp, ctypes.POINTER(_Calib), i32, i32, i32, ctypes.POINTER(i32),
+                                             ctypes.POINTER(i32), ctypes.POINTER(f64)]),
         "lvc_tuning_save": (ctypes.c_int, [vp, ctypes.c_char_p]),
         "lvc_tuning_load": (ctypes.c_int, [vp, ctypes.c_char_p]),
         "futhark_context_new": (vp, [vp]),
@@ -291,6 +293,14 @@ class Context:
         arr = _calib_array(calibs)
         self._check(self.lib.lvc_autotune(self._ctx, arr, len(calibs), precision, probe_steps))
         return self.tuning_entries()
+
+    def autotune_plan(self, calibs: Sequence[Calibration], precision: int = F64, max_steps: int = 32) -> dict:
+        """Time the whole plan under lvc.grid 0/1 x lvc.streams 2/4; keep the fastest."""
+        arr = _calib_array(calibs)
+        g, st, ms = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_double()
+        self._check(self.lib.lvc_autotune_plan(self._ctx, arr, len(calibs), precision, max_steps,
+                                               ctypes.byref(g), ctypes.byref(st), ctypes.byref(ms)))
+        return {"lvc.grid": g.value, "lvc.streams": st.value, "capped_plan_ms": ms.value}
 
     def tuning_save(self, path: str):
         self._check(self.lib.lvc_tuning_save(self._ctx, str(path).encode()))

@@ -45,11 +45,17 @@ using namespace lvc;
 //   lvc.streams  streams a batch plan forks its launch classes over (1..8)
 //   lvc.grid     0: persistent grids sized to the resident CTAs, items taken
 //                in strides; 1: one CTA (cluster) per strike instance, the
-//                block scheduler handing out items in descending work order
+//                block scheduler handing out items in descending work order;
+//                2: 0 for f64 plans, 1 for f32-state plans (the measured best
+//                of each on the uneven calibration mix)
 struct TuningParams {
   int streams = 4;
-  int grid = 0;
+  int grid = 2;
 };
+
+int grid_mode(const TuningParams& t, int precision) {
+  return t.grid == 2 ? (precision == LVC_F32_STATE ? 1 : 0) : t.grid;
+}
 const char* const kTuningNames[] = {"lvc.streams", "lvc.grid"};
 const char* const kTuningClasses[] = {"streams", "grid"};
 constexpr int kNumTuning = 2;
@@ -65,7 +71,7 @@ int set_tuning(TuningParams& t, const char* name, size_t v) {
     return 0;
   }
   if (!strcmp(name, "lvc.grid")) {
-    if (v > 1) return 1;
+    if (v > 2) return 1;
     t.grid = (int)v;
     return 0;
   }
@@ -861,7 +867,7 @@ int plan_new_locked(futhark_context* ctx, const lvc_calibration* cs, int n, int 
   P->max_sms = max_sms;
   P->shapes_gen = ctx->shapes_gen;
   if (use_graph && max_sms == 0) {  // batch plans follow the context's tuning
-    P->max_sms = ctx->tuning.grid == 1 ? -1 : 0;
+    P->max_sms = grid_mode(ctx->tuning, precision) == 1 ? -1 : 0;
     P->n_streams = ctx->tuning.streams;
     for (int k = 0; k < kMaxAux; k++) P->aux[k] = ctx->aux[k];
     LVC_CUDA(ctx, cudaEventCreateWithFlags(&P->ev_fork, cudaEventDisableTiming));
@@ -1368,7 +1374,7 @@ constexpr double kTuneMargin = 1.03;  // a shape replaces the built-in one only 
 int probe_us_per_step(futhark_context* ctx, const lvc_calibration& c, int precision, int reps, double* us) {
   if (!ctx->pool) ctx->pool = new DevicePool();
   lvc_plan* P = nullptr;
-  const int max_sms = ctx->tuning.grid == 1 ? -1 : 0;
+  const int max_sms = grid_mode(ctx->tuning, precision) == 1 ? -1 : 0;
   if (int rc = plan_new_locked(ctx, &c, 1, precision, &P, ctx->pool, /*use_graph=*/false, max_sms)) return rc;
   std::vector<cudaEvent_t> ev(2 * P->launches.size(), nullptr);
   for (auto& x : ev) {
@@ -1552,6 +1558,62 @@ int lvc_autotune(struct futhark_context* ctx, const struct lvc_calibration* cali
     ctx->shapes[key] = best;
   }
   ctx->shapes_gen++;
+  return 0;
+}
+
+int lvc_autotune_plan(struct futhark_context* ctx, const struct lvc_calibration* calibs, int32_t n,
+                      int32_t precision, int32_t max_steps, int32_t* grid, int32_t* streams, double* ms) {
+  std::lock_guard<std::mutex> g(ctx->mu);
+  if (!ctx->ok) return set_error(ctx, FUTHARK_PROGRAM_ERROR, "context has no usable CUDA device");
+  if (precision != LVC_F64 && precision != LVC_F32_STATE)
+    return set_error(ctx, FUTHARK_PROGRAM_ERROR, "unknown precision");
+  if (n <= 0 || !calibs) return set_error(ctx, FUTHARK_PROGRAM_ERROR, "bad calibration list");
+  LVC_CUDA(ctx, cudaSetDevice(ctx->device));
+  if (max_steps <= 0) max_steps = 32;
+  // the workload with its time lines capped: the same classes, instances and
+  // shapes, a fraction of the steps
+  std::vector<lvc_calibration> probe(calibs, calibs + n);
+  for (auto& c : probe) c.numT = std::min(c.numT, max_steps + 1);
+  const TuningParams keep = ctx->tuning;
+  TuningParams best = keep;
+  double best_ms = -1.0;
+  cudaEvent_t e0, e1;
+  LVC_CUDA(ctx, cudaEventCreate(&e0));
+  LVC_CUDA(ctx, cudaEventCreate(&e1));
+  int rc = 0;
+  for (int gm = 0; gm <= 1 && !rc; gm++) {
+    for (int st : {2, 4}) {
+      ctx->tuning.grid = gm;
+      ctx->tuning.streams = st;
+      lvc_plan* P = nullptr;
+      if ((rc = plan_new_locked(ctx, probe.data(), n, precision, &P))) break;
+      double t = 1e30;
+      for (int r = 0; r < 3 && !rc; r++) {
+        cudaError_t e = cudaEventRecord(e0, ctx->stream);
+        if (e == cudaSuccess) e = plan_launch(P, ctx->stream);
+        if (e == cudaSuccess) e = cudaEventRecord(e1, ctx->stream);
+        if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+        float x = 0.f;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&x, e0, e1);
+        if (e != cudaSuccess) rc = cuda_fail(ctx, e, "autotune plan run");
+        if (r > 0) t = std::min(t, (double)x);  // the first run warms up
+      }
+      if (!rc) rc = check_device_error(ctx, P);
+      plan_release(P);
+      if (rc) break;
+      if (best_ms < 0 || t < best_ms) {
+        best_ms = t;
+        best = ctx->tuning;
+      }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  ctx->tuning = rc ? keep : best;
+  if (rc) return rc;
+  if (grid) *grid = best.grid;
+  if (streams) *streams = best.streams;
+  if (ms) *ms = best_ms;
   return 0;
 }
 

@@ -64,9 +64,10 @@ LVC_API void futhark_context_config_set_cache_file(struct futhark_context_config
  * futhark_get_tuning_param_* enumeration).  Returns 0, or 1 for an unknown
  * name or an out-of-range value.  Names:
  *   "lvc.streams"  streams a batch plan forks its launch classes over (1..8, default 4)
- *   "lvc.grid"     0 (default): persistent grids, items taken in strides; 1: one
- *                  CTA or cluster per strike instance, handed out by the block
- *                  scheduler in descending order of work */
+ *   "lvc.grid"     0: persistent grids, items taken in strides; 1: one CTA or
+ *                  cluster per strike instance, handed out by the block
+ *                  scheduler in descending order of work; 2 (default): 0 for
+ *                  f64 plans, 1 for f32-state plans */
 LVC_API int futhark_context_config_set_tuning_param(struct futhark_context_config *cfg,
                                                     const char *param_name, size_t new_value);
 LVC_API int futhark_get_tuning_param_count(void);
@@ -296,6 +297,13 @@ LVC_API int32_t lvc_tuning_entries(struct futhark_context *ctx, struct lvc_tunin
  * probe_steps time steps (<= 0: 8), and keeps the fastest.  Synchronous. */
 LVC_API int lvc_autotune(struct futhark_context *ctx, const struct lvc_calibration *calibs,
                          int32_t n, int32_t precision, int32_t probe_steps);
+/* Plan-level autotuner: runs the workload's whole plan, with its time lines
+ * capped at max_steps (<= 0: 32), under lvc.grid 0/1 x lvc.streams 2/4, and
+ * keeps the fastest as the context's tuning parameters (reported through the
+ * optional pointers, with the capped plan's time in ms).  Synchronous. */
+LVC_API int lvc_autotune_plan(struct futhark_context *ctx, const struct lvc_calibration *calibs,
+                              int32_t n, int32_t precision, int32_t max_steps, int32_t *grid,
+                              int32_t *streams, double *ms);
 /* The tuning parameters and the table as a tuning file of name=value lines:
  *   lvc.streams=4
  *   lvc.shape.f64.256x256=line_pair,8      (family: line_pair|line_pair1|line_full|line|chunk|chunk_hbm, cluster) */

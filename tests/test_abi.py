@@ -72,7 +72,8 @@ def test_tuning_parameters_by_name(pkg):
         assert lib.futhark_context_config_set_tuning_param(cfg, b"lvc.grid", 1) == 0
         assert lib.futhark_context_config_set_tuning_param(cfg, b"lvc.streams", 0) == 1
         assert lib.futhark_context_config_set_tuning_param(cfg, b"lvc.streams", 9) == 1
-        assert lib.futhark_context_config_set_tuning_param(cfg, b"lvc.grid", 2) == 1
+        assert lib.futhark_context_config_set_tuning_param(cfg, b"lvc.grid", 2) == 0
+        assert lib.futhark_context_config_set_tuning_param(cfg, b"lvc.grid", 3) == 1
         assert lib.futhark_context_config_set_tuning_param(cfg, b"no.such.param", 1) == 1
     finally:
         lib.futhark_context_config_free(cfg)

@@ -105,3 +105,13 @@ def test_tuning_errors(ctx, pkg, tmp_path):
     with pytest.raises(pkg.FutharkError):
         ctx.set_tuning_param("lvc.streams", 0)
     assert ctx.main_f64(2, 32, 32, 4, 0.03, 5.0, 0.2, 0.6, 0.5).shape == (2,)
+
+
+def test_plan_autotuner_keeps_valid_parameters(pkg, oracle):
+    calibs = wl.uneven_mix(8, seed=23, sizes=(32, 64, 128), numT=(6, 12), outer=(2, 5))
+    with pkg.Context() as c:
+        for prec in (0, 1):
+            res = c.autotune_plan(calibs, precision=prec, max_steps=4)
+            assert res["lvc.grid"] in (0, 1) and res["lvc.streams"] in (2, 4) and res["capped_plan_ms"] > 0
+        got = c.batch(calibs)  # plans built afterwards run under the chosen parameters
+        assert rel_err(got, oracle.batch_f64(calibs)) <= 1e-9
