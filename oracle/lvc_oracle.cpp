@@ -284,6 +284,193 @@ void tridag_seq(int64_t m, const T* a, const T* b, const T* c, const T* y, T* ou
   for (int64_t i = m - 2; i >= 0; i--) out[i] = yp[i] - cp[i] * out[i + 1];
 }
 
+// ---------------------------------------------------------------------------
+// misc/ocean-sim/tke.fut:64-348 (entry main, DTYPE = f32 via typeinst32): the
+// turbulent-kinetic-energy step of the ocean model.  Arrays are row-major
+// [xdim][ydim][zdim] (z innermost), [xdim][ydim] and [n].  Every expression
+// keeps the reference's operand order (no contraction); the vertical
+// tridiagonal solve is tridag_par4 (misc/ocean-sim/tridiag.fut:4-79) over
+// the z columns, as tke.fut:4-17 maps tridagPar over them.
+// ---------------------------------------------------------------------------
+template <typename T>
+static T tke_limiter(T cr) {  // tke.fut:19-20
+  return std::max((T)0, std::max(std::min((T)1, (T)2 * cr), std::min((T)2, cr)));
+}
+
+template <typename T>
+static T tke_calcflux(T velfac, T velS, T dt_tracer, T dx, T varS, T varSM1, T varSP1, T varSP2, T maskS,
+                      T maskSM1, T maskSP1) {  // tke.fut:22-41
+  const T scaledVel = velfac * velS;
+  const T uCFL = std::fabs(scaledVel * dt_tracer / dx);
+  const T rjp = (varSP2 - varSP1) * maskSP1;
+  const T rj = (varSP1 - varS) * maskS;
+  const T rjm = (varS - varSM1) * maskSM1;
+  const T epsilon = (T)0.00000000000000000001;
+  const T divisor = (std::fabs(rj) < epsilon) ? epsilon : rj;
+  T cr = (velS > 0) ? rjm / divisor : rjp / divisor;
+  cr = tke_limiter<T>(cr);
+  return scaledVel * (varSP1 + varS) * (T)0.5 - std::fabs(scaledVel) * (((T)1.0 - cr) + uCFL * cr) * rj * (T)0.5;
+}
+
+template <typename T>
+static void tke_main(int X, int Y, int Z, const T* tketau, const T* tketaup1_in, const T* dtketau_in,
+                     const T* dtketaum1, const T* utau, const T* vtau, const T* wtau, const T* maskU,
+                     const T* maskV, const T* maskW, const T* dxt, const T* dxu, const T* dyt, const T* dyu,
+                     const T* dzt, const T* dzw, const T* cost, const T* cosu, const int32_t* kbot,
+                     const T* kappaM, const T* mxl, const T* forc, const T* forc_tke_surface, T* tketaup1,
+                     T* dtketau, T* tke_surf_corr) {
+  const T dt_tracer = 1, dt_mom = 1, AB_eps = (T)0.1, alpha_tke = 1, c_eps = (T)0.7, K_h_tke = 2000;
+  const T dt_tke = dt_mom;
+  const int64_t N = (int64_t)X * Y * Z;
+  auto I3 = [&](int x, int y, int z) { return ((int64_t)x * Y + y) * Z + z; };
+  auto I2 = [&](int x, int y) { return (int64_t)x * Y + y; };
+  auto interior = [&](int x, int y) { return x >= 2 && x < X - 2 && y >= 2 && y < Y - 2; };
+  std::vector<T> delta(N), a(N), b(N), c(N), d(N), sol(N), fe(N), fn(N), ft(N);
+  for (int x = 0; x < X; x++)  // :103-108
+    for (int y = 0; y < Y; y++)
+      for (int z = 0; z < Z; z++)
+        delta[I3(x, y, z)] = (interior(x, y) && z < Z - 1)
+                                 ? dt_tke / dzt[z + 1] * alpha_tke * (T)0.5 *
+                                       (kappaM[I3(x, y, z)] + kappaM[I3(x, y, z + 1)])
+                                 : (T)0;
+  for (int x = 0; x < X; x++)
+    for (int y = 0; y < Y; y++)
+      for (int z = 0; z < Z; z++) {
+        const int64_t i = I3(x, y, z);
+        const T sqrttke = std::sqrt(std::max((T)0, tketau[i]));
+        T av = 0, bv = 0, cv = 0, dv = 0;
+        if (interior(x, y)) {
+          const int ks = kbot[I2(x, y)] - 1;
+          const bool land = ks >= 0;
+          const bool edge = land && z == ks;
+          const bool water = land && z >= ks;
+          // a_tri (:109-122)
+          if (edge || !water) av = 0;
+          else if (z > 0 && z < Z - 1) av = -delta[I3(x, y, z - 1)] / dzw[z];
+          else if (z == Z - 1) av = -delta[I3(x, y, z - 1)] / ((T)0.5 * dzw[z]);
+          else av = 0;
+          // b_tri (:123-146)
+          if (!water) bv = 1;
+          else if (edge) bv = (T)1 + delta[i] / dzw[z] + dt_tke * c_eps / mxl[i] * sqrttke;
+          else if (z > 0 && z < Z - 1)
+            bv = (T)1 + (delta[i] + delta[I3(x, y, z - 1)]) / dzw[z] + dt_tke * c_eps * sqrttke / mxl[i];
+          else if (z == Z - 1)
+            bv = (T)1 + delta[I3(x, y, z - 1)] / ((T)0.5 * dzw[z]) + dt_tke * c_eps / mxl[i] * sqrttke;
+          else bv = 0;
+          // c_tri (:187-196)
+          if (z < Z - 1) cv = water ? -delta[i] / dzw[z] : (T)0;
+          // d_tri (:197-210)
+          if (water) {
+            const T tmp = tketau[i] + dt_tke * forc[i];
+            dv = (z == Z - 1) ? tmp + dt_tke * forc_tke_surface[I2(x, y)] / ((T)0.5 * dzw[z]) : tmp;
+          }
+        }
+        a[i] = av;
+        b[i] = bv;
+        c[i] = cv;
+        d[i] = dv;
+      }
+  {  // sol = tridiag a b c d (:211), tridagPar along z
+    std::vector<T> s1(Z), s2(Z);
+    for (int64_t col = 0; col < (int64_t)X * Y; col++)
+      tridag_par4<T>(Z, &a[col * Z], &b[col * Z], &c[col * Z], &d[col * Z], &sol[col * Z], s1.data(), s2.data());
+  }
+  for (int x = 0; x < X; x++)  // :212-218
+    for (int y = 0; y < Y; y++)
+      for (int z = 0; z < Z; z++) {
+        const int64_t i = I3(x, y, z);
+        const int ks = kbot[I2(x, y)] - 1;
+        const bool water = ks >= 0 && z >= ks;
+        tketaup1[i] = (interior(x, y) && water) ? sol[i] : tketaup1_in[i];
+      }
+  for (int x = 0; x < X; x++)  // :219-226
+    for (int y = 0; y < Y; y++) {
+      T v = 0;
+      if (interior(x, y)) {
+        const T tke_val = tketaup1[I3(x, y, Z - 1)];
+        v = tke_val < 0 ? -tke_val * (T)0.5 * dzw[Z - 1] / dt_tke : (T)0;
+      }
+      tke_surf_corr[I2(x, y)] = v;
+    }
+  for (int x = 0; x < X; x++)  // :227-235
+    for (int y = 0; y < Y; y++)
+      if (interior(x, y)) {
+        T& v = tketaup1[I3(x, y, Z - 1)];
+        v = v < 0 ? (T)0 : v;
+      }
+  for (int x = 0; x < X; x++)  // lateral diffusion fluxes :236-251
+    for (int y = 0; y < Y; y++)
+      for (int z = 0; z < Z; z++) {
+        const int64_t i = I3(x, y, z);
+        fe[i] = (x < X - 1) ? K_h_tke * (tketau[I3(x + 1, y, z)] - tketau[i]) / (cost[y] * dxu[x]) * maskU[i] : (T)0;
+        fn[i] = (y < Y - 1) ? K_h_tke * (tketau[I3(x, y + 1, z)] - tketau[i]) / dyu[y] * maskV[i] * cosu[y] : (T)0;
+      }
+  for (int x = 0; x < X; x++)  // :252-263
+    for (int y = 0; y < Y; y++) {
+      if (!interior(x, y)) continue;
+      const int z = Z - 1;
+      const int64_t i = I3(x, y, z);
+      tketaup1[i] = tketaup1[i] + dt_tke * maskW[i] *
+                                      ((fe[i] - fe[I3(x - 1, y, z)]) / (cost[y] * dxt[x]) +
+                                       (fn[i] - fn[I3(x, y - 1, z)]) / (cost[y] * dyt[y]));
+    }
+  for (int x = 0; x < X; x++)  // advection fluxes :264-319
+    for (int y = 0; y < Y; y++)
+      for (int z = 0; z < Z; z++) {
+        const int64_t i = I3(x, y, z);
+        T e = 0, n = 0, t = 0;
+        if (x >= 1 && x < X - 2 && y >= 2 && y < Y - 2) {
+          const T dx = cost[y] * dxt[x];
+          const T mWm1 = maskW[I3(x - 1, y, z)], mWs = maskW[i], mWp1 = maskW[I3(x + 1, y, z)],
+                  mWp2 = maskW[I3(x + 2, y, z)];
+          const T mtr = x < X - 1 ? mWs * mWp1 : (T)0;
+          const T mtrP1 = x < X - 1 ? mWp1 * mWp2 : (T)0;
+          const T mtrM1 = x < X - 1 ? mWm1 * mWs : (T)0;
+          e = tke_calcflux<T>((T)1, utau[i], dt_tracer, dx, tketau[i], tketau[I3(x - 1, y, z)],
+                              tketau[I3(x + 1, y, z)], tketau[I3(x + 2, y, z)], mtr, mtrM1, mtrP1);
+        }
+        if (y >= 1 && y < Y - 2 && x >= 2 && x < X - 2) {
+          const T dx = cost[y] * dyt[y];
+          const T mWm1 = maskW[I3(x, y - 1, z)], mWs = maskW[i], mWp1 = maskW[I3(x, y + 1, z)],
+                  mWp2 = maskW[I3(x, y + 2, z)];
+          const T mtr = y < Y - 1 ? mWs * mWp1 : (T)0;
+          const T mtrP1 = y < Y - 1 ? mWp1 * mWp2 : (T)0;
+          const T mtrM1 = y < Y - 1 ? mWm1 * mWs : (T)0;
+          n = tke_calcflux<T>(cosu[y], vtau[i], dt_tracer, dx, tketau[i], tketau[I3(x, y - 1, z)],
+                              tketau[I3(x, y + 1, z)], tketau[I3(x, y + 2, z)], mtr, mtrM1, mtrP1);
+        }
+        if (z < Z - 1 && interior(x, y)) {
+          const T varSM1 = z != 0 ? tketau[I3(x, y, z - 1)] : (T)0;
+          const T varS = tketau[i];
+          const T varSP2 = z < Z - 2 ? tketau[I3(x, y, z + 2)] : (T)0;
+          const T varSP1 = tketau[I3(x, y, z + 1)];
+          const T mWm1 = z != 0 ? maskW[I3(x, y, z - 1)] : (T)0;
+          const T mWs = maskW[i];
+          const T mWp1 = maskW[I3(x, y, z + 1)];
+          const T mWp2 = z < Z - 2 ? maskW[I3(x, y, z + 2)] : (T)0;
+          t = tke_calcflux<T>((T)1, wtau[i], dt_tracer, dzw[z], varS, varSM1, varSP1, varSP2, mWs * mWp1,
+                              mWm1 * mWs, mWp1 * mWp2);
+        }
+        fe[i] = e;
+        fn[i] = n;
+        ft[i] = t;
+      }
+  for (int x = 0; x < X; x++)  // dtketau :320-340
+    for (int y = 0; y < Y; y++)
+      for (int z = 0; z < Z; z++) {
+        const int64_t i = I3(x, y, z);
+        const T tmp = interior(x, y)
+                          ? maskW[i] * (-(fe[i] - fe[I3(x - 1, y, z)]) / (cost[y] * dxt[x]) -
+                                        (fn[i] - fn[I3(x, y - 1, z)]) / (cost[y] * dyt[y]))
+                          : dtketau_in[i];
+        const T z0 = z == 0 ? tmp - ft[I3(x, y, 0)] / dzw[0] : tmp;
+        const T zm = (z >= 1 && z < Z - 1) ? z0 - (ft[i] - ft[I3(x, y, z - 1)]) / dzw[z] : z0;
+        dtketau[i] = (z == Z - 1) ? zm - (ft[i] - ft[I3(x, y, z - 1)]) / ((T)0.5 * dzw[z]) : zm;
+      }
+  for (int64_t i = 0; i < N; i++)  // :341-347
+    tketaup1[i] = tketaup1[i] + dt_tracer * (((T)1.5 + AB_eps) * dtketau[i] - ((T)0.5 + AB_eps) * dtketaum1[i]);
+}
+
 // finpar/LocVolCalib.fut:126-153 (explicitMethod).  Arrays are row-major
 // [rows][m]; D/DD are [m][3].
 template <typename T>
@@ -497,6 +684,20 @@ LVC_TRIDAG_BATCH(lvc_oracle_tridag_seq_f32, float, tridag_seq)
 LVC_TRIDAG_BATCH(lvc_oracle_tridag_seq_f64, double, tridag_seq)
 LVC_TRIDAG_BATCH(lvc_oracle_tridag_par4_f32, float, tridag_par4)
 LVC_TRIDAG_BATCH(lvc_oracle_tridag_par4_f64, double, tridag_par4)
+
+// tke.fut's entry main (f32): the three arrays it computes; the other four
+// outputs are its inputs tketau, tketaum1, dtketaup1, dtketaum1 unchanged.
+void lvc_oracle_tke_f32(int X, int Y, int Z, const float* tketau, const float* tketaup1_in,
+                        const float* dtketau_in, const float* dtketaum1, const float* utau, const float* vtau,
+                        const float* wtau, const float* maskU, const float* maskV, const float* maskW,
+                        const float* dxt, const float* dxu, const float* dyt, const float* dyu, const float* dzt,
+                        const float* dzw, const float* cost, const float* cosu, const int32_t* kbot,
+                        const float* kappaM, const float* mxl, const float* forc, const float* forc_tke_surface,
+                        float* tketaup1, float* dtketau, float* tke_surf_corr) {
+  tke_main<float>(X, Y, Z, tketau, tketaup1_in, dtketau_in, dtketaum1, utau, vtau, wtau, maskU, maskV, maskW, dxt,
+                  dxu, dyt, dyu, dzt, dzw, cost, cosu, kbot, kappaM, mxl, forc, forc_tke_surface, tketaup1,
+                  dtketau, tke_surf_corr);
+}
 
 int lvc_oracle_max_threads(void) { return (int)std::thread::hardware_concurrency(); }
 

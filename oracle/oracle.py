@@ -103,3 +103,33 @@ def tridag(a, b, c, y, form="par") -> np.ndarray:
     getattr(load(), name)(rows, n, a.ctypes.data, b.ctypes.data, c.ctypes.data, y.ctypes.data,
                           out.ctypes.data)
     return out
+
+
+TKE_INPUTS = ["tketau", "tketaup1", "tketaum1", "dtketau", "dtketaup1", "dtketaum1", "utau", "vtau", "wtau",
+              "maskU", "maskV", "maskW", "dxt", "dxu", "dyt", "dyu", "dzt", "dzw", "cost", "cosu", "kbot",
+              "kappaM", "mxl", "forc", "forc_tke_surface"]
+
+
+def tke(*inputs):
+    """misc/ocean-sim/tke.fut's entry main (f32) on the 25 inputs in the
+    reference's order; returns its 7 outputs (tketau, tketaup1, tketaum1,
+    dtketau, dtketaup1, dtketaum1, tke_surf_corr)."""
+    v = dict(zip(TKE_INPUTS, inputs))
+    f32 = {k: np.ascontiguousarray(x, dtype=np.float32) for k, x in v.items() if k != "kbot"}
+    kbot = np.ascontiguousarray(v["kbot"], dtype=np.int32)
+    X, Y, Z = f32["tketau"].shape
+    tp1 = np.empty((X, Y, Z), np.float32)
+    dtk = np.empty((X, Y, Z), np.float32)
+    corr = np.empty((X, Y), np.float32)
+    L = load()
+    fn = L.lvc_oracle_tke_f32
+    fn.restype = None
+    fn.argtypes = [ctypes.c_int] * 3 + [ctypes.c_void_p] * 26
+    order = ["tketau", "tketaup1", "dtketau", "dtketaum1", "utau", "vtau", "wtau", "maskU", "maskV", "maskW",
+             "dxt", "dxu", "dyt", "dyu", "dzt", "dzw", "cost", "cosu"]
+    args = [f32[k].ctypes.data for k in order] + [kbot.ctypes.data] + \
+           [f32[k].ctypes.data for k in ("kappaM", "mxl", "forc", "forc_tke_surface")] + \
+           [tp1.ctypes.data, dtk.ctypes.data, corr.ctypes.data]
+    fn(X, Y, Z, *args)
+    return (f32["tketau"].copy(), tp1, f32["tketaum1"].copy(), dtk, f32["dtketaup1"].copy(),
+            f32["dtketaum1"].copy(), corr)

@@ -9,6 +9,8 @@ present:
 
   locvolcalib_golden.json   inputs + expected f32 prices for small/medium/large
   tridiag32_small.npz       a, b, c, y [100][115] f32 and the expected x
+  tke32_small.npz           misc/ocean-sim/data/tke32-small.{in,out}: in00..in24
+                            (the 25 inputs of tke.fut's main) and out0..out6
 
 Usage:  python tests/golden/make_golden.py [REFERENCE_ROOT]
 (REFERENCE_ROOT defaults to /root/reference.)
@@ -53,6 +55,13 @@ def main(ref_root: str) -> None:
     a, b, c, y = fd.read_file(os.path.join(tdir, "tridiag32-small.in"))
     (x,) = fd.read_file(os.path.join(tdir, "tridiag32-small.out"))
     np.savez_compressed(os.path.join(HERE, "tridiag32_small.npz"), a=a, b=b, c=c, y=y, x=x)
+
+    # misc/ocean-sim/tke.fut's test stanza: 25 inputs, 7 outputs ([20][20][10])
+    ins = fd.read_file(os.path.join(tdir, "tke32-small.in"))
+    outs = fd.read_file(os.path.join(tdir, "tke32-small.out"))
+    np.savez_compressed(os.path.join(HERE, "tke32_small.npz"),
+                        **{f"in{i:02d}": v for i, v in enumerate(ins)},
+                        **{f"out{i}": v for i, v in enumerate(outs)})
     print("wrote", os.listdir(HERE))
 
 

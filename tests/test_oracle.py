@@ -123,3 +123,12 @@ def test_tridag_par4_agrees_with_thomas_f64(oracle):
     for form in ("par", "par4"):
         xp = oracle.tridag(a, b, c, y, form=form)
         assert np.max(np.abs(xp - xs) / np.abs(xs)) <= 1e-9
+
+
+def test_tke_reproduces_golden_bit_exact(oracle):
+    # misc/ocean-sim/tke.fut's entry main restated in f32 with the reference's
+    # operand order: all seven outputs equal tke32-small.out bit for bit
+    z = np.load(os.path.join(GOLDEN, "tke32_small.npz"))
+    got = oracle.tke(*[z[f"in{i:02d}"] for i in range(25)])
+    for i, g in enumerate(got):
+        assert np.array_equal(g, z[f"out{i}"]), i
