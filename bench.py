@@ -66,6 +66,7 @@ def parse():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--no-tridiag", action="store_true", help="skip the batched tridiagonal solver section")
+    ap.add_argument("--no-tke", action="store_true", help="skip the ocean model's tke step section")
     ap.add_argument("--no-autotune", action="store_true", help="built-in shapes instead of the autotuner's")
     ap.add_argument("--serving-rates", default="100,1000,5000,20000",
                     help="Poisson arrival rates (requests/s) of the serving sweep")
@@ -335,6 +336,83 @@ def run_tridiag(pkg, wl, ctx, args):
     return res
 
 
+def run_tke(wl, args):
+    """The ocean model's tke step (misc/ocean-sim/tke.fut, libtke.so) on the
+    benchmark stanza's 200x200x100 f32 dataset shape: device-resident time per
+    step (L2 flushed between steps) through tke_step_f32, end to end through
+    futhark_entry_main with host arrays, bit-exactness against the oracle, CPU
+    baseline (the oracle, one thread, the whole step)."""
+    import importlib
+    import numpy as np
+    import torch
+    from oracle import oracle
+    tke = importlib.import_module("futhark-benchmarks_b200.tke")
+    X, Y, Z = wl.TKE_BENCH
+    host = wl.tke_inputs(X, Y, Z, seed=args.seed)
+    named = dict(zip(tke.INPUT_NAMES, host))
+    tctx = tke.TkeContext()
+    try:
+        dev = {k: torch.from_numpy(np.ascontiguousarray(named[k])).cuda() for k in tke.STEP_INPUTS}
+        out = {"tketaup1_out": torch.empty((X, Y, Z), dtype=torch.float32, device="cuda"),
+               "dtketau_out": torch.empty((X, Y, Z), dtype=torch.float32, device="cuda"),
+               "tke_surf_corr_out": torch.empty((X, Y), dtype=torch.float32, device="cuda")}
+        scratch = torch.empty(tctx.scratch_bytes(X, Y, Z), dtype=torch.uint8, device="cuda")
+        ptrs = {k: v.data_ptr() for k, v in dev.items()}
+        ptrs.update({k: v.data_ptr() for k, v in out.items()})
+        ptrs["scratch"] = scratch.data_ptr()
+        flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
+        ext = torch.cuda.ExternalStream(tctx.stream)
+        torch.cuda.synchronize()
+        for _ in range(max(3, args.warmup)):
+            tctx.step((X, Y, Z), ptrs)
+        tctx.check()
+        times = []
+        for _ in range(max(5, args.steps)):
+            flush.zero_()
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(ext)
+            tctx.step((X, Y, Z), ptrs)
+            e1.record(ext)
+            tctx.sync()
+            times.append(e0.elapsed_time(e1))
+        tctx.check()
+        ms = float(np.median(times))
+        t0 = time.perf_counter()
+        want = oracle.tke(*host)
+        cpu_s = time.perf_counter() - t0
+        exact = all(np.array_equal(out[k].cpu().numpy().view(np.uint32), want[i].view(np.uint32))
+                    for k, i in (("tketaup1_out", 1), ("dtketau_out", 3), ("tke_surf_corr_out", 6)))
+        # end to end: 25 host arrays in, 7 host arrays out, through futhark_entry_main
+        tctx.main(*host)
+        reps = 3
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            tctx.main(*host)
+        e2e_ms = 1e3 * (time.perf_counter() - t0) / reps
+        cells = X * Y * Z
+        # 13 [x][y][z] f32 inputs read, 2 written; kbot and forc_tke_surface read
+        # and tke_surf_corr written per column
+        alg_bytes = 60 * cells + 12 * X * Y
+        peak, peak_src = hbm_peak()
+        gbs = alg_bytes / (ms * 1e-3) / 1e9
+        h2d = sum(np.asarray(v).nbytes for v in host)
+        d2h = 6 * cells * 4 + X * Y * 4
+        del flush
+        return {"workload": f"[{X}][{Y}][{Z}] f32 fields on the reference's random-dataset bounds (synthetic)",
+                "entry": "futhark_entry_main (libtke.so)", "device_ms": ms, "cells_per_s": cells / (ms * 1e-3),
+                "launches_per_step": tctx.launches_per_step, "algorithmic_bytes_per_step": alg_bytes,
+                "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak,
+                             "peak_source": peak_src},
+                "e2e_ms": e2e_ms, "e2e_cells_per_s": cells / (e2e_ms * 1e-3), "e2e_h2d_bytes": h2d,
+                "e2e_d2h_bytes": d2h, "bit_exact_vs_oracle": exact,
+                "cpu_baseline": {"value": cells / cpu_s, "unit": "cells/s", "cores": 1, "kind": "port",
+                                 "sample": f"the whole {X}x{Y}x{Z} step, oracle"}}
+    finally:
+        tctx.close()
+
+
 def run_serving(pkg, wl, ctx, args, rank, precision):
     """Poisson request streams through the serving runtime (continuous batching)."""
     import numpy as np
@@ -487,6 +565,10 @@ def run_ours(args):
     if not args.no_tridiag and rank == 0:
         tridiag = run_tridiag(pkg, wl, ctx, args)
 
+    tke_res = None
+    if not args.no_tke and rank == 0:
+        tke_res = run_tke(wl, args)
+
     serving = None
     if not args.no_serving:
         serving = run_serving(pkg, wl, ctx, args, rank, precision)
@@ -529,6 +611,7 @@ def run_ours(args):
             "plain_per_call": plain,
             "serving": serving,
             "tridiag": tridiag,
+            "tke": tke_res,
             "batched_vs_plain": (value / plain["value"]) if plain else None,
             "cpu_baseline": cpu,
             "error_vs_fp64_oracle": err,

@@ -4,7 +4,8 @@
 
 produces, in tree (so the library travels with the repository):
 
-    futhark-benchmarks_b200/liblvc.so   the C-ABI library (include/LocVolCalib.h)
+    futhark-benchmarks_b200/liblvc.so   the C-ABI library (include/LocVolCalib.h, tridiag.h)
+    futhark-benchmarks_b200/libtke.so   the ocean model's tke step (include/tke.h)
     oracle/liblvc_oracle.so             the CPU oracle (tests and CPU baseline only)
 
 nvcc cross-compiles for sm_100a without a GPU.  CUDA runtime is linked
@@ -21,11 +22,14 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "liblvc.so")
+TKE_LIB = os.path.join(PKG, "libtke.so")
 ORACLE_DIR = os.path.join(REPO, "oracle")
 ORACLE_LIB = os.path.join(ORACLE_DIR, "liblvc_oracle.so")
 
 SOURCES = ["lvc_runtime.cu"]
 HEADERS = ["lvc_kernels.cuh", "lvc_layout.h", "lvc_probe.cuh", "lvc_line.cuh", "lvc_pair.cuh", "lvc_tridiag.cuh"]
+TKE_SOURCES = ["tke_runtime.cu"]
+TKE_HEADERS = ["lvc_line.cuh", "lvc_tridiag.cuh"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",
@@ -65,6 +69,23 @@ def build_lib(force: bool = False, verbose: bool = False, extra=()) -> str:
     return LIB
 
 
+def build_tke(force: bool = False, verbose: bool = False, extra=()) -> str:
+    """libtke.so: a library of its own, since misc/ocean-sim/tke.fut's entry
+    point is named futhark_entry_main like LocVolCalib's."""
+    deps = [os.path.join(CSRC, f) for f in TKE_SOURCES + TKE_HEADERS]
+    deps += [os.path.join(REPO, "include", "tke.h"), os.path.abspath(__file__)]
+    if not force and not _stale(TKE_LIB, deps):
+        return TKE_LIB
+    cmd = [nvcc(), *NVCC_FLAGS, *extra, "-I", os.path.join(REPO, "include"), "-I", CSRC,
+           "-o", TKE_LIB + ".tmp", *[os.path.join(CSRC, f) for f in TKE_SOURCES]]
+    if verbose:
+        cmd.insert(1, "-Xptxas=-v")
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True)
+    os.replace(TKE_LIB + ".tmp", TKE_LIB)
+    return TKE_LIB
+
+
 def build_oracle(force: bool = False) -> str:
     src = os.path.join(ORACLE_DIR, "lvc_oracle.cpp")
     if force or _stale(ORACLE_LIB, [src, os.path.join(ORACLE_DIR, "Makefile")]):
@@ -78,8 +99,10 @@ def main(argv=None) -> None:
     force = "--force" in argv
     verbose = "-v" in argv
     build_lib(force=force, verbose=verbose)
+    build_tke(force=force, verbose=verbose)
     build_oracle(force=force)
     print(LIB)
+    print(TKE_LIB)
     print(ORACLE_LIB)
 
 

@@ -72,3 +72,40 @@ TRIDIAG_BENCH = (57600, 115)
 def tridiag_inputs(rows: int, m: int, seed: int = 0):
     rng = np.random.default_rng(seed)
     return tuple(rng.uniform(lo, hi, size=(rows, m)).astype(np.float32) for lo, hi in TRIDIAG_BOUNDS)
+
+
+# misc/ocean-sim/tke.fut: the benchmark's "200x200x100" dataset shape, and the
+# value ranges of the reference's random-dataset recipe
+# (misc/ocean-sim/data/rand-dataset-tke.sh): f32 fields uniform on [0.5, 1.5],
+# kbot uniform on [-100, 10000].
+TKE_BENCH = (200, 200, 100)
+TKE_F32_BOUNDS = (0.5, 1.5)
+TKE_KBOT_BOUNDS = (-100, 10000)
+
+
+def tke_inputs(xdim: int, ydim: int, zdim: int, seed: int = 0, wet: bool = False):
+    """The 25 inputs of tke.fut's main, in the entry's order.  wet=False draws
+    them as the reference's recipe does; wet=True puts most columns' bottom
+    inside [0, zdim] and gives the state and velocity fields both signs, so that
+    every branch (land, edge and water cells, both upwind directions, the clip
+    of a negative surface value) is taken."""
+    rng = np.random.default_rng(seed)
+    lo, hi = TKE_F32_BOUNDS
+    f3 = lambda: rng.uniform(lo, hi, size=(xdim, ydim, zdim)).astype(np.float32)
+    f1 = lambda n: rng.uniform(lo, hi, size=n).astype(np.float32)
+    state = [f3() for _ in range(6)]
+    vel = [f3() for _ in range(3)]
+    masks = [f3() for _ in range(3)]
+    if wet:
+        state = [(s - np.float32(1.1)).astype(np.float32) for s in state]
+        vel = [(v - np.float32(1.0)).astype(np.float32) for v in vel]
+        masks = [(rng.uniform(size=(xdim, ydim, zdim)) < 0.85).astype(np.float32) for _ in range(3)]
+        kbot = rng.integers(-1, zdim + 1, size=(xdim, ydim), endpoint=True).astype(np.int32)
+    else:
+        kbot = rng.integers(TKE_KBOT_BOUNDS[0], TKE_KBOT_BOUNDS[1], size=(xdim, ydim), endpoint=True).astype(np.int32)
+    grid = [f1(xdim), f1(xdim), f1(ydim), f1(ydim), f1(zdim), f1(zdim), f1(ydim), f1(ydim)]
+    forcing = [f3() for _ in range(3)]
+    surf = rng.uniform(lo, hi, size=(xdim, ydim)).astype(np.float32)
+    if wet:
+        surf = (surf - np.float32(1.2)).astype(np.float32)
+    return (*state, *vel, *masks, *grid, kbot, *forcing, surf)

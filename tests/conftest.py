@@ -24,6 +24,11 @@ def pkg():
 
 
 @pytest.fixture(scope="session")
+def tke():
+    return importlib.import_module("futhark-benchmarks_b200.tke")
+
+
+@pytest.fixture(scope="session")
 def oracle():
     from oracle import oracle as o
     o.load()

@@ -11,12 +11,17 @@ import pytest
 from conftest import REPO
 
 HEADERS = sorted(glob.glob(os.path.join(REPO, "include", "*.h")))
-DECL = re.compile(r"^LVC_API\s+[^(]*?\b([A-Za-z_][A-Za-z_0-9]*)\s*\(", re.M)
+DECL = re.compile(r"^(?:LVC|TKE)_API\s+[^(]*?\b([A-Za-z_][A-Za-z_0-9]*)\s*\(", re.M)
+# which library implements each header
+HEADER_LIB = {"LocVolCalib.h": "liblvc.so", "tridiag.h": "liblvc.so", "tke.h": "libtke.so"}
 
 
-def declared_functions():
+def declared_functions(lib_name: str = "liblvc.so"):
     names = []
     for h in HEADERS:
+        assert os.path.basename(h) in HEADER_LIB, h
+        if HEADER_LIB[os.path.basename(h)] != lib_name:
+            continue
         with open(h) as f:
             names += DECL.findall(f.read())
     return names
@@ -31,14 +36,39 @@ def test_headers_declare_the_generated_api():
         assert required in names
 
 
-def test_library_exports_every_declared_symbol(pkg):
-    lib = ctypes.CDLL(pkg.LIB_PATH)
-    missing = [n for n in declared_functions() if not hasattr(lib, n)]
+@pytest.mark.parametrize("lib_name", sorted(set(HEADER_LIB.values())))
+def test_library_exports_every_declared_symbol(lib_name):
+    lib = ctypes.CDLL(os.path.join(REPO, "futhark-benchmarks_b200", lib_name))
+    names = declared_functions(lib_name)
+    assert names
+    missing = [n for n in names if not hasattr(lib, n)]
     assert not missing, missing
 
 
 def test_python_mirror_binds_every_symbol(pkg):
     pkg.load_library()  # raises if a signature names a missing symbol
+
+
+def test_tke_mirror_binds_every_declared_symbol(tke):
+    # every function of include/tke.h has its C signature declared in the mirror
+    lib = tke.load_library()
+    unbound = [n for n in declared_functions("libtke.so") if getattr(lib, n).argtypes is None]
+    assert not unbound, unbound
+
+
+def test_tke_context_without_gpu_reports_error(tke, pkg):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(pkg.FutharkError) as ei:
+        tke.TkeContext()
+    assert ei.value.code == pkg.FUTHARK_PROGRAM_ERROR
+
+
+def test_tke_step_args_layout(tke):
+    # struct tke_step_args: three int64 dimensions, then 27 pointers
+    assert ctypes.sizeof(tke._StepArgs) == 3 * 8 + (len(tke.STEP_INPUTS) + len(tke.STEP_OUTPUTS) + 1) * 8
+    assert len(tke.INPUT_NAMES) == 25 and len(tke.OUTPUT_NAMES) == 7
 
 
 def test_context_without_gpu_reports_error(pkg):
