@@ -67,6 +67,8 @@ def parse():
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--no-tridiag", action="store_true", help="skip the batched tridiagonal solver section")
     ap.add_argument("--no-tke", action="store_true", help="skip the ocean model's tke step section")
+    ap.add_argument("--only-tke", action="store_true",
+                    help="run only the tke step section (one GPU) and print its JSON object")
     ap.add_argument("--no-autotune", action="store_true", help="built-in shapes instead of the autotuner's")
     ap.add_argument("--serving-rates", default="100,1000,5000,20000",
                     help="Poisson arrival rates (requests/s) of the serving sweep")
@@ -629,6 +631,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.only_tke:
+        print(json.dumps(run_tke(importlib.import_module("futhark-benchmarks_b200.workloads"), args)))
     else:
         run_ours(args)
 

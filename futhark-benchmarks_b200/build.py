@@ -29,7 +29,7 @@ ORACLE_LIB = os.path.join(ORACLE_DIR, "liblvc_oracle.so")
 SOURCES = ["lvc_runtime.cu"]
 HEADERS = ["lvc_kernels.cuh", "lvc_layout.h", "lvc_probe.cuh", "lvc_line.cuh", "lvc_pair.cuh", "lvc_tridiag.cuh"]
 TKE_SOURCES = ["tke_runtime.cu"]
-TKE_HEADERS = ["lvc_line.cuh", "lvc_tridiag.cuh"]
+TKE_HEADERS: list = []
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",

@@ -4,22 +4,33 @@
 // its own: the program's entry point is named futhark_entry_main like
 // LocVolCalib's.
 //
-// One step is three kernels on the context's stream:
-//   tke_coef_kernel    delta and the tridiagonal coefficients a, b, c, d of
-//                      every z column (tke.fut:103-210), one thread per cell;
-//   lvc_tridag_block_kernel<1>  tridagPar along z (tke.fut:4-17, 211), the
-//                      batched solver of lvc_tridiag.cuh with rows = xdim*ydim
-//                      columns of length zdim;
-//   tke_update_kernel  everything after the solve (tke.fut:212-347) for one
-//                      cell: the water mask, the surface correction and the
-//                      clip of the top cell, lateral diffusion, the advection
-//                      fluxes east, north and top (recomputed at each
-//                      neighbour rather than stored), dtketau and the
-//                      Adams-Bashforth update.
+// One step is two kernels on the context's stream:
+//   tke_advect_kernel  the advection fluxes east, north and top
+//                      (tke.fut:264-319) and dtketau (:320-340).  A thread
+//                      owns one (y, z) of the plane and marches along x over
+//                      a segment, carrying the east flux of x - 1 in a
+//                      register; the north flux of y - 1 and the top flux of
+//                      z - 1 come from the neighbouring threads through shared
+//                      memory, so each flux is evaluated about once.
+//   tke_column_kernel  everything else, one lane per (x, y) column, a warp per
+//                      32 consecutive columns: the coefficients (:103-210) and
+//                      tridagPar's two forward recurrences
+//                      (misc/ocean-sim/tridiag.fut:9-56) in one pass down the
+//                      column, the backward recurrence (:61-79), the water
+//                      mask, the surface correction, clip and lateral
+//                      diffusion of the top cell (:212-263), and the
+//                      Adams-Bashforth update (:341-347) with dtketau from the
+//                      first kernel.  The four fields the coefficients need
+//                      are staged through shared memory in chunks of 8 z
+//                      (cp.async, three stages) as [z][column] tiles, so both
+//                      the coalesced copy and the lane-per-column reads are
+//                      free of bank conflicts; the forward pass leaves the two
+//                      quotients of the backward recurrence, y'/b' and -c/b',
+//                      in an L2-resident [z][column] scratch.
 // Every operation is explicitly rounded (no fused multiply-add) in the
-// reference's operand order, so the outputs equal the CPU oracle's -- which
-// reproduces the reference's golden outputs bit for bit -- exactly.  The work
-// is a few tens of operations per cell over ~25 input arrays: HBM-bound.
+// reference's operand order -- the fold order of each recurrence included --
+// so the outputs equal the CPU oracle's, which reproduces the reference's
+// golden outputs, bit for bit.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -30,17 +41,22 @@
 #include <new>
 #include <string>
 
-#include "lvc_tridiag.cuh"
 #include "tke.h"
-
-using namespace lvc;
 
 namespace {
 
 __device__ __forceinline__ float M_(float a, float b) { return __fmul_rn(a, b); }
 __device__ __forceinline__ float A_(float a, float b) { return __fadd_rn(a, b); }
 __device__ __forceinline__ float S_(float a, float b) { return __fsub_rn(a, b); }
-__device__ __forceinline__ float D_(float a, float b) { return __fdiv_rn(a, b); }
+// a / b correctly rounded.  A zero dividend over a finite non-zero divisor is
+// answered directly (IEEE 754: a zero whose sign is the XOR of the operands'
+// signs): such quotients are common here -- dry cells have a = c = d = 0 --
+// and would otherwise leave the division's fast path.
+__device__ __forceinline__ float D_(float a, float b) {
+  if (a == 0.0f && b != 0.0f && fabsf(b) <= 3.402823466e38f)
+    return __int_as_float((__float_as_int(a) ^ __float_as_int(b)) & (int)0x80000000);
+  return __fdiv_rn(a, b);
+}
 // std::max / std::min as the oracle evaluates them
 __device__ __forceinline__ float max_(float a, float b) { return (a < b) ? b : a; }
 __device__ __forceinline__ float min_(float a, float b) { return (b < a) ? b : a; }
@@ -53,8 +69,9 @@ struct TkeArgs {
   const float *dxt, *dxu, *dyt, *dyu, *dzt, *dzw, *cost, *cosu;
   const int32_t* kbot;
   const float *kappaM, *mxl, *forc, *forc_tke_surface;
-  float *a, *b, *c, *d, *sol;                                 // scratch [X][Y][Z]
-  float *tketaup1_out, *dtketau_out, *tke_surf_corr_out;      // outputs
+  float *q0, *q1;         // scratch [zdim][ncolp]: y'_z / b'_z and -c_z / b'_z of each column
+  int64_t ncolp;          // xdim * ydim rounded up to 32
+  float *tketaup1_out, *dtketau_out, *tke_surf_corr_out;  // outputs
 };
 
 __device__ __forceinline__ int64_t i3(const TkeArgs& p, int x, int y, int z) {
@@ -62,50 +79,6 @@ __device__ __forceinline__ int64_t i3(const TkeArgs& p, int x, int y, int z) {
 }
 __device__ __forceinline__ bool interior(const TkeArgs& p, int x, int y) {
   return x >= 2 && x < p.X - 2 && y >= 2 && y < p.Y - 2;
-}
-// tke.fut:103-108
-__device__ __forceinline__ float delta_at(const TkeArgs& p, int x, int y, int z) {
-  if (!(interior(p, x, y) && z < p.Z - 1)) return 0.0f;
-  return M_(M_(M_(D_(kDtTke, p.dzt[z + 1]), kAlphaTke), 0.5f),
-            A_(p.kappaM[i3(p, x, y, z)], p.kappaM[i3(p, x, y, z + 1)]));
-}
-
-__global__ void __launch_bounds__(256) tke_coef_kernel(TkeArgs p) {
-  const int64_t n = (int64_t)p.X * p.Y * p.Z;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    const int z = (int)(i % p.Z);
-    const int64_t xy = i / p.Z;
-    const int y = (int)(xy % p.Y), x = (int)(xy / p.Y);
-    const float sqrttke = __fsqrt_rn(max_(0.0f, p.tketau[i]));
-    float av = 0.0f, bv = 0.0f, cv = 0.0f, dv = 0.0f;
-    if (interior(p, x, y)) {
-      const int ks = p.kbot[xy] - 1;
-      const bool land = ks >= 0, edge = land && z == ks, water = land && z >= ks;
-      const float dz = p.dzw[z];
-      const float d0 = delta_at(p, x, y, z);
-      const float dm = z > 0 ? delta_at(p, x, y, z - 1) : 0.0f;
-      // a_tri (:109-122)
-      if (edge || !water) av = 0.0f;
-      else if (z > 0 && z < p.Z - 1) av = D_(-dm, dz);
-      else if (z == p.Z - 1) av = D_(-dm, M_(0.5f, dz));
-      // b_tri (:123-146)
-      if (!water) bv = 1.0f;
-      else if (edge) bv = A_(A_(1.0f, D_(d0, dz)), M_(D_(M_(kDtTke, kCEps), p.mxl[i]), sqrttke));
-      else if (z > 0 && z < p.Z - 1) bv = A_(A_(1.0f, D_(A_(d0, dm), dz)), D_(M_(M_(kDtTke, kCEps), sqrttke), p.mxl[i]));
-      else if (z == p.Z - 1) bv = A_(A_(1.0f, D_(dm, M_(0.5f, dz))), M_(D_(M_(kDtTke, kCEps), p.mxl[i]), sqrttke));
-      // c_tri (:187-196)
-      if (z < p.Z - 1) cv = water ? D_(-d0, dz) : 0.0f;
-      // d_tri (:197-210)
-      if (water) {
-        const float tmp = A_(p.tketau[i], M_(kDtTke, p.forc[i]));
-        dv = (z == p.Z - 1) ? A_(tmp, D_(M_(kDtTke, p.forc_tke_surface[xy]), M_(0.5f, dz))) : tmp;
-      }
-    }
-    p.a[i] = av;
-    p.b[i] = bv;
-    p.c[i] = cv;
-    p.d[i] = dv;
-  }
 }
 
 // tke.fut:19-41
@@ -122,7 +95,7 @@ __device__ __forceinline__ float calcflux(float velfac, float velS, float dt_tra
   const float rjm = M_(S_(varS, varSM1), maskSM1);
   const float epsilon = 0.00000000000000000001f;
   const float divisor = (fabsf(rj) < epsilon) ? epsilon : rj;
-  float cr = (velS > 0.0f) ? D_(rjm, divisor) : D_(rjp, divisor);
+  float cr = D_((velS > 0.0f) ? rjm : rjp, divisor);  // one division of the selected dividend
   cr = limiter(cr);
   return S_(M_(M_(scaledVel, A_(varSP1, varS)), 0.5f),
             M_(M_(M_(fabsf(scaledVel), A_(S_(1.0f, cr), M_(uCFL, cr))), rj), 0.5f));
@@ -174,48 +147,415 @@ __device__ __forceinline__ float adv_top(const TkeArgs& p, int x, int y, int z) 
                   M_(mWs, mWp1), M_(mWm1, mWs), M_(mWp1, mWp2));
 }
 
-__global__ void __launch_bounds__(256) tke_update_kernel(TkeArgs p) {
-  const int64_t n = (int64_t)p.X * p.Y * p.Z;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    const int z = (int)(i % p.Z);
-    const int64_t xy = i / p.Z;
-    const int y = (int)(xy % p.Y), x = (int)(xy / p.Y);
-    const bool inner = interior(p, x, y);
-    const int ks = p.kbot[xy] - 1;
-    const bool water = ks >= 0 && z >= ks;
-    float tp = (inner && water) ? p.sol[i] : p.tketaup1[i];  // :212-218
-    if (z == p.Z - 1) {
-      // surface correction (:219-226), from the value before the clip
-      float corr = 0.0f;
-      if (inner && tp < 0.0f) corr = D_(M_(M_(-tp, 0.5f), p.dzw[p.Z - 1]), kDtTke);
-      p.tke_surf_corr_out[xy] = corr;
-      if (inner) {
-        tp = tp < 0.0f ? 0.0f : tp;  // :227-235
-        // lateral diffusion (:252-263)
-        tp = A_(tp, M_(M_(kDtTke, p.maskW[i]),
-                       A_(D_(S_(diff_east(p, x, y, z), diff_east(p, x - 1, y, z)), M_(p.cost[y], p.dxt[x])),
-                          D_(S_(diff_north(p, x, y, z), diff_north(p, x, y - 1, z)), M_(p.cost[y], p.dyt[y])))));
+// ---------------------------------------------------------------------------
+// tke_advect_kernel
+// ---------------------------------------------------------------------------
+constexpr int kAdvThreads = 512;
+
+// Block b.x covers kAdvThreads consecutive (y, z) of the plane (z fastest),
+// block b.y the x segment [b.y * xseg, ...).  A thread keeps tketau and maskW
+// of x - 1 .. x + 2 at its (y, z) in registers (the east flux, :264-281) and
+// publishes those of x in shared memory, where its neighbours (y +- 1, y + 2)
+// and (z +- 1, z + 2) read them for the north (:282-299) and top (:300-319)
+// fluxes -- from global memory where the neighbour is outside the block.  The
+// north flux of (y - 1, z) is thread t - zdim's and the top flux of
+// (y, z - 1) thread t - 1's, again through shared memory; the first zdim
+// threads (resp. thread 0) evaluate that neighbour's flux themselves.
+__global__ void __launch_bounds__(kAdvThreads, 2) tke_advect_kernel(TkeArgs p, int xseg) {
+  __shared__ float sT[kAdvThreads], sW[kAdvThreads], sfn[kAdvThreads], sft[kAdvThreads];
+  const int t = threadIdx.x;
+  const int64_t plane = (int64_t)p.Y * p.Z;
+  const int64_t qi = (int64_t)blockIdx.x * kAdvThreads + t;
+  const bool live = qi < plane;
+  const int Z = p.Z;
+  const int y = live ? (int)(qi / Z) : 0, z = live ? (int)(qi % Z) : 0;
+  const int xs = blockIdx.y * xseg, xe = min(p.X, xs + xseg);
+  const bool n_in = t - Z >= 0 && t + 2 * Z < kAdvThreads;  // (y - 1 .. y + 2, z) in this block
+  const bool t_in = t >= 1 && t + 2 < kAdvThreads;           // (y, z - 1 .. z + 2) in this block
+  const bool yint = y >= 2 && y < p.Y - 2;
+  const float cy = live ? p.cost[y] : 1.0f, cuy = live ? p.cosu[y] : 1.0f, dyt = live ? p.dyt[y] : 1.0f;
+  const float dz = live ? p.dzw[z] : 1.0f;
+  auto ldT = [&](int xx) { return (live && xx >= 0 && xx < p.X) ? p.tketau[xx * plane + qi] : 0.0f; };
+  auto ldW = [&](int xx) { return (live && xx >= 0 && xx < p.X) ? p.maskW[xx * plane + qi] : 0.0f; };
+  float T0 = ldT(xs - 1), T1 = ldT(xs), T2 = ldT(xs + 1), T3 = ldT(xs + 2);  // x - 1 .. x + 2
+  float W0 = ldW(xs - 1), W1 = ldW(xs), W2 = ldW(xs + 1), W3 = ldW(xs + 2);
+  float fe_prev = (live && xs >= 1) ? adv_east(p, xs - 1, y, z) : 0.0f;
+  for (int x = xs; x < xe; x++) {
+    const int64_t i = x * plane + qi;
+    sT[t] = T1;
+    sW[t] = W1;
+    const float nT = ldT(x + 3), nW = ldW(x + 3);  // next step's window end
+    __syncthreads();
+    float fe = 0.0f, fn = 0.0f, ft = 0.0f;
+    if (live) {
+      const bool xint = x >= 2 && x < p.X - 2;
+      if (x >= 1 && x < p.X - 2 && yint) {
+        const bool in = x < p.X - 1;
+        fe = calcflux(1.0f, p.utau[i], kDtTracer, M_(cy, p.dxt[x]), T1, T0, T2, T3, in ? M_(W1, W2) : 0.0f,
+                      in ? M_(W0, W1) : 0.0f, in ? M_(W2, W3) : 0.0f);
+      }
+      if (y >= 1 && y < p.Y - 2 && xint) {
+        float tm, tp1, tp2, wm, wp1, wp2;
+        if (n_in) {
+          tm = sT[t - Z];
+          tp1 = sT[t + Z];
+          tp2 = sT[t + 2 * Z];
+          wm = sW[t - Z];
+          wp1 = sW[t + Z];
+          wp2 = sW[t + 2 * Z];
+        } else {
+          tm = p.tketau[i - Z];
+          tp1 = p.tketau[i + Z];
+          tp2 = p.tketau[i + 2 * Z];
+          wm = p.maskW[i - Z];
+          wp1 = p.maskW[i + Z];
+          wp2 = p.maskW[i + 2 * Z];
+        }
+        const bool in = y < p.Y - 1;
+        fn = calcflux(cuy, p.vtau[i], kDtTracer, M_(cy, dyt), T1, tm, tp1, tp2, in ? M_(W1, wp1) : 0.0f,
+                      in ? M_(wm, W1) : 0.0f, in ? M_(wp1, wp2) : 0.0f);
+      }
+      if (z < Z - 1 && xint && yint) {
+        float tm = 0.0f, tp1, tp2 = 0.0f, wm = 0.0f, wp1, wp2 = 0.0f;
+        if (t_in) {
+          if (z != 0) {
+            tm = sT[t - 1];
+            wm = sW[t - 1];
+          }
+          tp1 = sT[t + 1];
+          wp1 = sW[t + 1];
+          if (z < Z - 2) {
+            tp2 = sT[t + 2];
+            wp2 = sW[t + 2];
+          }
+        } else {
+          if (z != 0) {
+            tm = p.tketau[i - 1];
+            wm = p.maskW[i - 1];
+          }
+          tp1 = p.tketau[i + 1];
+          wp1 = p.maskW[i + 1];
+          if (z < Z - 2) {
+            tp2 = p.tketau[i + 2];
+            wp2 = p.maskW[i + 2];
+          }
+        }
+        ft = calcflux(1.0f, p.wtau[i], kDtTracer, dz, T1, tm, tp1, tp2, M_(W1, wp1), M_(wm, W1), M_(wp1, wp2));
       }
     }
-    // dtketau (:320-340)
-    float tmp = p.dtketau[i];
-    if (inner)
-      tmp = M_(p.maskW[i], S_(D_(-S_(adv_east(p, x, y, z), adv_east(p, x - 1, y, z)), M_(p.cost[y], p.dxt[x])),
-                              D_(S_(adv_north(p, x, y, z), adv_north(p, x, y - 1, z)), M_(p.cost[y], p.dyt[y]))));
-    const float ft = adv_top(p, x, y, z);
-    const float ftm = z >= 1 ? adv_top(p, x, y, z - 1) : 0.0f;
-    const float z0 = z == 0 ? S_(tmp, D_(ft, p.dzw[0])) : tmp;
-    const float zm = (z >= 1 && z < p.Z - 1) ? S_(z0, D_(S_(ft, ftm), p.dzw[z])) : z0;
-    const float dtk = (z == p.Z - 1) ? S_(zm, D_(S_(ft, ftm), M_(0.5f, p.dzw[z]))) : zm;
-    p.dtketau_out[i] = dtk;
-    // Adams-Bashforth (:341-347)
-    p.tketaup1_out[i] =
-        A_(tp, M_(kDtTracer, S_(M_(A_(1.5f, kABEps), dtk), M_(A_(0.5f, kABEps), p.dtketaum1[i]))));
+    sfn[t] = fn;
+    sft[t] = ft;
+    __syncthreads();
+    if (live) {  // dtketau (:320-340)
+      const float fnm = t >= Z ? sfn[t - Z] : (y >= 1 ? adv_north(p, x, y - 1, z) : 0.0f);
+      const float ftm = t >= 1 ? sft[t - 1] : (z >= 1 ? adv_top(p, x, y, z - 1) : 0.0f);
+      float tmp;
+      if (x >= 2 && x < p.X - 2 && yint)
+        tmp = M_(W1, S_(D_(-S_(fe, fe_prev), M_(cy, p.dxt[x])), D_(S_(fn, fnm), M_(cy, dyt))));
+      else
+        tmp = p.dtketau[i];
+      const float z0 = z == 0 ? S_(tmp, D_(ft, dz)) : tmp;
+      const float zm = (z >= 1 && z < Z - 1) ? S_(z0, D_(S_(ft, ftm), dz)) : z0;
+      p.dtketau_out[i] = (z == Z - 1) ? S_(zm, D_(S_(ft, ftm), M_(0.5f, dz))) : zm;
+    }
+    fe_prev = fe;
+    T0 = T1;
+    T1 = T2;
+    T2 = T3;
+    T3 = nT;
+    W0 = W1;
+    W1 = W2;
+    W2 = W3;
+    W3 = nW;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// tke_column_kernel
+// ---------------------------------------------------------------------------
+constexpr int kColWarps = 4;   // warps per CTA, each on its own 32 columns
+constexpr int kColCh = 8;      // z values per staged chunk
+constexpr int kColStages = 3;  // chunks in flight: current, next (kappaM[z + 1]), prefetch
+constexpr int kColPad = 33;    // [z][column] tile row stride
+constexpr int kColStageFloats = 4 * kColCh * kColPad;  // tketau, kappaM, mxl, forc
+constexpr int kColWarpFloats = kColStages * kColStageFloats + kColCh * kColPad;  // + output tile
+constexpr size_t kColSmem = sizeof(float) * kColWarps * kColWarpFloats;
+
+__device__ __forceinline__ void cp_async4(float* dst, const float* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all_but_one() {
+  asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+}
+
+// Chunk k (z = 8k .. 8k+7) of the four fields of columns col0 .. col0+31
+// into st[field][z - 8k][column]: lane l copies z = 8k + l % 8 of columns
+// l / 8, l / 8 + 4, ..., so a warp instruction reads 32-byte runs of 4 columns.
+__device__ __forceinline__ void col_stage_chunk(const TkeArgs& p, float* st, int64_t col0, int64_t ncol, int k,
+                                                int lane) {
+  const int zz = lane & (kColCh - 1), z = k * kColCh + zz;
+  if (z >= p.Z) return;
+#pragma unroll
+  for (int j = 0; j < 32 / 4; j++) {
+    const int c = j * 4 + (lane >> 3);
+    const int64_t col = col0 + c;
+    if (col < ncol) {
+      const int64_t g = col * p.Z + z;
+      float* d = st + zz * kColPad + c;
+      cp_async4(d, p.tketau + g);
+      cp_async4(d + kColCh * kColPad, p.kappaM + g);
+      cp_async4(d + 2 * kColCh * kColPad, p.mxl + g);
+      cp_async4(d + 3 * kColCh * kColPad, p.forc + g);
+    }
+  }
+}
+
+// Chunk k of the three fields the cells' update reads (dtketau from the
+// advection kernel, dtketaum1, tketaup1) into st[field][z - 8k][column], in
+// the pattern of col_stage_chunk.
+constexpr int kColUpdFloats = 3 * kColCh * kColPad;
+static_assert(2 * kColUpdFloats <= kColStages * kColStageFloats, "update stages reuse the forward stages");
+__device__ __forceinline__ void col_stage_update(const TkeArgs& p, float* st, int64_t col0, int64_t ncol, int k,
+                                                 int lane) {
+  const int zz = lane & (kColCh - 1), z = k * kColCh + zz;
+  if (z >= p.Z) return;
+#pragma unroll
+  for (int j = 0; j < 32 / 4; j++) {
+    const int c = j * 4 + (lane >> 3);
+    const int64_t col = col0 + c;
+    if (col < ncol) {
+      const int64_t g = col * p.Z + z;
+      float* d = st + zz * kColPad + c;
+      cp_async4(d, p.dtketau_out + g);
+      cp_async4(d + kColCh * kColPad, p.dtketaum1 + g);
+      cp_async4(d + 2 * kColCh * kColPad, p.tketaup1 + g);
+    }
+  }
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+__global__ void __launch_bounds__(kColWarps * 32, 3) tke_column_kernel(TkeArgs p) {
+  extern __shared__ float smem[];
+  constexpr unsigned kAll = 0xffffffffu;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t ncol = (int64_t)p.X * p.Y;
+  const int64_t col0 = ((int64_t)blockIdx.x * kColWarps + warp) * 32;
+  if (col0 >= ncol) return;  // whole warps only; the warps of a CTA share no barrier
+  float* st = smem + warp * kColWarpFloats;
+  float* tile = st + kColStages * kColStageFloats;
+  const int Z = p.Z;
+  const int64_t col = col0 + lane;
+  const bool valid = col < ncol;
+  const int x = valid ? (int)(col / p.Y) : 0, y = valid ? (int)(col % p.Y) : 0;
+  const bool inner = valid && interior(p, x, y);
+  const int ks = valid ? p.kbot[col] - 1 : -1;
+  const bool land = ks >= 0;
+  const float fts = inner ? p.forc_tke_surface[col] : 0.0f;
+  const int nch = (Z + kColCh - 1) / kColCh;
+  const int64_t qs = p.ncolp;
+  float* q0 = p.q0 + col;
+  float* q1 = p.q1 + col;
+
+  // Forward, a chunk of 8 z at a time: (A) the coefficients (tke.fut:103-210),
+  // independent across z; (B) tridagPar's recurrences 1 (the 4-tuple scan
+  // for b', tridiag.fut:9-33) and 2 (y', :38-56) folded left to right --
+  // recurrence 2 at z needs b' of z - 1 only; (C) the two quotients the
+  // backward recurrence folds.  Every lane runs A and B (the shuffles need
+  // the whole warp); only interior columns store.
+  float s0 = 1.0f, s1 = 0.0f, s2 = 0.0f, s3 = 1.0f, b0 = 0.0f, y0 = 0.0f, r0 = 0.0f, r1 = 1.0f;
+  float dm = 0.0f, cprev = 0.0f, bpprev = 0.0f;
+  col_stage_chunk(p, st, col0, ncol, 0, lane);
+  cp_async_commit();
+  if (nch > 1) col_stage_chunk(p, st + kColStageFloats, col0, ncol, 1, lane);
+  cp_async_commit();
+  for (int k = 0; k < nch; k++) {
+    if (k + 2 < nch) col_stage_chunk(p, st + ((k + 2) % kColStages) * kColStageFloats, col0, ncol, k + 2, lane);
+    cp_async_commit();
+    cp_async_wait_all_but_one();  // chunks k and k + 1 have landed
+    __syncwarp();
+    const float* cur = st + (k % kColStages) * kColStageFloats;
+    const float* nxt = st + ((k + 1) % kColStages) * kColStageFloats;
+    const int zbase = k * kColCh;
+    const int zn = min(kColCh, Z - zbase);
+    // the chunk's per-z constants, lane l holding those of z = zbase + l % 8
+    float fac_l = 0.0f, dz_l = 1.0f;
+    {
+      const int zl = zbase + (lane & (kColCh - 1));
+      if (zl < Z) dz_l = p.dzw[zl];
+      if (zl < Z - 1) fac_l = M_(M_(D_(kDtTke, p.dzt[zl + 1]), kAlphaTke), 0.5f);
+    }
+    float av[kColCh], bv[kColCh], cv[kColCh], dv[kColCh];
+#pragma unroll
+    for (int zz = 0; zz < kColCh; zz++) {  // (A)
+      const float fac = __shfl_sync(kAll, fac_l, zz);
+      const float dz = __shfl_sync(kAll, dz_l, zz);
+      const int z = zbase + zz;
+      const float t = cur[zz * kColPad + lane];
+      const float kap = cur[(kColCh + zz) * kColPad + lane];
+      const float mx = cur[(2 * kColCh + zz) * kColPad + lane];
+      const float fo = cur[(3 * kColCh + zz) * kColPad + lane];
+      const float kapn = zz + 1 < kColCh ? cur[(kColCh + zz + 1) * kColPad + lane] : nxt[kColCh * kColPad + lane];
+      const float d0 = z < Z - 1 ? M_(fac, A_(kap, kapn)) : 0.0f;  // delta (:103-108)
+      const bool edge = land && z == ks, water = land && z >= ks;
+      const float sq = __fsqrt_rn(max_(0.0f, t));
+      float a_ = 0.0f, b_ = 0.0f, c_ = 0.0f, d_ = 0.0f;
+      // a_tri (:109-122)
+      if (edge || !water) a_ = 0.0f;
+      else if (z > 0 && z < Z - 1) a_ = D_(-dm, dz);
+      else if (z == Z - 1) a_ = D_(-dm, M_(0.5f, dz));
+      // b_tri (:123-146)
+      if (!water) b_ = 1.0f;
+      else if (edge) b_ = A_(A_(1.0f, D_(d0, dz)), M_(D_(M_(kDtTke, kCEps), mx), sq));
+      else if (z > 0 && z < Z - 1) b_ = A_(A_(1.0f, D_(A_(d0, dm), dz)), D_(M_(M_(kDtTke, kCEps), sq), mx));
+      else if (z == Z - 1) b_ = A_(A_(1.0f, D_(dm, M_(0.5f, dz))), M_(D_(M_(kDtTke, kCEps), mx), sq));
+      // c_tri (:187-196)
+      if (z < Z - 1) c_ = water ? D_(-d0, dz) : 0.0f;
+      // d_tri (:197-210)
+      if (water) {
+        const float tmp = A_(t, M_(kDtTke, fo));
+        d_ = (z == Z - 1) ? A_(tmp, D_(M_(kDtTke, fts), M_(0.5f, dz))) : tmp;
+      }
+      av[zz] = a_;
+      bv[zz] = b_;
+      cv[zz] = c_;
+      dv[zz] = d_;
+      dm = d0;
+    }
+    float bp[kColCh], yp[kColCh];
+#pragma unroll
+    for (int zz = 0; zz < kColCh; zz++) {  // (B)
+      if (zz >= zn) break;
+      const int z = zbase + zz;
+      float m0 = 1.0f, m1 = 0.0f, m2 = 0.0f, m3 = 1.0f;
+      if (z > 0) {
+        m0 = bv[zz];
+        m1 = S_(0.0f, M_(av[zz], cprev));
+        m2 = 1.0f;
+        m3 = 0.0f;
+      } else {
+        b0 = bv[zz];
+      }
+      const float value = __frcp_rn(M_(s0, m0));  // 1 / (s0 m0), correctly rounded
+      const float n0 = M_(A_(M_(m0, s0), M_(m1, s2)), value);
+      const float n1 = M_(A_(M_(m0, s1), M_(m1, s3)), value);
+      const float n2 = M_(A_(M_(m2, s0), M_(m3, s2)), value);
+      const float n3 = M_(A_(M_(m2, s1), M_(m3, s3)), value);
+      s0 = n0;
+      s1 = n1;
+      s2 = n2;
+      s3 = n3;
+      bp[zz] = D_(A_(M_(s0, b0), s1), A_(M_(s2, b0), s3));
+      float l0 = 0.0f, l1 = 1.0f;
+      if (z > 0) {
+        l0 = dv[zz];
+        l1 = S_(0.0f, D_(av[zz], bpprev));
+      } else {
+        y0 = dv[zz];
+      }
+      const float rn0 = A_(l0, M_(l1, r0)), rn1 = M_(r1, l1);
+      r0 = rn0;
+      r1 = rn1;
+      yp[zz] = A_(r0, M_(r1, y0));
+      cprev = cv[zz];
+      bpprev = bp[zz];
+    }
+    if (inner) {
+#pragma unroll
+      for (int zz = 0; zz < kColCh; zz++) {  // (C) y'/b' and -c/b' (:61-79)
+        if (zz >= zn) break;
+        const int64_t o = (int64_t)(zbase + zz) * qs;
+        q0[o] = D_(yp[zz], bp[zz]);
+        q1[o] = S_(0.0f, D_(cv[zz], bp[zz]));
+      }
+    }
+    __syncwarp();  // the next iteration refills this chunk's stage
+  }
+  cp_async_wait_all();
+
+  // Backward, a chunk at a time from the top: recurrence 3 down the column
+  // into the tile, then the chunk's cells (coalesced): take the solution or
+  // keep tketaup1 (:212-218), the top cell's correction, clip and lateral
+  // diffusion (:219-263), Adams-Bashforth (:341-347).  The next chunk's
+  // quotients (registers) and update fields (cp.async) load meanwhile.
+  float* ust = st;
+  const float yn = inner ? q0[(int64_t)(Z - 1) * qs] : 0.0f;  // y'_{n-1} / b'_{n-1}
+  r0 = 0.0f;
+  r1 = 1.0f;
+  if (valid && !inner) p.tke_surf_corr_out[col] = 0.0f;
+  float qa0[kColCh], qa1[kColCh];
+  {
+    const int k = nch - 1, zn = Z - k * kColCh;
+#pragma unroll
+    for (int zz = 0; zz < kColCh; zz++) {  // element n - 1 folds the neutral (0, 1)
+      const int z = k * kColCh + zz;
+      const bool ld = inner && zz < zn && z < Z - 1;
+      qa0[zz] = ld ? q0[(int64_t)z * qs] : 0.0f;
+      qa1[zz] = ld ? q1[(int64_t)z * qs] : 1.0f;
+    }
+  }
+  col_stage_update(p, ust + ((nch - 1) & 1) * kColUpdFloats, col0, ncol, nch - 1, lane);
+  cp_async_commit();
+  for (int k = nch - 1; k >= 0; k--) {
+    const int zn = min(kColCh, Z - k * kColCh);
+    float qn0[kColCh], qn1[kColCh];
+    if (k >= 1) col_stage_update(p, ust + ((k - 1) & 1) * kColUpdFloats, col0, ncol, k - 1, lane);
+    cp_async_commit();
+#pragma unroll
+    for (int zz = 0; zz < kColCh; zz++) {  // chunk k - 1 is full and below the top cell
+      const int64_t o = (int64_t)((k - 1) * kColCh + zz) * qs;
+      qn0[zz] = (inner && k >= 1) ? q0[o] : 0.0f;
+      qn1[zz] = (inner && k >= 1) ? q1[o] : 1.0f;
+    }
+    if (inner) {
+#pragma unroll
+      for (int zz = kColCh - 1; zz >= 0; zz--) {
+        if (zz >= zn) continue;
+        const int z = k * kColCh + zz;
+        const float rn0 = A_(qa0[zz], M_(qa1[zz], r0)), rn1 = M_(r1, qa1[zz]);
+        r0 = rn0;
+        r1 = rn1;
+        float v = A_(r0, M_(r1, yn));
+        if (z == Z - 1) {  // the top cell
+          float tp = (land && z >= ks) ? v : p.tketaup1[col * Z + z];
+          p.tke_surf_corr_out[col] = tp < 0.0f ? D_(M_(M_(-tp, 0.5f), p.dzw[Z - 1]), kDtTke) : 0.0f;
+          tp = tp < 0.0f ? 0.0f : tp;
+          v = A_(tp, M_(M_(kDtTke, p.maskW[col * Z + z]),
+                        A_(D_(S_(diff_east(p, x, y, z), diff_east(p, x - 1, y, z)), M_(p.cost[y], p.dxt[x])),
+                           D_(S_(diff_north(p, x, y, z), diff_north(p, x, y - 1, z)), M_(p.cost[y], p.dyt[y])))));
+        }
+        tile[zz * kColPad + lane] = v;
+      }
+    }
+    cp_async_wait_all_but_one();  // chunk k's update fields have landed
+    __syncwarp();
+    const float* u = ust + (k & 1) * kColUpdFloats;
+#pragma unroll
+    for (int j = 0; j < 32 / 4; j++) {
+      const int c = j * 4 + (lane >> 3), zz = lane & (kColCh - 1);
+      const int in_c = __shfl_sync(kAll, (int)inner, c);
+      const int ks_c = __shfl_sync(kAll, ks, c);
+      const int64_t cc = col0 + c;
+      if (cc < ncol && zz < zn) {
+        const int z = k * kColCh + zz;
+        const bool take = in_c && (z == Z - 1 || (ks_c >= 0 && z >= ks_c));
+        const float* uf = u + zz * kColPad + c;
+        const float tp = take ? tile[zz * kColPad + c] : uf[2 * kColCh * kColPad];
+        p.tketaup1_out[cc * Z + z] =
+            A_(tp, M_(kDtTracer, S_(M_(A_(1.5f, kABEps), uf[0]), M_(A_(0.5f, kABEps), uf[kColCh * kColPad]))));
+      }
+    }
+    __syncwarp();  // the tile and this stage are rewritten two chunks on
+#pragma unroll
+    for (int zz = 0; zz < kColCh; zz++) {
+      qa0[zz] = qn0[zz];
+      qa1[zz] = qn1[zz];
+    }
   }
 }
 
 }  // namespace
-
 // ---------------------------------------------------------------------------
 // Contexts and arrays (the generated API's shapes)
 // ---------------------------------------------------------------------------
@@ -353,11 +693,11 @@ int values_array(futhark_context* ctx, A* a, T* out) {
   return e == cudaSuccess ? 0 : cuda_fail(ctx, e, "device to host copy");
 }
 
+int64_t padded_columns(int64_t X, int64_t Y) { return (X * Y + 31) & ~int64_t(31); }
+
 size_t scratch_bytes(int64_t X, int64_t Y, int64_t Z) {
-  // a, b, c, d, sol and the generic solver's pivots (zdim > kTriBlockMaxM),
-  // each on a 128-byte boundary for the block solver's bulk copies
-  const int64_t ns = (X * Y * Z + 31) & ~int64_t(31);
-  return 6 * sizeof(float) * (size_t)std::max<int64_t>(32, ns);
+  // the two quotient planes q0, q1 of [zdim][ncolp] floats
+  return 2 * sizeof(float) * (size_t)std::max<int64_t>(32, Z * padded_columns(X, Y));
 }
 
 // Enqueues one step on the context's stream (lock held, device set).
@@ -373,7 +713,6 @@ int step_launch(futhark_context* ctx, const tke_step_args* q) {
   if (n == 0) return 0;
   if (((uintptr_t)q->scratch & 127) != 0)
     return set_error(ctx, FUTHARK_PROGRAM_ERROR, "tke step: scratch is not on a 128-byte boundary");
-  const int64_t ns = (n + 31) & ~int64_t(31);
   float* scratch = static_cast<float*>(q->scratch);
   TkeArgs p;
   p.X = (int)X;
@@ -402,52 +741,40 @@ int step_launch(futhark_context* ctx, const tke_step_args* q) {
   p.mxl = q->mxl;
   p.forc = q->forc;
   p.forc_tke_surface = q->forc_tke_surface;
-  p.a = scratch;
-  p.b = scratch + ns;
-  p.c = scratch + 2 * ns;
-  p.d = scratch + 3 * ns;
-  p.sol = scratch + 4 * ns;
+  p.ncolp = padded_columns(X, Y);
+  p.q0 = scratch;
+  p.q1 = scratch + Z * p.ncolp;
   p.tketaup1_out = q->tketaup1_out;
   p.dtketau_out = q->dtketau_out;
   p.tke_surf_corr_out = q->tke_surf_corr_out;
   cudaStream_t s = ctx->stream;
-  const int grid = (int)std::min<int64_t>((n + 255) / 256, 32LL * ctx->num_sms);
-  tke_coef_kernel<<<grid, 256, 0, s>>>(p);
+  // advection and dtketau: x segments so that about four waves of CTAs run
+  const int64_t plane_blocks = (Y * Z + kAdvThreads - 1) / kAdvThreads;
+  const int64_t want_blocks = 4LL * 2 * ctx->num_sms;  // two CTAs per SM
+  const int64_t nseg = std::max<int64_t>(1, std::min<int64_t>(X, (want_blocks + plane_blocks - 1) / plane_blocks));
+  const int xseg = (int)((X + nseg - 1) / nseg);
+  const int64_t segs = (X + xseg - 1) / xseg;
+  if (plane_blocks > INT32_MAX || segs > 65535)
+    return set_error(ctx, FUTHARK_PROGRAM_ERROR, "tke step: plane too large");
+  tke_advect_kernel<<<dim3((unsigned)plane_blocks, (unsigned)segs), kAdvThreads, 0, s>>>(p, xseg);
   cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return cuda_fail(ctx, e, "tke coefficient launch");
-  // the vertical solve: X*Y systems of length Z (tke.fut:4-17, 211)
-  const int64_t rows = X * Y;
-  if (Z <= kTriBlockMaxM) {
-    const size_t bs = (size_t)((kTriBlockRows * Z + 3) & ~int64_t(3));
-    const size_t smem = 16 + 4 * bs * sizeof(float);
-    const size_t smem_max = 16 + 4 * (size_t)((kTriBlockRows * kTriBlockMaxM + 3) & ~3) * sizeof(float);
-    e = cudaFuncSetAttribute((const void*)lvc_tridag_block_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem_max);
-    if (e != cudaSuccess) return cuda_fail(ctx, e, "tke solver attributes");
-    lvc_tridag_block_kernel<1><<<(unsigned)((rows + kTriBlockRows - 1) / kTriBlockRows), kTriBlockRows, smem, s>>>(
-        rows, (int)Z, p.a, p.b, p.c, p.d, p.sol, 1);
-  } else {
-    lvc_tridag_kernel<1><<<(unsigned)((rows + kTriThreads - 1) / kTriThreads), kTriThreads, 0, s>>>(
-        rows, (int)Z, p.a, p.b, p.c, p.d, p.sol, scratch + 5 * ns);
-  }
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "tke advection launch");
+  // the columns: coefficients, tridagPar, tketaup1 (tke.fut:103-263, 341-347)
+  const int64_t col_blocks = (X * Y + 32 * kColWarps - 1) / (32 * kColWarps);
+  if (col_blocks > INT32_MAX) return set_error(ctx, FUTHARK_PROGRAM_ERROR, "tke step: too many columns");
+  e = cudaFuncSetAttribute((const void*)tke_column_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kColSmem);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "tke column attributes");
+  tke_column_kernel<<<(unsigned)col_blocks, 32 * kColWarps, kColSmem, s>>>(p);
   e = cudaGetLastError();
-  if (e != cudaSuccess) return cuda_fail(ctx, e, "tke solver launch");
-  tke_update_kernel<<<grid, 256, 0, s>>>(p);
-  e = cudaGetLastError();
-  if (e != cudaSuccess) return cuda_fail(ctx, e, "tke update launch");
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "tke column launch");
   return 0;
 }
 
-// Synchronises and reads (then clears) the solver's timeout flag (lock held).
+// Synchronises the context's stream and reports a failed step (lock held).
 int check_locked(futhark_context* ctx) {
-  int flag = 0;
-  const int zero = 0;
-  cudaError_t e = cudaMemcpyFromSymbolAsync(&flag, lvc_tridag_err, sizeof flag, 0, cudaMemcpyDeviceToHost, ctx->stream);
-  if (e == cudaSuccess) e = cudaMemcpyToSymbolAsync(lvc_tridag_err, &zero, sizeof zero, 0, cudaMemcpyHostToDevice, ctx->stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
-  if (e != cudaSuccess) return cuda_fail(ctx, e, "tke step");
-  if (flag) return set_error(ctx, FUTHARK_PROGRAM_ERROR, "tke step: the vertical solve gave up waiting on a copy");
-  return 0;
+  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  return e == cudaSuccess ? 0 : cuda_fail(ctx, e, "tke step");
 }
 
 }  // namespace
@@ -686,6 +1013,6 @@ int tke_check(struct futhark_context* ctx) {
   return check_locked(ctx);
 }
 void* tke_context_stream(struct futhark_context* ctx) { return ctx && ctx->ok ? (void*)ctx->stream : nullptr; }
-int tke_launches_per_step(void) { return 3; }
+int tke_launches_per_step(void) { return 2; }
 
 }  // extern "C"
