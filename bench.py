@@ -69,6 +69,9 @@ def parse():
     ap.add_argument("--no-tke", action="store_true", help="skip the ocean model's tke step section")
     ap.add_argument("--only-tke", action="store_true",
                     help="run only the tke step section (one GPU) and print its JSON object")
+    ap.add_argument("--no-op", action="store_true", help="skip the OptionPricing section")
+    ap.add_argument("--only-op", action="store_true",
+                    help="run only the OptionPricing section (one GPU) and print its JSON object")
     ap.add_argument("--no-autotune", action="store_true", help="built-in shapes instead of the autotuner's")
     ap.add_argument("--serving-rates", default="100,1000,5000,20000",
                     help="Poisson arrival rates (requests/s) of the serving sweep")
@@ -415,6 +418,75 @@ def run_tke(wl, args):
         tctx.close()
 
 
+def run_op(args):
+    """finpar OptionPricing (libop.so) on the reference's three datasets
+    (finpar/OptionPricing-data, kept as fixtures under tests/golden): device
+    time per pricing through op_price_f32 with the inputs resident, end to end
+    through futhark_entry_main with host arrays, agreement with the golden
+    outputs and the oracle, CPU baseline (the oracle on all host threads, a
+    bounded number of paths)."""
+    import numpy as np
+    import torch
+    from oracle import oracle
+    op = importlib.import_module("futhark-benchmarks_b200.op")
+    here = os.path.dirname(os.path.abspath(__file__))
+    octx = op.OpContext()
+    res = {"entry": "futhark_entry_main (libop.so)", "datasets": {}}
+    try:
+        for name in ("small", "medium", "large"):
+            z = np.load(os.path.join(here, "tests", "golden", f"optionpricing_{name}.npz"))
+            ins = [z[f"in{i:02d}"] for i in range(11)]
+            golden = z["out0"]
+            contract, paths = int(ins[0]), int(ins[1])
+            dims = op.dims_of(ins)
+            dev = {n: torch.from_numpy(np.ascontiguousarray(v)).cuda() for n, v in zip(op.ARRAY_NAMES, ins[2:])}
+            ptrs = {n: t.data_ptr() for n, t in dev.items()}
+            out = torch.empty(dims["num_models"], dtype=torch.float32, device="cuda")
+            scratch = torch.empty(octx.scratch_bytes(contract, paths, dims), dtype=torch.uint8, device="cuda")
+            ext = torch.cuda.ExternalStream(octx.stream)
+            torch.cuda.synchronize()
+            for _ in range(max(3, args.warmup)):
+                octx.price(contract, paths, dims, ptrs, out.data_ptr(), scratch.data_ptr())
+            octx.check()
+            times = []
+            for _ in range(max(5, args.steps)):
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(ext)
+                octx.price(contract, paths, dims, ptrs, out.data_ptr(), scratch.data_ptr())
+                e1.record(ext)
+                octx.check()
+                times.append(e0.elapsed_time(e1))
+            ms = float(np.median(times))
+            got = out.cpu().numpy()
+            octx.main(*ins)
+            reps = 3
+            t0 = time.perf_counter()
+            for _ in range(reps):
+                e2e = octx.main(*ins)
+            e2e_ms = 1e3 * (time.perf_counter() - t0) / reps
+            # CPU baseline: the oracle on all host threads, about a second of paths
+            threads = os.cpu_count() or 1
+            sample = min(paths, {"small": 1 << 22, "medium": 1 << 19, "large": 1 << 14}[name])
+            t0 = time.perf_counter()
+            oracle.option_pricing_sums(*ins, count=sample, threads=threads)
+            cpu_s = time.perf_counter() - t0
+            want = oracle.option_pricing(*ins, threads=threads)
+            res["datasets"][name] = {
+                "contract": contract, "paths": paths, "dates_x_underlyings": [dims["num_dates"], dims["num_und"]],
+                "device_ms": ms, "paths_per_s": paths / (ms * 1e-3), "e2e_ms": e2e_ms,
+                "e2e_paths_per_s": paths / (e2e_ms * 1e-3), "price": float(got[0]), "golden": float(golden[0]),
+                "rel_vs_golden": float(abs(got[0] - golden[0]) / abs(golden[0])),
+                "rel_vs_oracle": float(abs(got[0] - want[0]) / abs(want[0])),
+                "e2e_equals_device": bool(np.array_equal(e2e, got)),
+                "cpu_baseline": {"value": sample / cpu_s, "unit": "paths/s", "cores": threads, "kind": "port",
+                                 "sample": f"{sample} of the {paths} paths, oracle"}}
+            del dev, out, scratch
+    finally:
+        octx.close()
+    return res
+
+
 def run_serving(pkg, wl, ctx, args, rank, precision):
     """Poisson request streams through the serving runtime (continuous batching)."""
     import numpy as np
@@ -571,6 +643,10 @@ def run_ours(args):
     if not args.no_tke and rank == 0:
         tke_res = run_tke(wl, args)
 
+    op_res = None
+    if not args.no_op and rank == 0:
+        op_res = run_op(args)
+
     serving = None
     if not args.no_serving:
         serving = run_serving(pkg, wl, ctx, args, rank, precision)
@@ -614,6 +690,7 @@ def run_ours(args):
             "serving": serving,
             "tridiag": tridiag,
             "tke": tke_res,
+            "option_pricing": op_res,
             "batched_vs_plain": (value / plain["value"]) if plain else None,
             "cpu_baseline": cpu,
             "error_vs_fp64_oracle": err,
@@ -633,6 +710,8 @@ def main():
         run_reference(args)
     elif args.only_tke:
         print(json.dumps(run_tke(importlib.import_module("futhark-benchmarks_b200.workloads"), args)))
+    elif args.only_op:
+        print(json.dumps(run_op(args)))
     else:
         run_ours(args)
 

@@ -5,7 +5,7 @@
  * context, the array types of the entry point's parameters, and
  * futhark_entry_main with its seven outputs first and twenty-five inputs
  * after, returning 0 or a FUTHARK_* error code with the message in
- * futhark_context_get_error.  The library is separate from libLocVolCalib.so
+ * futhark_context_get_error.  The library is separate from liblvc.so
  * because both programs' entry points are named futhark_entry_main, as two
  * Futhark-compiled programs would be.  Part 2 is an engine extension: one
  * step on caller-owned device memory, without allocations.
@@ -129,8 +129,7 @@ struct tke_step_args {
 };
 TKE_API size_t tke_scratch_bytes(int64_t xdim, int64_t ydim, int64_t zdim);
 TKE_API int tke_step_f32(struct futhark_context *ctx, const struct tke_step_args *args);
-/* Synchronises the context's stream and reports (FUTHARK_PROGRAM_ERROR) a step
- * since the last check whose vertical solve gave up waiting on a copy. */
+/* Synchronises the context's stream and reports a failed step. */
 TKE_API int tke_check(struct futhark_context *ctx);
 /* The context's CUDA stream (a cudaStream_t). */
 TKE_API void *tke_context_stream(struct futhark_context *ctx);

@@ -133,3 +133,53 @@ def tke(*inputs):
     fn(X, Y, Z, *args)
     return (f32["tketau"].copy(), tp1, f32["tketaum1"].copy(), dtk, f32["dtketaup1"].copy(),
             f32["dtketaum1"].copy(), corr)
+
+
+# finpar/OptionPricing.fut's entry main (op_oracle.cpp): the inputs in the
+# entry point's order.
+OP_INPUTS = ["contract_number", "num_mc_it", "dir_vs", "md_cs", "md_vols", "md_drifts", "md_sts", "md_detvals",
+             "md_discts", "bb_inds", "bb_data"]
+
+
+def _op_arrays(inputs):
+    v = dict(zip(OP_INPUTS, inputs))
+    a = {k: np.ascontiguousarray(v[k], dtype=np.int32 if k in ("dir_vs", "bb_inds") else np.float32)
+         for k in OP_INPUTS[2:]}
+    num_models, num_dates, num_und = a["md_vols"].shape
+    dims = (int(v["contract_number"]), int(a["dir_vs"].shape[1]), num_models, num_und, num_dates,
+            int(a["md_discts"].shape[1]))
+    return int(v["num_mc_it"]), a, dims
+
+
+def option_pricing_sums(*inputs, first: int = 0, count: int | None = None, threads: int | None = None):
+    """Per-model f64 sums of the payoffs of paths [first, first + count)."""
+    num_mc_it, a, dims = _op_arrays(inputs)
+    L = load()
+    fn = L.lvc_oracle_op_sums
+    fn.restype = None
+    fn.argtypes = [ctypes.c_int] * 6 + [ctypes.c_void_p] * 9 + [ctypes.c_int64, ctypes.c_int64, ctypes.c_int,
+                                                                  ctypes.c_void_p]
+    count = num_mc_it - first if count is None else count
+    threads = threads or max(1, min(os.cpu_count() or 1, 64))
+    sums = np.zeros(dims[2], np.float64)
+    fn(*dims, *[a[k].ctypes.data for k in OP_INPUTS[2:]], first, count, threads, sums.ctypes.data)
+    return sums
+
+
+def option_pricing(*inputs, threads: int | None = None) -> np.ndarray:
+    """finpar/OptionPricing.fut's main (f32): [num_models] mean payoffs."""
+    num_mc_it = int(inputs[1])
+    sums = option_pricing_sums(*inputs, threads=threads)
+    return (sums.astype(np.float32) / np.float32(num_mc_it)).astype(np.float32)
+
+
+def option_pricing_path(*inputs, n: int) -> np.ndarray:
+    """One path's (Sobol index n, 1-based) f32 payoffs per model."""
+    _, a, dims = _op_arrays(inputs)
+    L = load()
+    fn = L.lvc_oracle_op_path
+    fn.restype = None
+    fn.argtypes = [ctypes.c_int] * 6 + [ctypes.c_void_p] * 9 + [ctypes.c_int32, ctypes.c_void_p]
+    out = np.zeros(dims[2], np.float64)
+    fn(*dims, *[a[k].ctypes.data for k in OP_INPUTS[2:]], n, out.ctypes.data)
+    return out.astype(np.float32)

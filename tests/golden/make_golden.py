@@ -11,6 +11,10 @@ present:
   tridiag32_small.npz       a, b, c, y [100][115] f32 and the expected x
   tke32_small.npz           misc/ocean-sim/data/tke32-small.{in,out}: in00..in24
                             (the 25 inputs of tke.fut's main) and out0..out6
+  optionpricing_{small,medium,large}.npz
+                            finpar/OptionPricing-data/*.{in,out} (the test stanza of
+                            finpar/OptionPricing.fut:1-11): in00..in10 (the 11 inputs
+                            of main) and out0
 
 Usage:  python tests/golden/make_golden.py [REFERENCE_ROOT]
 (REFERENCE_ROOT defaults to /root/reference.)
@@ -62,6 +66,14 @@ def main(ref_root: str) -> None:
     np.savez_compressed(os.path.join(HERE, "tke32_small.npz"),
                         **{f"in{i:02d}": v for i, v in enumerate(ins)},
                         **{f"out{i}": v for i, v in enumerate(outs)})
+    # finpar/OptionPricing.fut's test stanza: 11 inputs, 1 output
+    odir = os.path.join(ref_root, "finpar", "OptionPricing-data")
+    for name in ("small", "medium", "large"):
+        ins = fd.read_file(os.path.join(odir, f"{name}.in"))
+        outs = fd.read_file(os.path.join(odir, f"{name}.out"))
+        np.savez_compressed(os.path.join(HERE, f"optionpricing_{name}.npz"),
+                            **{f"in{i:02d}": np.asarray(v) for i, v in enumerate(ins)},
+                            **{f"out{i}": np.asarray(v) for i, v in enumerate(outs)})
     print("wrote", os.listdir(HERE))
 
 

@@ -3,6 +3,7 @@ include/*.h declares, and a context on a machine without a usable device
 reports an error instead of crashing."""
 import ctypes
 import glob
+import importlib
 import os
 import re
 
@@ -11,9 +12,9 @@ import pytest
 from conftest import REPO
 
 HEADERS = sorted(glob.glob(os.path.join(REPO, "include", "*.h")))
-DECL = re.compile(r"^(?:LVC|TKE)_API\s+[^(]*?\b([A-Za-z_][A-Za-z_0-9]*)\s*\(", re.M)
+DECL = re.compile(r"^(?:LVC|TKE|OP)_API\s+[^(]*?\b([A-Za-z_][A-Za-z_0-9]*)\s*\(", re.M)
 # which library implements each header
-HEADER_LIB = {"LocVolCalib.h": "liblvc.so", "tridiag.h": "liblvc.so", "tke.h": "libtke.so"}
+HEADER_LIB = {"LocVolCalib.h": "liblvc.so", "tridiag.h": "liblvc.so", "tke.h": "libtke.so", "op.h": "libop.so"}
 
 
 def declared_functions(lib_name: str = "liblvc.so"):
@@ -54,6 +55,15 @@ def test_tke_mirror_binds_every_declared_symbol(tke):
     lib = tke.load_library()
     unbound = [n for n in declared_functions("libtke.so") if getattr(lib, n).argtypes is None]
     assert not unbound, unbound
+
+
+def test_op_mirror_binds_every_declared_symbol():
+    op = importlib.import_module("futhark-benchmarks_b200.op")
+    lib = op.load_library()
+    unbound = [n for n in declared_functions("libop.so") if getattr(lib, n).argtypes is None]
+    assert not unbound, unbound
+    # struct op_args: seven int32 sizes, then nine pointers
+    assert ctypes.sizeof(op._OpArgs) == 8 * 4 + 9 * 8
 
 
 def test_tke_context_without_gpu_reports_error(tke, pkg):
