@@ -30,14 +30,14 @@ struct futhark_context {
   cudaStream_t stream = nullptr;
   std::string error;
   bool ok = false;
-  void* scratch = nullptr;  // the entry point's step scratch, grown on demand
+  void* scratch = nullptr;  // the entry point's scratch, grown on demand
   size_t scratch_bytes = 0;
 };
 
 namespace {
 
-// Device storage shared by the arrays that view it: the entry point returns
-// its four pass-through outputs as views of the consumed inputs' storage.
+// Device storage shared by the arrays that view it, so that an entry point can
+// return a consumed input unchanged as an output without copying it.
 struct DevMem {
   void* p = nullptr;
   int refs = 1;

@@ -95,15 +95,23 @@ __device__ __forceinline__ float poly_appr(float x, const float* a, const float*
   return num / den;
 }
 
-// :120-136
-__device__ __forceinline__ float ugaussian_el(float p) {
-  const float dp = p - 0.5f;
-  if ((dp < 0.0f && 0.0f - dp <= 0.425f) || (0.0f <= dp && dp <= 0.425f))
-    return dp * poly_appr(0.180625f - dp * dp, kSmallA, kSmallB);
+// :120-136, split at its branch: gauss_central for |p - 0.5| <= 0.425,
+// gauss_tail otherwise
+__device__ __forceinline__ bool gauss_is_central(float dp) {
+  return (dp < 0.0f && 0.0f - dp <= 0.425f) || (0.0f <= dp && dp <= 0.425f);
+}
+__device__ __forceinline__ float gauss_central(float dp) {
+  return dp * poly_appr(0.180625f - dp * dp, kSmallA, kSmallB);
+}
+__device__ __forceinline__ float gauss_tail(float dp) {
   const float pp = dp < 0.0f ? dp + 0.5f : 0.5f - dp;
   const float r = sqrtf(-f32log(pp));
   const float x = r <= 5.0f ? poly_appr(r - 1.6f, kInterA, kInterB) : poly_appr(r - 5.0f, kTailA, kTailB);
   return dp < 0.0f ? 0.0f - x : x;
+}
+__device__ __forceinline__ float ugaussian_el(float p) {
+  const float dp = p - 0.5f;
+  return gauss_is_central(dp) ? gauss_central(dp) : gauss_tail(dp);
 }
 
 // :234-240
@@ -382,10 +390,31 @@ __global__ void __launch_bounds__(kWarpPathWarps * 32, 2) op_paths_warp_kernel(O
 #pragma unroll 4
       for (int k = lane; k < K; k += 32) sX[k] ^= row[k];
     }
-    for (int k = lane; k < K; k += 32) {  // Gaussians (:120-136)
-      sG[k] = ugaussian_el((float)sX[k] / divisor);
-      sB[k] = 0.0f;
+    // Gaussians (:120-136) in two passes, so neither branch runs on a
+    // partly idle warp: the central branch for every dimension, queueing
+    // (in sB, free until the bridge) the dimensions that need the tail
+    // branch; then the queue, densely
+    int32_t* queue = reinterpret_cast<int32_t*>(sB);
+    int nq = 0;
+    for (int k0 = 0; k0 < K; k0 += 32) {
+      const int k = k0 + lane;
+      bool tail = false;
+      if (k < K) {
+        const float dp = (float)sX[k] / divisor - 0.5f;
+        if (gauss_is_central(dp)) sG[k] = gauss_central(dp);
+        else tail = true;
+      }
+      const unsigned ball = __ballot_sync(kAll, tail);
+      if (tail) queue[nq + __popc(ball & ((1u << lane) - 1u))] = k;
+      nq += __popc(ball);
     }
+    __syncwarp();
+    for (int q = lane; q < nq; q += 32) {
+      const int k = queue[q];
+      sG[k] = gauss_tail((float)sX[k] / divisor - 0.5f);
+    }
+    __syncwarp();
+    for (int k = lane; k < K; k += 32) sB[k] = 0.0f;
     __syncwarp();
     if (lane < U) sB[(s_ind[0] - 1) * U + lane] = s_dat[0] * sG[lane];
     __syncwarp();

@@ -21,7 +21,7 @@
 //                      diffusion of the top cell (:212-263), and the
 //                      Adams-Bashforth update (:341-347) with dtketau from the
 //                      first kernel.  The four fields the coefficients need
-//                      are staged through shared memory in chunks of 8 z
+//                      are staged through shared memory in chunks of 4 z
 //                      (cp.async, three stages) as [z][column] tiles, so both
 //                      the coalesced copy and the lane-per-column reads are
 //                      free of bank conflicts; the forward pass leaves the two
@@ -275,7 +275,7 @@ __global__ void __launch_bounds__(kAdvThreads, 2) tke_advect_kernel(TkeArgs p, i
 // tke_column_kernel
 // ---------------------------------------------------------------------------
 constexpr int kColWarps = 4;   // warps per CTA, each on its own 32 columns
-constexpr int kColCh = 8;      // z values per staged chunk
+constexpr int kColCh = 4;      // z values per staged chunk (a power of two <= 32)
 constexpr int kColStages = 3;  // chunks in flight: current, next (kappaM[z + 1]), prefetch
 constexpr int kColPad = 33;    // [z][column] tile row stride
 constexpr int kColStageFloats = 4 * kColCh * kColPad;  // tketau, kappaM, mxl, forc
@@ -291,16 +291,17 @@ __device__ __forceinline__ void cp_async_wait_all_but_one() {
   asm volatile("cp.async.wait_group 1;\n" ::: "memory");
 }
 
-// Chunk k (z = 8k .. 8k+7) of the four fields of columns col0 .. col0+31
-// into st[field][z - 8k][column]: lane l copies z = 8k + l % 8 of columns
-// l / 8, l / 8 + 4, ..., so a warp instruction reads 32-byte runs of 4 columns.
+// Chunk k (z = k*kColCh .. +kColCh-1) of the four fields of columns
+// col0 .. col0+31 into st[field][z - k*kColCh][column]: lane l copies
+// z = k*kColCh + l % kColCh of columns l / kColCh + j * (32 / kColCh), so a
+// warp instruction reads runs of kColCh floats of 32 / kColCh columns.
 __device__ __forceinline__ void col_stage_chunk(const TkeArgs& p, float* st, int64_t col0, int64_t ncol, int k,
                                                 int lane) {
   const int zz = lane & (kColCh - 1), z = k * kColCh + zz;
   if (z >= p.Z) return;
 #pragma unroll
-  for (int j = 0; j < 32 / 4; j++) {
-    const int c = j * 4 + (lane >> 3);
+  for (int j = 0; j < kColCh; j++) {
+    const int c = j * (32 / kColCh) + lane / kColCh;
     const int64_t col = col0 + c;
     if (col < ncol) {
       const int64_t g = col * p.Z + z;
@@ -314,8 +315,8 @@ __device__ __forceinline__ void col_stage_chunk(const TkeArgs& p, float* st, int
 }
 
 // Chunk k of the three fields the cells' update reads (dtketau from the
-// advection kernel, dtketaum1, tketaup1) into st[field][z - 8k][column], in
-// the pattern of col_stage_chunk.
+// advection kernel, dtketaum1, tketaup1) into st[field][z - k*kColCh][column],
+// in the pattern of col_stage_chunk.
 constexpr int kColUpdFloats = 3 * kColCh * kColPad;
 static_assert(2 * kColUpdFloats <= kColStages * kColStageFloats, "update stages reuse the forward stages");
 __device__ __forceinline__ void col_stage_update(const TkeArgs& p, float* st, int64_t col0, int64_t ncol, int k,
@@ -323,8 +324,8 @@ __device__ __forceinline__ void col_stage_update(const TkeArgs& p, float* st, in
   const int zz = lane & (kColCh - 1), z = k * kColCh + zz;
   if (z >= p.Z) return;
 #pragma unroll
-  for (int j = 0; j < 32 / 4; j++) {
-    const int c = j * 4 + (lane >> 3);
+  for (int j = 0; j < kColCh; j++) {
+    const int c = j * (32 / kColCh) + lane / kColCh;
     const int64_t col = col0 + c;
     if (col < ncol) {
       const int64_t g = col * p.Z + z;
@@ -359,7 +360,7 @@ __global__ void __launch_bounds__(kColWarps * 32, 3) tke_column_kernel(TkeArgs p
   float* q0 = p.q0 + col;
   float* q1 = p.q1 + col;
 
-  // Forward, a chunk of 8 z at a time: (A) the coefficients (tke.fut:103-210),
+  // Forward, a chunk of kColCh z at a time: (A) the coefficients (tke.fut:103-210),
   // independent across z; (B) tridagPar's recurrences 1 (the 4-tuple scan
   // for b', tridiag.fut:9-33) and 2 (y', :38-56) folded left to right --
   // recurrence 2 at z needs b' of z - 1 only; (C) the two quotients the
@@ -380,7 +381,7 @@ __global__ void __launch_bounds__(kColWarps * 32, 3) tke_column_kernel(TkeArgs p
     const float* nxt = st + ((k + 1) % kColStages) * kColStageFloats;
     const int zbase = k * kColCh;
     const int zn = min(kColCh, Z - zbase);
-    // the chunk's per-z constants, lane l holding those of z = zbase + l % 8
+    // the chunk's per-z constants, lane l holding those of z = zbase + l % kColCh
     float fac_l = 0.0f, dz_l = 1.0f;
     {
       const int zl = zbase + (lane & (kColCh - 1));
@@ -533,8 +534,8 @@ __global__ void __launch_bounds__(kColWarps * 32, 3) tke_column_kernel(TkeArgs p
     __syncwarp();
     const float* u = ust + (k & 1) * kColUpdFloats;
 #pragma unroll
-    for (int j = 0; j < 32 / 4; j++) {
-      const int c = j * 4 + (lane >> 3), zz = lane & (kColCh - 1);
+    for (int j = 0; j < kColCh; j++) {
+      const int c = j * (32 / kColCh) + lane / kColCh, zz = lane & (kColCh - 1);
       const int in_c = __shfl_sync(kAll, (int)inner, c);
       const int ks_c = __shfl_sync(kAll, ks, c);
       const int64_t cc = col0 + c;
