@@ -32,6 +32,8 @@ struct futhark_context {
   bool ok = false;
   void* scratch = nullptr;  // the entry point's scratch, grown on demand
   size_t scratch_bytes = 0;
+  cudaStream_t aux = nullptr;  // a second stream for work that overlaps `stream`'s,
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;  // forked and joined by these events
 };
 
 namespace {
@@ -155,6 +157,19 @@ int values_array(futhark_context* ctx, A* a, T* out) {
   return e == cudaSuccess ? 0 : cuda_fail(ctx, e, "device to host copy");
 }
 
+// Creates the context's auxiliary stream and its fork/join events on first
+// use (lock held, device set).
+bool ensure_aux_stream(futhark_context* ctx) {
+  if (ctx->aux) return true;
+  if (cudaStreamCreateWithFlags(&ctx->aux, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return true;
+}
+
 // Grows the context's scratch to at least `bytes` (lock held, device set).
 bool ensure_scratch(futhark_context* ctx, size_t bytes) {
   if (ctx->scratch_bytes >= bytes) return true;
@@ -219,6 +234,12 @@ void futhark_context_free(struct futhark_context* ctx) {
   if (ctx->ok) {
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
+    if (ctx->aux) {
+      cudaStreamSynchronize(ctx->aux);
+      cudaStreamDestroy(ctx->aux);
+      cudaEventDestroy(ctx->ev_fork);
+      cudaEventDestroy(ctx->ev_join);
+    }
     if (ctx->scratch) cudaFree(ctx->scratch);
     cudaStreamDestroy(ctx->stream);
   }

@@ -4,7 +4,11 @@
 // its own: the program's entry point is named futhark_entry_main like
 // LocVolCalib's.
 //
-// One step is two kernels on the context's stream:
+// One step is three kernels: tke_column_kernel on the context's stream and
+// tke_advect_kernel on an auxiliary stream run side by side (the first is
+// latency-bound, the second issue-bound, and they share no data), then
+// tke_ab_kernel applies the Adams-Bashforth update (:341-347) once both are
+// done.
 //   tke_advect_kernel  the advection fluxes east, north and top
 //                      (tke.fut:264-319) and dtketau (:320-340).  A thread
 //                      owns one (y, z) of the plane and marches along x over
@@ -18,10 +22,10 @@
 //                      (misc/ocean-sim/tridiag.fut:9-56) in one pass down the
 //                      column, the backward recurrence (:61-79), the water
 //                      mask, the surface correction, clip and lateral
-//                      diffusion of the top cell (:212-263), and the
-//                      Adams-Bashforth update (:341-347) with dtketau from the
-//                      first kernel.  The four fields the coefficients need
-//                      are staged through shared memory in chunks of 4 z
+//                      diffusion of the top cell (:212-263), giving tketaup1
+//                      before the Adams-Bashforth update.  The four fields
+//                      the coefficients need are staged through shared
+//                      memory in chunks of 4 z
 //                      (cp.async, three stages) as [z][column] tiles, so both
 //                      the coalesced copy and the lane-per-column reads are
 //                      free of bank conflicts; the forward pass leaves the two
@@ -151,7 +155,7 @@ __device__ __forceinline__ float adv_top(const TkeArgs& p, int x, int y, int z) 
 // ---------------------------------------------------------------------------
 // tke_advect_kernel
 // ---------------------------------------------------------------------------
-constexpr int kAdvThreads = 512;
+constexpr int kAdvThreads = 256;  // at <= 64 registers a CTA fits beside two column-kernel CTAs
 
 // Block b.x covers kAdvThreads consecutive (y, z) of the plane (z fastest),
 // block b.y the x segment [b.y * xseg, ...).  A thread keeps tketau and maskW
@@ -162,7 +166,7 @@ constexpr int kAdvThreads = 512;
 // north flux of (y - 1, z) is thread t - zdim's and the top flux of
 // (y, z - 1) thread t - 1's, again through shared memory; the first zdim
 // threads (resp. thread 0) evaluate that neighbour's flux themselves.
-__global__ void __launch_bounds__(kAdvThreads, 2) tke_advect_kernel(TkeArgs p, int xseg) {
+__global__ void __launch_bounds__(kAdvThreads, 4) tke_advect_kernel(TkeArgs p, int xseg) {
   __shared__ float sT[kAdvThreads], sW[kAdvThreads], sfn[kAdvThreads], sft[kAdvThreads];
   const int t = threadIdx.x;
   const int64_t plane = (int64_t)p.Y * p.Z;
@@ -314,10 +318,9 @@ __device__ __forceinline__ void col_stage_chunk(const TkeArgs& p, float* st, int
   }
 }
 
-// Chunk k of the three fields the cells' update reads (dtketau from the
-// advection kernel, dtketaum1, tketaup1) into st[field][z - k*kColCh][column],
-// in the pattern of col_stage_chunk.
-constexpr int kColUpdFloats = 3 * kColCh * kColPad;
+// Chunk k of tketaup1 -- what a cell keeps where the solution does not apply
+// -- into st[z - k*kColCh][column], in the pattern of col_stage_chunk.
+constexpr int kColUpdFloats = kColCh * kColPad;
 static_assert(2 * kColUpdFloats <= kColStages * kColStageFloats, "update stages reuse the forward stages");
 __device__ __forceinline__ void col_stage_update(const TkeArgs& p, float* st, int64_t col0, int64_t ncol, int k,
                                                  int lane) {
@@ -330,9 +333,7 @@ __device__ __forceinline__ void col_stage_update(const TkeArgs& p, float* st, in
     if (col < ncol) {
       const int64_t g = col * p.Z + z;
       float* d = st + zz * kColPad + c;
-      cp_async4(d, p.dtketau_out + g);
-      cp_async4(d + kColCh * kColPad, p.dtketaum1 + g);
-      cp_async4(d + 2 * kColCh * kColPad, p.tketaup1 + g);
+      cp_async4(d, p.tketaup1 + g);
     }
   }
 }
@@ -479,8 +480,9 @@ __global__ void __launch_bounds__(kColWarps * 32, 3) tke_column_kernel(TkeArgs p
   // Backward, a chunk at a time from the top: recurrence 3 down the column
   // into the tile, then the chunk's cells (coalesced): take the solution or
   // keep tketaup1 (:212-218), the top cell's correction, clip and lateral
-  // diffusion (:219-263), Adams-Bashforth (:341-347).  The next chunk's
-  // quotients (registers) and update fields (cp.async) load meanwhile.
+  // diffusion (:219-263) -- tketaup1 before the Adams-Bashforth update, which
+  // tke_ab_kernel applies once the advection kernel is done.  The next
+  // chunk's quotients (registers) and tketaup1 (cp.async) load meanwhile.
   float* ust = st;
   const float yn = inner ? q0[(int64_t)(Z - 1) * qs] : 0.0f;  // y'_{n-1} / b'_{n-1}
   r0 = 0.0f;
@@ -543,9 +545,7 @@ __global__ void __launch_bounds__(kColWarps * 32, 3) tke_column_kernel(TkeArgs p
         const int z = k * kColCh + zz;
         const bool take = in_c && (z == Z - 1 || (ks_c >= 0 && z >= ks_c));
         const float* uf = u + zz * kColPad + c;
-        const float tp = take ? tile[zz * kColPad + c] : uf[2 * kColCh * kColPad];
-        p.tketaup1_out[cc * Z + z] =
-            A_(tp, M_(kDtTracer, S_(M_(A_(1.5f, kABEps), uf[0]), M_(A_(0.5f, kABEps), uf[kColCh * kColPad]))));
+        p.tketaup1_out[cc * Z + z] = take ? tile[zz * kColPad + c] : uf[0];
       }
     }
     __syncwarp();  // the tile and this stage are rewritten two chunks on
@@ -555,6 +555,15 @@ __global__ void __launch_bounds__(kColWarps * 32, 3) tke_column_kernel(TkeArgs p
       qa1[zz] = qn1[zz];
     }
   }
+}
+
+// Adams-Bashforth (tke.fut:341-347) on the column kernel's tketaup1, with
+// dtketau from the advection kernel: both have finished when it runs.
+__global__ void __launch_bounds__(256) tke_ab_kernel(TkeArgs p) {
+  const int64_t n = (int64_t)p.X * p.Y * p.Z;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    p.tketaup1_out[i] = A_(p.tketaup1_out[i], M_(kDtTracer, S_(M_(A_(1.5f, kABEps), p.dtketau_out[i]),
+                                                               M_(A_(0.5f, kABEps), p.dtketaum1[i]))));
 }
 
 int64_t padded_columns(int64_t X, int64_t Y) { return (X * Y + 31) & ~int64_t(31); }
@@ -612,18 +621,14 @@ int step_launch(futhark_context* ctx, const tke_step_args* q) {
   p.dtketau_out = q->dtketau_out;
   p.tke_surf_corr_out = q->tke_surf_corr_out;
   cudaStream_t s = ctx->stream;
-  // advection and dtketau: x segments so that about four waves of CTAs run
-  const int64_t plane_blocks = (Y * Z + kAdvThreads - 1) / kAdvThreads;
-  const int64_t want_blocks = 4LL * 2 * ctx->num_sms;  // two CTAs per SM
-  const int64_t nseg = std::max<int64_t>(1, std::min<int64_t>(X, (want_blocks + plane_blocks - 1) / plane_blocks));
-  const int xseg = (int)((X + nseg - 1) / nseg);
-  const int64_t segs = (X + xseg - 1) / xseg;
-  if (plane_blocks > INT32_MAX || segs > 65535)
-    return set_error(ctx, FUTHARK_PROGRAM_ERROR, "tke step: plane too large");
-  tke_advect_kernel<<<dim3((unsigned)plane_blocks, (unsigned)segs), kAdvThreads, 0, s>>>(p, xseg);
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return cuda_fail(ctx, e, "tke advection launch");
-  // the columns: coefficients, tridagPar, tketaup1 (tke.fut:103-263, 341-347)
+  if (!ensure_aux_stream(ctx)) return set_error(ctx, FUTHARK_PROGRAM_ERROR, "tke step: cannot create a stream");
+  // The column kernel (latency-bound, a warp per 32 columns) on the context's
+  // stream and the advection kernel (issue-bound) on the auxiliary stream run
+  // side by side: they share no data until tke_ab_kernel.
+  cudaError_t e = cudaEventRecord(ctx->ev_fork, s);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->aux, ctx->ev_fork, 0);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "tke step fork");
+  // the columns: coefficients, tridagPar, tketaup1 (tke.fut:103-263)
   const int64_t col_blocks = (X * Y + 32 * kColWarps - 1) / (32 * kColWarps);
   if (col_blocks > INT32_MAX) return set_error(ctx, FUTHARK_PROGRAM_ERROR, "tke step: too many columns");
   e = cudaFuncSetAttribute((const void*)tke_column_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kColSmem);
@@ -631,6 +636,24 @@ int step_launch(futhark_context* ctx, const tke_step_args* q) {
   tke_column_kernel<<<(unsigned)col_blocks, 32 * kColWarps, kColSmem, s>>>(p);
   e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(ctx, e, "tke column launch");
+  // advection and dtketau: x segments so that about four waves of CTAs run
+  const int64_t plane_blocks = (Y * Z + kAdvThreads - 1) / kAdvThreads;
+  const int64_t want_blocks = 4LL * 4 * ctx->num_sms;  // four CTAs per SM
+  const int64_t nseg = std::max<int64_t>(1, std::min<int64_t>(X, (want_blocks + plane_blocks - 1) / plane_blocks));
+  const int xseg = (int)((X + nseg - 1) / nseg);
+  const int64_t segs = (X + xseg - 1) / xseg;
+  if (plane_blocks > INT32_MAX || segs > 65535)
+    return set_error(ctx, FUTHARK_PROGRAM_ERROR, "tke step: plane too large");
+  tke_advect_kernel<<<dim3((unsigned)plane_blocks, (unsigned)segs), kAdvThreads, 0, ctx->aux>>>(p, xseg);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "tke advection launch");
+  e = cudaEventRecord(ctx->ev_join, ctx->aux);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(s, ctx->ev_join, 0);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "tke step join");
+  // Adams-Bashforth (:341-347)
+  tke_ab_kernel<<<(unsigned)std::min<int64_t>((n + 255) / 256, 8LL * ctx->num_sms), 256, 0, s>>>(p);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "tke update launch");
   return 0;
 }
 
@@ -773,6 +796,6 @@ int tke_check(struct futhark_context* ctx) {
   return check_locked(ctx);
 }
 void* tke_context_stream(struct futhark_context* ctx) { return ctx && ctx->ok ? (void*)ctx->stream : nullptr; }
-int tke_launches_per_step(void) { return 2; }
+int tke_launches_per_step(void) { return 3; }
 
 }  // extern "C"
