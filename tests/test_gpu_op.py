@@ -142,3 +142,27 @@ def test_device_pointer_form_matches_entry(octx, op, oracle):
     octx.check()
     assert np.array_equal(out.cpu().numpy(), octx.main(*ins))
     assert close_to(out.cpu().numpy(), oracle.option_pricing(*ins), ORACLE_REL_TOL)
+
+
+@pytest.mark.parametrize("name", ["small", "medium", "large"])
+def test_device_form_guards_bridge_indices(octx, op, name):
+    # op_price_f32 leaves bb_inds' values to the caller; the kernels check
+    # them themselves and price NaN rather than read outside a path
+    import torch
+    ins, _ = load_op(name)
+    ins[1] = np.int32(1000)
+    bad = np.array(ins[9], copy=True)
+    bad[0, -1] = bad.shape[1] + 1  # a date past the path's end
+    ins[9] = bad
+    dims = op.dims_of(ins)
+    dev = {n: torch.from_numpy(np.ascontiguousarray(v)).cuda() for n, v in zip(op.ARRAY_NAMES, ins[2:])}
+    out = torch.zeros(dims["num_models"], dtype=torch.float32, device="cuda")
+    scratch = torch.empty(octx.scratch_bytes(int(ins[0]), int(ins[1]), dims), dtype=torch.uint8, device="cuda")
+    torch.cuda.synchronize()
+    octx.price(int(ins[0]), int(ins[1]), dims, {n: t.data_ptr() for n, t in dev.items()}, out.data_ptr(),
+               scratch.data_ptr())
+    octx.check()
+    assert np.isnan(out.cpu().numpy()).all()
+    good, _ = load_op(name)
+    good[1] = np.int32(1000)
+    assert np.isfinite(octx.main(*good)).all()
