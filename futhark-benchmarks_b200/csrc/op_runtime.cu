@@ -43,18 +43,18 @@ struct OpShape;
 // sized for (contract 2's 15-dimension paths want the registers of one)
 template <>
 struct OpShape<1> {
-  static constexpr int D = 1, U = 1, kMinCtas = 2;
+  static constexpr int D = 1, U = 1, kMinCtas = 4;
 };
 template <>
 struct OpShape<2> {
-  static constexpr int D = 5, U = 3, kMinCtas = 1;
+  static constexpr int D = 5, U = 3, kMinCtas = 3;
 };
 template <>
 struct OpShape<3> {  // priced by op_paths_warp_kernel
   static constexpr int D = 367, U = 3;
 };
 
-constexpr int kOpThreads = 256;
+constexpr int kOpThreads = 128;  // thread-per-path CTAs: contract 2 fits three per SM
 constexpr int kOpModels = 4;  // models priced per launch (accumulators in registers)
 
 struct OpDev {
@@ -534,15 +534,15 @@ __global__ void __launch_bounds__(kOpReduceThreads) op_reduce_kernel(const doubl
 
 constexpr size_t kWarpSmem3 = sizeof(float) * OpWarpSmem<3>::kWords;
 
-// CTAs of the paths kernel for `paths` paths of contract c: four 256-thread
-// CTAs per SM (thread per path), or two 8-warp CTAs per SM (warp per path,
+// CTAs of the paths kernel for `paths` paths of contract c: eight 128-thread
+// CTAs per SM (thread per path), or two 7-warp CTAs per SM (warp per path,
 // contract 3); fewer when there are fewer paths.
 int64_t op_ctas(const futhark_context* ctx, int c, int64_t paths) {
   const int64_t per = c == 3 ? kWarpPathWarps : kOpThreads;  // paths a CTA takes at once
-  const int64_t want = (int64_t)ctx->num_sms * (c == 3 ? 2 : 4);
+  const int64_t want = (int64_t)ctx->num_sms * (c == 3 ? 2 : 8);
   return std::max<int64_t>(1, std::min(want, (paths + per - 1) / per));
 }
-constexpr int kOpMaxCtasPerSm = 4;
+constexpr int kOpMaxCtasPerSm = 8;
 
 // Shapes and sizes of one pricing (lock held); the message names the failure.
 int op_validate(futhark_context* ctx, const op_args* q) {
