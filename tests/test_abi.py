@@ -75,6 +75,16 @@ def test_tke_context_without_gpu_reports_error(tke, pkg):
     assert ei.value.code == pkg.FUTHARK_PROGRAM_ERROR
 
 
+def test_op_context_without_gpu_reports_error(pkg):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    op = importlib.import_module("futhark-benchmarks_b200.op")
+    with pytest.raises(pkg.FutharkError) as ei:
+        op.OpContext()
+    assert ei.value.code == pkg.FUTHARK_PROGRAM_ERROR
+
+
 def test_tke_step_args_layout(tke):
     # struct tke_step_args: three int64 dimensions, then 27 pointers
     assert ctypes.sizeof(tke._StepArgs) == 3 * 8 + (len(tke.STEP_INPUTS) + len(tke.STEP_OUTPUTS) + 1) * 8
