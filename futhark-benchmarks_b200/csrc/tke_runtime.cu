@@ -155,7 +155,7 @@ __device__ __forceinline__ float adv_top(const TkeArgs& p, int x, int y, int z) 
 // ---------------------------------------------------------------------------
 // tke_advect_kernel
 // ---------------------------------------------------------------------------
-constexpr int kAdvThreads = 256;  // at <= 64 registers a CTA fits beside two column-kernel CTAs
+constexpr int kAdvThreads = 256;  // at <= 64 registers two CTAs fit beside two column-kernel CTAs
 
 // Block b.x covers kAdvThreads consecutive (y, z) of the plane (z fastest),
 // block b.y the x segment [b.y * xseg, ...).  A thread keeps tketau and maskW
@@ -339,7 +339,9 @@ __device__ __forceinline__ void col_stage_update(const TkeArgs& p, float* st, in
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
-__global__ void __launch_bounds__(kColWarps * 32, 3) tke_column_kernel(TkeArgs p) {
+// At most 128 registers (four CTAs' worth per SM): two CTAs then leave room
+// for two advection CTAs beside them.
+__global__ void __launch_bounds__(kColWarps * 32, 4) tke_column_kernel(TkeArgs p) {
   extern __shared__ float smem[];
   constexpr unsigned kAll = 0xffffffffu;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
