@@ -43,11 +43,12 @@ UNIT = "options/s"
 # implicit-X coefficients 12, tridiagonal X 10, combine 3, implicit-Y
 # coefficients 12, tridiagonal Y 10.
 F_ALG = 77
-# DRAM bytes (read + write) of the rollback launches of one run of the default
-# workload (uneven mix, 512 calibrations, seed 0, f64), from the ncu launch list
-# of `python bench.py --steps 2 --warmup 3 --no-plain --no-serving --cpu-seconds 3`
-# (dram__bytes_read.sum + dram__bytes_write.sum over the 13 plan runs / 13).
-ROLLBACK_DRAM_BYTES_DEFAULT = 382.956e9 / 13
+# DRAM bytes (read + write) per option-cell-step of the rollback launches, by
+# state precision, from an ncu capture of those launches (the profile named
+# beside each figure); bench.py scales it by the step's option-cell-steps.
+TRAFFIC_PER_CELL_STEP = {
+    "f64": (382.956e9 / 13 / 44624944128, "profiles/launches_bench_uneven.txt"),
+}
 CALIB_DEV_BYTES = 112  # sizeof(lvc::CalibDev) (static_assert in lvc_layout.h), uploaded per calibration per step
 
 
@@ -65,6 +66,9 @@ def parse():
                     help="time the plain per-call form on the first N calibrations (0 = all)")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--no-plain-configs", action="store_true",
+                    help="skip the plain form on the reference's three datasets")
+    ap.add_argument("--no-f32", action="store_true", help="skip the FP32-state section")
     ap.add_argument("--no-tridiag", action="store_true", help="skip the batched tridiagonal solver section")
     ap.add_argument("--no-tke", action="store_true", help="skip the ocean model's tke step section")
     ap.add_argument("--only-tke", action="store_true",
@@ -429,14 +433,15 @@ def run_op(args):
     import torch
     from oracle import oracle
     op = importlib.import_module("futhark-benchmarks_b200.op")
+    fd = importlib.import_module("futhark-benchmarks_b200.futhark_data")
     here = os.path.dirname(os.path.abspath(__file__))
     octx = op.OpContext()
     res = {"entry": "futhark_entry_main (libop.so)", "datasets": {}}
     try:
         for name in ("small", "medium", "large"):
-            z = np.load(os.path.join(here, "tests", "golden", f"optionpricing_{name}.npz"))
-            ins = [z[f"in{i:02d}"] for i in range(11)]
-            golden = z["out0"]
+            stem = os.path.join(here, "tests", "golden", "datasets", "finpar", "OptionPricing-data", name)
+            ins = fd.read_file(stem + ".in.gz")
+            golden = np.asarray(fd.read_file(stem + ".out.gz")[0])
             contract, paths = int(ins[0]), int(ins[1])
             dims = op.dims_of(ins)
             dev = {n: torch.from_numpy(np.ascontiguousarray(v)).cuda() for n, v in zip(op.ARRAY_NAMES, ins[2:])}
@@ -488,45 +493,199 @@ def run_op(args):
 
 
 def run_serving(pkg, wl, ctx, args, rank, precision):
-    """Poisson request streams through the serving runtime (continuous batching)."""
+    """Poisson request streams through the serving runtime (continuous batching).
+
+    First a saturating stream measures the capacity (requests/s); then the
+    configured rates and 50/80/95 % of that capacity.  Every request's solo
+    latency (submitted alone into an idle server) is measured too, so the
+    stream latencies can be read against a request's own compute time.  All
+    requests of the lowest rate are checked bit for bit against a batched run
+    of the same calibrations, and a sample against the FP64 oracle."""
     import numpy as np
-    out = []
     reqs = wl.uneven_mix(args.serving_requests, seed=1000 + args.seed + rank)
+
+    def stream(srv, rate, seed):
+        srv.reset_stats()
+        arrivals = wl.poisson_arrivals(rate, len(reqs), seed=seed)
+        t0 = time.perf_counter()
+        tickets = []
+        for c, ta in zip(reqs, arrivals):
+            dt = t0 + ta - time.perf_counter()
+            if dt > 0:
+                time.sleep(dt)
+            tickets.append(srv.submit(c))
+        res = [srv.result(t) for t in tickets]
+        st = srv.stats()
+        rec = {"rate_req_per_s": rate, "requests": len(reqs),
+               "throughput_options_per_s": st["throughput_options_per_s"],
+               "throughput_req_per_s": st["completed"] / st["span_s"] if st["span_s"] else None,
+               "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "max_ms": st["max_ms"],
+               "batches": st["batches"], "failed": st["failed"]}
+        return rec, res
+
+    out = []
     with pkg.Server(ctx, precision=precision) as srv:
-        # warm-up: kernels and pool
-        for t in [srv.submit(c) for c in reqs[:8]]:
+        for t in [srv.submit(c) for c in reqs[:8]]:  # warm-up: kernels and pool
             srv.result(t)
-        check = None
-        for rate in [float(r) for r in args.serving_rates.split(",") if r]:
-            srv.reset_stats()
-            arrivals = wl.poisson_arrivals(rate, len(reqs), seed=7 + int(rate))
+        # solo latency of every request (one at a time into an idle server)
+        solo = []
+        for c in reqs:
             t0 = time.perf_counter()
-            tickets = []
-            for c, ta in zip(reqs, arrivals):
-                dt = t0 + ta - time.perf_counter()
-                if dt > 0:
-                    time.sleep(dt)
-                tickets.append(srv.submit(c))
-            res = [srv.result(t) for t in tickets]
-            st = srv.stats()
-            out.append({"rate_req_per_s": rate, "requests": len(reqs),
-                        "throughput_options_per_s": st["throughput_options_per_s"],
-                        "throughput_req_per_s": st["completed"] / st["span_s"] if st["span_s"] else None,
-                        "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "max_ms": st["max_ms"],
-                        "batches": st["batches"], "failed": st["failed"]})
+            srv.result(srv.submit(c))
+            solo.append(1e3 * (time.perf_counter() - t0))
+        solo_p50 = float(np.median(solo))
+        sat, _ = stream(srv, 20000.0, seed=7 + 20000)
+        cap = sat["throughput_req_per_s"] or 1.0
+        rates = [float(r) for r in args.serving_rates.split(",") if r]
+        fracs = [0.5, 0.8, 0.95]
+        plan = sorted([(r, None) for r in rates] + [(f * cap, f) for f in fracs])
+        check = None
+        for rate, frac in plan:
+            rec, res = stream(srv, rate, seed=7 + int(rate))
+            rec["fraction_of_capacity"] = frac if frac is not None else rate / cap
+            rec["p50_over_solo_p50"] = rec["p50_ms"] / solo_p50 if solo_p50 else None
+            out.append(rec)
             if check is None:
                 check = res
-    # max relative error vs the FP64 oracle on the first few requests
+    # every request of the lowest rate: bit-identical to a batched run
+    batched = ctx.batch(reqs, precision=precision)
+    identical = bool(np.array_equal(np.concatenate(check), batched))
     err = None
-    if rank == 0 and check is not None and precision == pkg.F64:
+    if rank == 0 and precision == pkg.F64:
         from oracle import oracle
-        k = 3
-        ref = oracle.batch_f64(reqs[:k])
-        got = np.concatenate(check[:k])
+        idx = list(range(0, len(reqs), max(1, len(reqs) // 12)))[:12]
+        ref = oracle.batch_f64([reqs[i] for i in idx])
+        got = np.concatenate([check[i] for i in idx])
         err = float(np.max(np.abs(got - ref) / np.abs(ref)))
-    return {"sweep": out, "max_rel_err_vs_fp64_oracle": err,
-            "oracle_sample": "first 3 requests of the stream",
+    return {"capacity_req_per_s": cap, "capacity_options_per_s": sat["throughput_options_per_s"],
+            "saturating_stream": sat, "sweep": out,
+            "solo_latency_ms": {"p50": solo_p50, "p99": float(np.percentile(solo, 99)),
+                                "what": "each request submitted alone into an idle server"},
+            "lowest_rate_bit_identical_to_batched": identical,
+            "lowest_rate_requests_checked": len(check),
+            "max_rel_err_vs_fp64_oracle": err,
+            "oracle_sample": "12 requests of the lowest-rate stream, evenly spaced",
             "workload": f"{len(reqs)} requests per rate drawn as the uneven mix (seed 1000+rank)"}
+
+
+def run_plain_configs(pkg, wl, ctx, args, fp64_peak):
+    """The plain per-call form on the reference's three datasets
+    (finpar/LocVolCalib-data/{small,medium,large}.in) at f64: device time of a
+    run (the one-calibration plan, CUDA events), end to end through
+    futhark_entry_main_f64 (prices copied to host), the FP64 roofline, the CPU
+    baseline (the oracle on all host threads and on one, median of 5 runs over
+    a sample of the strikes) and the error against the oracle on the strikes it
+    priced."""
+    import numpy as np
+    from oracle import oracle
+    threads = oracle.max_threads()
+    # strikes per one-thread sample: about half a second of oracle time each
+    one_thread_strikes = {"small": 4, "medium": 16, "large": 2}
+    res = {}
+    for name in ("small", "medium", "large"):
+        c = wl.DATASETS[name]
+        a9 = (c.outer, c.numX, c.numY, c.numT, c.s0, c.t, c.alpha, c.nu, c.beta)
+        got = ctx.main_f64(*a9)  # builds and keeps the entry point's plan
+        e2e = []
+        for _ in range(5):
+            t0 = time.perf_counter()
+            ctx.main_f64(*a9)
+            e2e.append(time.perf_counter() - t0)
+        plan = ctx.plan([c])
+        plan.run()
+        ms_run = plan.time(5)
+        classes = plan.classes()
+        roll_ms = sum(x["ms"] for x in classes)
+        plan.free()
+        work = c.work()
+        achieved = F_ALG * work / (ms_run * 1e-3) / 1e12
+
+        def cpu(k, nthreads):
+            ts = []
+            ref = None
+            for _ in range(5):
+                t0 = time.perf_counter()
+                ref = oracle.main_f64(k, *a9[1:], threads=nthreads)
+                ts.append(time.perf_counter() - t0)
+            return k / statistics.median(ts), ref
+
+        k1 = one_thread_strikes[name]
+        v1, ref1 = cpu(k1, 1)
+        kn = min(c.outer, k1 * threads)
+        vn, refn = cpu(kn, threads)
+        rel = np.abs(got[:kn] - refn) / np.abs(refn)
+        res[name] = {
+            "shape": {"outer": c.outer, "numX": c.numX, "numY": c.numY, "numT": c.numT},
+            "option_cell_steps": work,
+            "device_ms": ms_run, "value": c.outer / (ms_run * 1e-3), "unit": UNIT,
+            "rollback_ms": roll_ms, "classes": classes,
+            "e2e_ms": 1e3 * statistics.median(e2e), "e2e_value": c.outer / statistics.median(e2e),
+            "e2e_path": "futhark_entry_main_f64 + futhark_values_f64_1d (prices to host)",
+            "roofline": {"bound": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
+                         "frac": achieved / fp64_peak, "flops_per_unit": F_ALG,
+                         "timing": "whole run (setup + pivot + rollback) with CUDA events"},
+            "cpu_baseline": {"all_threads": {"value": vn, "cores": threads, "strikes": kn},
+                             "one_thread": {"value": v1, "cores": 1, "strikes": k1},
+                             "unit": UNIT, "kind": "port",
+                             "sample": "the first strikes of the dataset, f64 oracle, median of 5 runs"},
+            "max_rel_err_vs_fp64_oracle": float(rel.max()),
+            "oracle_strikes_checked": kn,
+        }
+    return res
+
+
+def run_f32_state(pkg, wl, ctx, calibs, args, ref, sample):
+    """The FP32-state variant: the uneven mix (device-resident and end to end)
+    and the large dataset, each with its error against the FP64 oracle."""
+    import numpy as np
+    from oracle import oracle
+    F32 = pkg.F32_STATE
+    plan = ctx.plan(calibs, precision=F32)
+    ext = torch_stream(ctx)
+    import torch
+    for _ in range(max(3, args.warmup)):
+        plan.run()
+    ctx.sync()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(ext)
+    for _ in range(args.steps):
+        plan.run()
+    e1.record(ext)
+    ctx.sync()
+    ms = e0.elapsed_time(e1) / args.steps
+    n_opts = wl.total_options(calibs)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        plan.set_params(calibs)
+        plan.run()
+        prices = plan.prices()
+    e2e = n_opts * args.steps / (time.perf_counter() - t0)
+    plan.free()
+    mix_err = error_vs_oracle(prices, ref, sample)
+    big = wl.LARGE
+    lp = ctx.plan([big], precision=F32)
+    lp.run()
+    lms = lp.time(3)
+    lprices = lp.prices()
+    lp.free()
+    idx = list(range(0, big.outer, 16))
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=oracle.max_threads()) as ex:
+        lref = np.array(list(ex.map(lambda i: oracle.value_f64(big.numX, big.numY, big.numT, big.s0, 0.001 * i,
+                                                                big.t, big.alpha, big.nu, big.beta), idx)))
+    lrel = np.abs(lprices[idx] - lref) / np.abs(lref)
+    return {"mix": {"value": n_opts / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms, "e2e_value": e2e,
+                    "error_vs_fp64_oracle": mix_err},
+            "large": {"value": big.outer / (lms * 1e-3), "unit": UNIT, "device_ms": lms,
+                      "max_rel_err_vs_fp64_oracle": float(lrel.max()), "oracle_strikes_checked": len(idx)},
+            "contract": "1e-4 relative on prices above 1e-3 of their calibration's largest, 1e-7 absolute below"}
+
+
+def torch_stream(ctx):
+    import torch
+    return torch.cuda.ExternalStream(ctx.stream)
 
 
 def run_ours(args):
@@ -570,7 +729,9 @@ def run_ours(args):
                                          if e.us_per_step_default > 0
                                          and e.us_per_step_best < e.us_per_step_default * 0.999],
                 "plan_params": plan_params}
+    t0 = time.perf_counter()
     plan = ctx.plan(calibs, precision=precision)
+    plan_build_s = time.perf_counter() - t0
     ext = torch.cuda.ExternalStream(ctx.stream, device=f"cuda:{local}")
     n_opts = wl.total_options(calibs)
     work = wl.total_work(calibs)
@@ -594,11 +755,13 @@ def run_ours(args):
     ms = ev0.elapsed_time(ev1)
     clk = clocks.stop()
     value, ms_max = job_throughput(ms, n_opts, args.steps, world, dev)
+    ms_step = ms / args.steps
 
-    # ---- the rollback kernel alone (events around each rollback launch) ----
+    # ---- the rollback launch classes one after another (events around each) ----
     plan.time(max(1, args.steps))
-    roll_ms = plan.rollback_ms
-    achieved = F_ALG * work / (roll_ms * 1e-3) / 1e12
+    classes = plan.classes()
+    for c in classes:
+        c["g_cell_steps_per_s"] = c["cell_steps"] / (c["ms"] * 1e-3) / 1e9 if c["ms"] else None
 
     # ---- end to end through the C ABI with host buffers ----
     for _ in range(1):
@@ -615,10 +778,21 @@ def run_ours(args):
     torch.cuda.synchronize()
     e2e_s = max_over_ranks(time.perf_counter() - t0)
     e2e = sum_over_ranks(n_opts) * args.steps / e2e_s
-    # one-shot batched call (plan build + run + copy + free), once
+    # one-shot batched call, its parts timed apart: plan build (tables and
+    # pivot arenas allocated, work lists, graph capture), run, copy, free
     t0 = time.perf_counter()
-    ctx.batch(calibs, precision=precision)
-    oneshot = n_opts / (time.perf_counter() - t0)
+    one = ctx.plan(calibs, precision=precision)
+    t1 = time.perf_counter()
+    one.run()
+    ctx.sync()
+    t2 = time.perf_counter()
+    one.prices()
+    t3 = time.perf_counter()
+    one.free()
+    t4 = time.perf_counter()
+    oneshot = {"value": n_opts / (t4 - t0), "build_s": t1 - t0, "run_s": t2 - t1, "copy_s": t3 - t2,
+               "free_s": t4 - t3, "first_plan_build_s": plan_build_s,
+               "what": "plan build + run + copy + free of the whole workload, once (lvc_batch's steps)"}
 
     # ---- plain per-call form on the same workload ----
     plain = None
@@ -634,6 +808,10 @@ def run_ours(args):
         dt = time.perf_counter() - t0
         plain = {"value": sum(c.outer for c in sub) / dt, "unit": UNIT,
                  "calls": len(sub), "form": "futhark_entry_main_f64 once per calibration"}
+
+    plain_cfg = None
+    if not args.no_plain_configs and rank == 0:
+        plain_cfg = run_plain_configs(pkg, wl, ctx, args, fp64_peak)
 
     tridiag = None
     if not args.no_tridiag and rank == 0:
@@ -651,17 +829,33 @@ def run_ours(args):
     if not args.no_serving:
         serving = run_serving(pkg, wl, ctx, args, rank, precision)
 
-    cpu = err = None
+    cpu = err = f32 = None
     if rank == 0 and world == 1:
         cpu, ref, sample = cpu_baseline(calibs, args.cpu_seconds)
         err = error_vs_oracle(prices, ref, sample)
+        if precision == pkg.F64 and not args.no_f32:
+            f32 = run_f32_state(pkg, wl, ctx, calibs, args, ref, sample)
 
-    default_workload = (args.workload == "uneven" and args.calibs == 512 and args.seed == 0
-                        and args.precision == "f64")
-    traffic = ROLLBACK_DRAM_BYTES_DEFAULT if default_workload else None
-    traffic_src = ("ncu launch list of the default workload: DRAM bytes of the rollback launches per step "
-                   "(the per-step pivot rows come from L2; the grids stay in shared memory)"
-                   if default_workload else "not measured for this workload")
+    # roofline: all option-cell-steps of a step at F_ALG FP64 flops over the
+    # wall time of the step (the launch classes overlap on several streams),
+    # and the dominant kernel's launches timed one after another
+    achieved = F_ALG * work / (ms_step * 1e-3) / 1e12
+    by_kernel = {}
+    for c in classes:
+        key = f"{c['family']}, {c['threads']} threads"
+        k = by_kernel.setdefault(key, {"kernel": key, "launches": 0, "cell_steps": 0, "ms": 0.0, "clusters": []})
+        k["launches"] += 1
+        k["cell_steps"] += c["cell_steps"]
+        k["ms"] += c["ms"]
+        k["clusters"].append(c["cluster"])
+    serial_ms = sum(c["ms"] for c in classes)
+    dom = max(by_kernel.values(), key=lambda k: k["ms"]) if by_kernel else None
+    if dom:
+        dom["achieved"] = F_ALG * dom["cell_steps"] / (dom["ms"] * 1e-3) / 1e12
+        dom["frac"] = dom["achieved"] / fp64_peak
+        dom["share_of_serial_rollback_time"] = dom["ms"] / serial_ms if serial_ms else None
+    tr = TRAFFIC_PER_CELL_STEP.get(args.precision)
+    traffic = tr[0] * work if tr else None
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -673,20 +867,31 @@ def run_ours(args):
                            option_cell_steps_per_rank=work,
                            l2="inputs larger than L2: the per-step pivot tables of the mix exceed 126 MB"),
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": CALIB_DEV_BYTES * len(calibs),
-                    "d2h_bytes_per_step": 8 * n_opts, "oneshot_value": oneshot,
-                    "path": "lvc_plan_set_params + lvc_plan_run + lvc_plan_copy_prices"},
+                    "d2h_bytes_per_step": 8 * n_opts,
+                    "path": "lvc_plan_set_params + lvc_plan_run + lvc_plan_copy_prices",
+                    "oneshot": oneshot},
             "gpu_launches": args.steps * plan.num_launches,
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
                          "frac": achieved / fp64_peak, "traffic": traffic,
-                         "traffic_source": traffic_src,
-                         "kernel": "rollback launches (lvc_line_pair_kernel for numX % 64 == 0, "
-                                   "lvc_line_full_kernel for numX == 32), summed per step",
+                         "traffic_source": (f"{tr[0]:.3f} DRAM bytes per option-cell-step of the rollback "
+                                            f"launches ({tr[1]}) x the step's option-cell-steps") if tr else
+                                           "not measured for this precision",
+                         "timing": "the whole step (wall time between CUDA events on the plan's stream)",
+                         "kernel": "all rollback launches of the step (lvc_line_pair_kernel dominates)",
                          "flops_per_unit": F_ALG, "unit_of_work": "option-cell-step",
-                         "units_per_step": work, "kernel_ms_per_step": roll_ms,
+                         "units_per_step": work,
                          "peak_source": "measured live: lvc_probe_dfma_kernel on this GPU "
                                         "(MEASURED_PEAKS.json has no FP64 figure)",
-                         "smem_peak_gbs": smem_peak},
+                         "smem_peak_gbs": smem_peak,
+                         "dominant_kernel": dom,
+                         "serial_rollback_ms_per_step": serial_ms,
+                         "serial_timing": "launch classes timed one after another on one stream "
+                                          "(CUDA events around each launch); their sum exceeds the "
+                                          "step time because the step overlaps them on several streams"},
+            "launch_classes": classes,
             "plain_per_call": plain,
+            "plain_configs": plain_cfg,
+            "f32_state": f32,
             "serving": serving,
             "tridiag": tridiag,
             "tke": tke_res,

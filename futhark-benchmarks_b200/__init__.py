@@ -85,6 +85,16 @@ class Shape(ctypes.Structure):
         return (self.family, self.cluster, self.hbm_state)
 
 
+class LaunchInfo(ctypes.Structure):
+    """struct lvc_launch_info: one rollback launch class of a plan."""
+    _fields_ = [("family", ctypes.c_int32), ("cluster", ctypes.c_int32), ("threads", ctypes.c_int32),
+                ("items", ctypes.c_int32), ("cell_steps", ctypes.c_int64), ("ms", ctypes.c_double)]
+
+    def as_dict(self) -> dict:
+        return {"family": Shape.FAMILIES.get(self.family, "?"), "cluster": self.cluster,
+                "threads": self.threads, "items": self.items, "cell_steps": self.cell_steps, "ms": self.ms}
+
+
 class TuningEntry(ctypes.Structure):
     """struct lvc_tuning_entry."""
     _fields_ = [("numX", ctypes.c_int32), ("numY", ctypes.c_int32), ("precision", ctypes.c_int32),
@@ -163,6 +173,8 @@ def load_library(path: str = LIB_PATH):
         "lvc_plan_time": (ctypes.c_int, [vp, vp, i32, ctypes.POINTER(f64)]),
         "lvc_plan_rollback_ms": (f64, [vp]),
         "lvc_plan_num_launches": (i32, [vp]),
+        "lvc_plan_num_classes": (i32, [vp]),
+        "lvc_plan_launch_info": (ctypes.c_int, [vp, i32, ctypes.POINTER(LaunchInfo)]),
         "lvc_batch": (ctypes.c_int, [vp, ctypes.POINTER(_Calib), i32, i32, vp]),
         "lvc_context_stream": (vp, [vp]),
         "futhark_new_f32_2d": (vp, [vp, vp, i64, i64]),
@@ -175,6 +187,7 @@ def load_library(path: str = LIB_PATH):
         "futhark_entry_tridagNestedSeqConst": (ctypes.c_int, [vp, ctypes.POINTER(vp), vp, vp, vp, vp]),
         "lvc_tridag_f32": (ctypes.c_int, [vp, i32, i64, i64, vp, vp, vp, vp, vp]),
         "lvc_tridag_check": (ctypes.c_int, [vp]),
+        "lvc_wait_selftest": (ctypes.c_int, [vp, i32, i32]),
         "lvc_probe_peaks": (ctypes.c_int, [vp, ctypes.POINTER(f64), ctypes.POINTER(f64)]),
         "lvc_server_new": (ctypes.c_int, [vp, ctypes.POINTER(_ServerConfig), ctypes.POINTER(vp)]),
         "lvc_server_submit": (ctypes.c_int, [vp, ctypes.POINTER(_Calib), ctypes.POINTER(ctypes.c_uint64)]),
@@ -347,6 +360,11 @@ class Context:
         """Raises if a device-pointer solve since the last check had a copy time out."""
         self._check(self.lib.lvc_tridag_check(self._ctx))
 
+    def wait_selftest(self, polls: int, arrive: bool):
+        """lvc_wait_selftest: a bounded device wait that runs out (arrive=False)
+        raises FutharkError; one that completes returns quietly."""
+        self._check(self.lib.lvc_wait_selftest(self._ctx, polls, int(bool(arrive))))
+
     @property
     def stream(self) -> int:
         return self.lib.lvc_context_stream(self._ctx) or 0
@@ -440,6 +458,16 @@ class Plan:
     @property
     def num_launches(self) -> int:
         return int(self.ctx.lib.lvc_plan_num_launches(self._p))
+
+    def classes(self) -> list:
+        """The plan's rollback launch classes (largest work first), with their
+        device times from the last time() call."""
+        out = []
+        for i in range(int(self.ctx.lib.lvc_plan_num_classes(self._p))):
+            li = LaunchInfo()
+            if self.ctx.lib.lvc_plan_launch_info(self._p, i, ctypes.byref(li)) == 0:
+                out.append(li.as_dict())
+        return out
 
     @property
     def device_prices(self) -> int:

@@ -213,6 +213,8 @@ struct Launch {
   int64_t gstate_per_cta;  // elements of the state type
   int64_t gstate_off;      // elements
   double sm_per_cta = 1.0; // SMs one CTA of this launch occupies at full residency
+  int64_t work = 0;        // option-cell-steps of the launch's items
+  double ms = 0.0;         // device time in the last lvc_plan_time (mean per run)
 };
 
 }  // namespace
@@ -783,6 +785,7 @@ int plan_build(futhark_context* ctx, const lvc_calibration* cs, int n, lvc_plan*
       work += e.first;
     }
     class_work.push_back(work);
+    L.work = work;
     if (L.n_items > 0) {
       if (int rc = prepare_launch<S, PV>(ctx, L, P->max_sms)) return rc;
       P->sms = std::max(P->sms, std::min<double>(L.grid * L.sm_per_cta, ctx->num_sms));
@@ -894,6 +897,7 @@ int check_device_error(futhark_context* ctx, lvc_plan* P) {
   int h = 0;
   LVC_CUDA(ctx, cudaMemcpyAsync(&h, P->d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
   LVC_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if (h == 3) return set_error(ctx, FUTHARK_PROGRAM_ERROR, "rollback kernel: a bounded wait for a bulk copy timed out");
   if (h) return set_error(ctx, FUTHARK_PROGRAM_ERROR, "rollback kernel rejected a work item");
   return 0;
 }
@@ -1279,6 +1283,7 @@ int lvc_plan_time(struct futhark_context* ctx, struct lvc_plan* plan, int32_t it
   std::vector<cudaEvent_t> ev(2 * plan->launches.size());
   for (auto& x : ev) LVC_CUDA(ctx, cudaEventCreate(&x));
   double roll = 0.0;
+  for (Launch& L : plan->launches) L.ms = 0.0;
   for (int i = 0; i < iters; i++) {
     cudaError_t e = plan_enqueue(plan, ctx->stream, ev.data());
     if (e != cudaSuccess) return cuda_fail(ctx, e, "plan_enqueue");
@@ -1288,6 +1293,7 @@ int lvc_plan_time(struct futhark_context* ctx, struct lvc_plan* plan, int32_t it
       float t = 0.f;
       LVC_CUDA(ctx, cudaEventElapsedTime(&t, ev[2 * l], ev[2 * l + 1]));
       roll += t;
+      plan->launches[l].ms += t / iters;
     }
   }
   plan->rollback_ms = roll / iters;
@@ -1298,6 +1304,25 @@ int lvc_plan_time(struct futhark_context* ctx, struct lvc_plan* plan, int32_t it
 }
 
 double lvc_plan_rollback_ms(const struct lvc_plan* plan) { return plan ? plan->rollback_ms : 0.0; }
+
+int32_t lvc_plan_num_classes(const struct lvc_plan* plan) { return plan ? (int32_t)plan->launches.size() : 0; }
+
+int lvc_plan_launch_info(const struct lvc_plan* plan, int32_t i, struct lvc_launch_info* out) {
+  if (!plan || !out || i < 0 || i >= (int32_t)plan->launches.size()) return -1;
+  const Launch& L = plan->launches[i];
+  Config c{};
+  c.kind = L.kind;
+  c.full = L.full;
+  c.pair = L.pair;
+  c.upw = L.upw;
+  out->family = family_of(c);
+  out->cluster = L.C;
+  out->threads = L.NT;
+  out->items = L.n_items;
+  out->cell_steps = L.work;
+  out->ms = L.ms;
+  return 0;
+}
 
 int lvc_batch(struct futhark_context* ctx, const struct lvc_calibration* calibs, int32_t n,
               int32_t precision, double* prices) {
@@ -1892,6 +1917,7 @@ extern "C" int lvc_entry_main_f64_noalloc(struct futhark_context* ctx, double* p
   int h = 0;
   LVC_CUDA(ctx, cudaMemcpyAsync(&h, d_err, sizeof(int), cudaMemcpyDeviceToHost, s));
   LVC_CUDA(ctx, cudaStreamSynchronize(s));
+  if (h == 3) return set_error(ctx, FUTHARK_PROGRAM_ERROR, "rollback kernel: a bounded wait for a bulk copy timed out");
   if (h) return set_error(ctx, FUTHARK_PROGRAM_ERROR, "rollback kernel rejected a work item");
   return 0;
 }
@@ -2502,6 +2528,16 @@ int lvc_tridag_check(struct futhark_context* ctx) {
   std::lock_guard<std::mutex> g(ctx->mu);
   if (!ctx->ok) return set_error(ctx, FUTHARK_PROGRAM_ERROR, "context has no usable CUDA device");
   LVC_CUDA(ctx, cudaSetDevice(ctx->device));
+  return tridag_check_locked(ctx);
+}
+
+int lvc_wait_selftest(struct futhark_context* ctx, int32_t polls, int32_t arrive) {
+  std::lock_guard<std::mutex> g(ctx->mu);
+  if (!ctx->ok) return set_error(ctx, FUTHARK_PROGRAM_ERROR, "context has no usable CUDA device");
+  if (polls < 1 || polls > kWaitPolls) return set_error(ctx, FUTHARK_PROGRAM_ERROR, "polls out of range");
+  LVC_CUDA(ctx, cudaSetDevice(ctx->device));
+  lvc_wait_selftest_kernel<<<1, 32, 0, ctx->stream>>>(polls, arrive);
+  LVC_CUDA(ctx, cudaGetLastError());
   return tridag_check_locked(ctx);
 }
 

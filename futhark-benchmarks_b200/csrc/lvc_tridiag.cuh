@@ -35,6 +35,25 @@ __device__ int lvc_tridag_err;
 
 constexpr int kTriThreads = 128;  // threads (systems) per CTA of lvc_tridag_kernel
 
+// Self-test of the bounded wait: one warp waits on a fresh mbarrier for at
+// most `polls` polls.  With arrive == 0 nothing ever completes its phase (no
+// copy targets it and no thread arrives), so the wait runs out and the kernel
+// raises lvc_tridag_err exactly as a solve whose bulk copy never landed
+// does; with arrive != 0 lane 0 arrives first and the wait succeeds.  No
+// asynchronous operation is in flight either way, so the CTA may exit at once.
+__global__ void lvc_wait_selftest_kernel(int polls, int arrive) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncwarp();
+  if (arrive && threadIdx.x == 0)
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(&bar)) : "memory");
+  const bool ok = mbar_wait(&bar, 0, polls);
+  if (!ok && threadIdx.x == 0) atomicExch(&lvc_tridag_err, 1);
+}
+
 __device__ __forceinline__ float tri_mul(float a, float b) { return __fmul_rn(a, b); }
 __device__ __forceinline__ float tri_add(float a, float b) { return __fadd_rn(a, b); }
 __device__ __forceinline__ float tri_sub(float a, float b) { return __fsub_rn(a, b); }

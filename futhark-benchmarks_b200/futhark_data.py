@@ -184,6 +184,11 @@ def read_values(data: bytes | str) -> List[np.ndarray]:
 
 
 def read_file(path: str) -> List[np.ndarray]:
+    """Values of a dataset file; a name ending in ``.gz`` is gunzipped first."""
+    if path.endswith(".gz"):
+        import gzip
+        with gzip.open(path, "rb") as f:
+            return read_values(f.read())
     with open(path, "rb") as f:
         return read_values(f.read())
 

@@ -163,6 +163,22 @@ LVC_API int lvc_plan_time(struct futhark_context *ctx, struct lvc_plan *plan, in
 LVC_API double lvc_plan_rollback_ms(const struct lvc_plan *plan);
 /* Number of kernel launches one lvc_plan_run performs. */
 LVC_API int32_t lvc_plan_num_launches(const struct lvc_plan *plan);
+/* One rollback launch class of a plan (no counterpart in the reference): the
+ * kernel shape its instances share, their count and option-cell-steps, and
+ * the class's device time in the last lvc_plan_time (mean per run, the
+ * classes timed one after another on one stream). */
+struct lvc_launch_info {
+  int32_t family;     /* LVC_FAMILY_* */
+  int32_t cluster;    /* CTAs per strike instance */
+  int32_t threads;    /* threads per CTA */
+  int32_t items;      /* strike instances */
+  int64_t cell_steps; /* sum of numX * numY * (numT - 1) over the instances */
+  double ms;          /* 0 before the first lvc_plan_time */
+};
+/* Number of rollback launch classes of a plan. */
+LVC_API int32_t lvc_plan_num_classes(const struct lvc_plan *plan);
+/* Class i (0 .. lvc_plan_num_classes - 1, largest work first); -1 when out of range. */
+LVC_API int lvc_plan_launch_info(const struct lvc_plan *plan, int32_t i, struct lvc_launch_info *out);
 
 /* One-shot batched call from host memory: plan, run, copy back, free. */
 LVC_API int lvc_batch(struct futhark_context *ctx, const struct lvc_calibration *calibs, int32_t n,

@@ -66,6 +66,14 @@ LVC_API int lvc_tridag_f32(struct futhark_context *ctx, int32_t form, int64_t ro
  * solve since the last check whose input copy timed out -- its systems were
  * written as NaN.  The entry points check on every call. */
 LVC_API int lvc_tridag_check(struct futhark_context *ctx);
+/* Self-test of the kernels' bounded waits (no counterpart in the reference):
+ * one warp waits at most `polls` polls (1 .. 2^22) on a fresh mbarrier that
+ * nothing completes (arrive == 0) or that it completes itself first
+ * (arrive != 0).  A wait that runs out raises the same device flag as a solve
+ * whose copy never landed, so this returns what lvc_tridag_check reports:
+ * FUTHARK_PROGRAM_ERROR ("... timed out") for arrive == 0, 0 otherwise.  The
+ * context stays usable either way. */
+LVC_API int lvc_wait_selftest(struct futhark_context *ctx, int32_t polls, int32_t arrive);
 
 #ifdef __cplusplus
 }

@@ -5,7 +5,7 @@ import os
 import numpy as np
 import pytest
 
-from conftest import GOLDEN
+from conftest import GOLDEN, golden_npz
 
 fd = importlib.import_module("futhark-benchmarks_b200.futhark_data")
 
@@ -63,7 +63,7 @@ def test_text_roundtrip():
 
 
 def test_tridiag_fixture_shapes():
-    z = np.load(os.path.join(GOLDEN, "tridiag32_small.npz"))
+    z = golden_npz("tridiag32_small")
     for k in "abcyx":
         assert z[k].shape == (100, 115) and z[k].dtype == np.float32
 

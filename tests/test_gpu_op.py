@@ -9,7 +9,7 @@ import os
 import numpy as np
 import pytest
 
-from conftest import GOLDEN
+from conftest import GOLDEN, golden_npz
 
 pytestmark = pytest.mark.gpu
 
@@ -18,7 +18,7 @@ ORACLE_REL_TOL = 1e-6
 
 
 def load_op(name):
-    z = np.load(os.path.join(GOLDEN, f"optionpricing_{name}.npz"))
+    z = golden_npz(f"optionpricing_{name}")
     return [z[f"in{i:02d}"] for i in range(11)], z["out0"]
 
 

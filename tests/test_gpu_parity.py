@@ -9,6 +9,7 @@ finpar/LocVolCalib.fut line by line):
     golden files are f32 results carrying up to 2.8e-6 of their own error).
 """
 import importlib
+import os
 
 import numpy as np
 import pytest
@@ -30,11 +31,26 @@ def rel_err(got, exp):
 
 
 def oracle_for(oracle, c, strikes=None):
-    """f64 oracle prices of calibration c (optionally only some strike indices)."""
+    """f64 oracle prices of calibration c (optionally only some strike indices,
+    priced on all host threads)."""
     if strikes is None:
         return oracle.main_f64(*[getattr(c, k) for k in FIELDS])
-    return np.array([oracle.value_f64(c.numX, c.numY, c.numT, c.s0, 0.001 * i, c.t, c.alpha, c.nu, c.beta)
-                     for i in strikes])
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=max(1, os.cpu_count() or 1)) as ex:
+        return np.array(list(ex.map(
+            lambda i: oracle.value_f64(c.numX, c.numY, c.numT, c.s0, 0.001 * i, c.t, c.alpha, c.nu, c.beta),
+            strikes)))
+
+
+def check_f32_state(got, exp):
+    """The FP32-state contract: 1e-4 relative on every price above 1e-3 of the
+    calibration's largest, 1e-7 absolute below; returns the max relative error
+    over the significant prices."""
+    big = np.abs(exp) > 1e-3 * np.max(np.abs(exp))
+    err = rel_err(got[big], exp[big])
+    assert err <= F32S_RTOL
+    assert np.max(np.abs(got[~big] - exp[~big]), initial=0.0) <= 1e-7
+    return err
 
 
 @pytest.mark.parametrize("name", ["small", "medium"])
@@ -92,6 +108,50 @@ def test_f32_state_error_vs_oracle(ctx, oracle):
         big = np.abs(e) > 1e-3 * np.max(np.abs(e))
         assert rel_err(g[big], e[big]) <= F32S_RTOL
         assert np.max(np.abs(g[~big] - e[~big]), initial=0.0) <= 1e-7
+
+
+def test_f32_state_large_config(ctx, oracle):
+    # the large dataset's shape (256 x 256 x 64, a cluster per strike) in FP32
+    # state; the oracle prices every eighth strike
+    c = wl.LARGE
+    got = ctx.batch([c], precision=1)
+    idx = np.arange(0, 256, 8)
+    check_f32_state(got[idx], oracle_for(oracle, c, idx))
+
+
+def test_f32_state_long_time_line(ctx, oracle):
+    # 255 steps on 256-sized grids, where the f32 drift is largest
+    for X, Y in ((256, 256), (256, 64), (64, 256)):
+        c = wl.Calibration(12, X, Y, 256, 0.041, 9.5, 0.27, 0.75, 0.65)
+        got = ctx.batch([c], precision=1)
+        check_f32_state(got, oracle.main_f64(*[getattr(c, k) for k in FIELDS]))
+
+
+def mix_slice(n_big=3, n_rand=8):
+    """Calibrations of the benchmark's own mix (512 from seed 0): its n_big
+    largest by work and n_rand more at random."""
+    mix = wl.uneven_mix(512, seed=0)
+    order = sorted(range(len(mix)), key=lambda i: -mix[i].work())
+    rng = np.random.default_rng(1)
+    pick = order[:n_big] + list(rng.choice(order[n_big:], size=n_rand, replace=False))
+    return [mix[i] for i in sorted(pick)]
+
+
+def test_benchmark_mix_slice_f64(ctx, oracle):
+    calibs = mix_slice()
+    assert max(c.numT for c in calibs) > 200 and max(c.numX * c.numY for c in calibs) == 65536
+    got = ctx.batch(calibs)
+    exp = oracle.batch_f64(calibs)
+    assert rel_err(got, exp) <= F64_RTOL
+
+
+def test_benchmark_mix_slice_f32_state(ctx, oracle):
+    calibs = mix_slice(2, 5)
+    got = ctx.batch(calibs, precision=1)
+    exp = oracle.batch_f64(calibs)
+    offs = np.concatenate([[0], np.cumsum([c.outer for c in calibs])])
+    for i in range(len(calibs)):
+        check_f32_state(got[offs[i]:offs[i + 1]], exp[offs[i]:offs[i + 1]])
 
 
 def test_alone_equals_in_mix(ctx):

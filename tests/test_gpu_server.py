@@ -80,3 +80,27 @@ def test_server_rejects_invalid_request(ctx, pkg):
             srv.submit(wl.Calibration(4, 2, 16, 8, 0.03, 5.0, 0.2, 0.6, 0.5))
         ok = srv.result(srv.submit(wl.Calibration(2, 32, 32, 6, 0.03, 5.0, 0.2, 0.6, 0.5)))
         assert ok.shape == (2,)
+
+
+def test_server_poisson_stream_every_request_vs_oracle(ctx, pkg, oracle):
+    # a Poisson stream drawn as the uneven mix (short time lines so that the
+    # oracle stays cheap), submitted at its arrival times: every request's
+    # prices within 1e-9 of the FP64 oracle and bit-identical to a batched run
+    reqs = wl.uneven_mix(60, seed=77, numT=(8, 40))
+    arrivals = wl.poisson_arrivals(2000.0, len(reqs), seed=78)
+    with pkg.Server(ctx) as srv:
+        t0 = time.perf_counter()
+        tickets = []
+        for c, ta in zip(reqs, arrivals):
+            dt = t0 + ta - time.perf_counter()
+            if dt > 0:
+                time.sleep(dt)
+            tickets.append(srv.submit(c))
+        got = [srv.result(t) for t in tickets]
+        st = srv.stats()
+    assert st["completed"] == len(reqs) and st["failed"] == 0
+    ref = oracle.batch_f64(reqs)
+    batched = ctx.batch(reqs)
+    flat = np.concatenate(got)
+    assert np.array_equal(flat, batched)
+    assert np.max(np.abs(flat - ref) / np.abs(ref)) <= 1e-9

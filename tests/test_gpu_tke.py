@@ -8,7 +8,7 @@ import os
 import numpy as np
 import pytest
 
-from conftest import GOLDEN
+from conftest import GOLDEN, golden_npz
 
 pytestmark = pytest.mark.gpu
 
@@ -31,7 +31,7 @@ def tctx(tke):
 
 def test_golden_bit_exact(tctx, tke):
     # misc/ocean-sim/data/tke32-small.{in,out}: [20][20][10]
-    z = np.load(os.path.join(GOLDEN, "tke32_small.npz"))
+    z = golden_npz("tke32_small")
     outs = tctx.main(*[z[f"in{i:02d}"] for i in range(25)])
     for k, name in enumerate(tke.OUTPUT_NAMES):
         assert same_bits(outs[k], z[f"out{k}"]), name

@@ -14,7 +14,7 @@ import os
 import numpy as np
 import pytest
 
-from conftest import GOLDEN
+from conftest import GOLDEN, golden_npz
 
 pytestmark = pytest.mark.gpu
 
@@ -23,7 +23,7 @@ wl = importlib.import_module("futhark-benchmarks_b200.workloads")
 
 @pytest.fixture(scope="module")
 def golden_tridiag():
-    return np.load(os.path.join(GOLDEN, "tridiag32_small.npz"))
+    return golden_npz("tridiag32_small")
 
 
 @pytest.mark.parametrize("const", [False, True])
@@ -102,3 +102,18 @@ def test_device_pointer_form_with_unaligned_arrays(ctx, oracle):
         ctx.tridag_check()
         got = out[1:].cpu().numpy().reshape(rows, m)
         assert np.array_equal(got, oracle.tridag(*host, form=oform))
+
+
+def test_bounded_wait_runs_out_safely(ctx, pkg):
+    # a device wait on a barrier nothing completes gives up after its poll
+    # limit and reports the timeout through the error flag the solvers use;
+    # the context stays usable
+    with pytest.raises(pkg.FutharkError) as ei:
+        ctx.wait_selftest(64, arrive=False)
+    assert ei.value.code == pkg.FUTHARK_PROGRAM_ERROR and "timed out" in str(ei.value)
+    ctx.wait_selftest(1 << 20, arrive=True)  # completes: no error, and the flag was cleared
+    ctx.tridag_check()
+    z = golden_npz("tridiag32_small")
+    assert np.array_equal(ctx.tridag(z["a"], z["b"], z["c"], z["y"], form="seq"), z["x"])
+    with pytest.raises(pkg.FutharkError):
+        ctx.wait_selftest(0, arrive=True)  # poll limit out of range

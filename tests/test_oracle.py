@@ -14,7 +14,7 @@ import os
 import numpy as np
 import pytest
 
-from conftest import GOLDEN, dataset_args
+from conftest import GOLDEN, dataset_args, golden_npz
 
 GOLDEN_ABS_TOL = 5e-6
 
@@ -47,14 +47,14 @@ def test_oracle_large_matches_reference_outputs(oracle, golden):
 
 
 def test_tridag_seq_reproduces_golden_bit_exact(oracle):
-    z = np.load(os.path.join(GOLDEN, "tridiag32_small.npz"))
+    z = golden_npz("tridiag32_small")
     x = oracle.tridag(z["a"], z["b"], z["c"], z["y"], form="seq")
     assert x.dtype == np.float32
     assert np.array_equal(x, z["x"])
 
 
 def test_tridag_scan_form_agrees_with_thomas_f64(oracle):
-    z = np.load(os.path.join(GOLDEN, "tridiag32_small.npz"))
+    z = golden_npz("tridiag32_small")
     a, b, c, y = (z[k].astype(np.float64) for k in "abcy")
     xp = oracle.tridag(a, b, c, y, form="par")
     xs = oracle.tridag(a, b, c, y, form="seq")
@@ -117,7 +117,7 @@ def test_tridag_par4_agrees_with_thomas_f64(oracle):
     # solution as tridagSeq in exact arithmetic: at f64 on the reference's own
     # test inputs the two agree to ~4e-11 (the f32 runs differ by up to 6e-2
     # on the worst element of these ill-conditioned random systems, median 2e-6)
-    z = np.load(os.path.join(GOLDEN, "tridiag32_small.npz"))
+    z = golden_npz("tridiag32_small")
     a, b, c, y = (z[k].astype(np.float64) for k in "abcy")
     xs = oracle.tridag(a, b, c, y, form="seq")
     for form in ("par", "par4"):
@@ -128,14 +128,14 @@ def test_tridag_par4_agrees_with_thomas_f64(oracle):
 def test_tke_reproduces_golden_bit_exact(oracle):
     # misc/ocean-sim/tke.fut's entry main restated in f32 with the reference's
     # operand order: all seven outputs equal tke32-small.out bit for bit
-    z = np.load(os.path.join(GOLDEN, "tke32_small.npz"))
+    z = golden_npz("tke32_small")
     got = oracle.tke(*[z[f"in{i:02d}"] for i in range(25)])
     for i, g in enumerate(got):
         assert np.array_equal(g, z[f"out{i}"]), i
 
 
 def load_op(name):
-    z = np.load(os.path.join(GOLDEN, f"optionpricing_{name}.npz"))
+    z = golden_npz(f"optionpricing_{name}")
     return [z[f"in{i:02d}"] for i in range(11)], z["out0"]
 
 
