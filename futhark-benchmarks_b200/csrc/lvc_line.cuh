@@ -106,6 +106,56 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, int li
   return false;
 }
 
+// ---- pushes to another CTA of the cluster (distributed shared memory) ----
+// The address of `p` (a shared-memory location of this CTA) in the shared
+// window of cluster rank `rank`: every CTA of a launch has the same layout,
+// so the same offset names the same buffer there.
+__device__ __forceinline__ unsigned cluster_addr(const void* p, int rank) {
+  unsigned r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;\n" : "=r"(r) : "r"(smem_u32(p)), "r"(rank));
+  return r;
+}
+// st.async: stores into a remote CTA's shared memory and counts the bytes on
+// that CTA's mbarrier (complete_tx, release at cluster scope), so the
+// receiver learns of the data by its own barrier -- no cluster barrier.
+__device__ __forceinline__ void st_async(unsigned dst, double v, unsigned bar) {
+  asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.b64 [%0], %1, [%2];\n" ::"r"(dst),
+               "l"(__double_as_longlong(v)), "r"(bar)
+               : "memory");
+}
+__device__ __forceinline__ void st_async(unsigned dst, float v, unsigned bar) {
+  asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.b32 [%0], %1, [%2];\n" ::"r"(dst),
+               "r"(__float_as_uint(v)), "r"(bar)
+               : "memory");
+}
+__device__ __forceinline__ void st_async2(unsigned dst, double a, double b, unsigned bar) {
+  asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.v2.b64 [%0], {%1, %2}, [%3];\n" ::"r"(dst),
+               "l"(__double_as_longlong(a)), "l"(__double_as_longlong(b)), "r"(bar)
+               : "memory");
+}
+__device__ __forceinline__ void st_async2(unsigned dst, float a, float b, unsigned bar) {
+  asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.v2.b32 [%0], {%1, %2}, [%3];\n" ::"r"(dst),
+               "r"(__float_as_uint(a)), "r"(__float_as_uint(b)), "r"(bar)
+               : "memory");
+}
+// Wait for a barrier that remote st.async pushes complete: acquire at cluster
+// scope, so the pushed data are visible after it.  Bounded like mbar_wait.
+__device__ __forceinline__ bool mbar_try_wait_cluster(uint64_t* bar, unsigned parity) {
+  unsigned done;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(done)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+__device__ __forceinline__ bool mbar_wait_cluster(uint64_t* bar, unsigned parity, int limit = kWaitPolls) {
+  for (int i = 0; i < limit; i++)
+    if (mbar_try_wait_cluster(bar, parity)) return true;
+  return false;
+}
+
 template <typename S, typename PV, int NT>
 __global__ void __launch_bounds__(NT, (NT >= 512 ? 1 : 512 / NT)) lvc_line_kernel(RollbackArgs<S, PV> args) {
   constexpr int K = kLineK;

@@ -32,12 +32,15 @@ namespace lvc {
 
 struct PairLayout {
   int LD, Ycs, CHx, Ux, CG2, CHy, Uy;
-  int bar, A, B, w0, w1, w2, grow, gx, ex, tab0, tab1, xf, xb, yf, yb, blkF, blkB, zin, xin, tot, total;
+  int bar, barF, barB, barH, A, B, w0, w1, w2, grow, gx, ex, tab0, tab1, xf, xb, yf, yb, inF, totF, inB, totB,
+      zin, xin, total;
 };
 
-// Byte offsets of the shared-memory buffers.
+// Byte offsets of the shared-memory buffers of a CTA holding Ycs rows of an
+// X-column grid split over a cluster of C CTAs.  The four mbarriers sit at
+// fixed offsets (initialised once per launch, whatever the items).
 template <typename S>
-LVC_HD PairLayout pair_layout(int X, int Ycs, int upw) {
+LVC_HD PairLayout pair_layout(int X, int Ycs, int upw, int C) {
   PairLayout L;
   auto up = [](int n) { return (n + 15) / 16 * 16; };
   const int s = (int)sizeof(S);
@@ -49,7 +52,10 @@ LVC_HD PairLayout pair_layout(int X, int Ycs, int upw) {
   L.CHy = Ycs / kLineK;
   L.Uy = L.CG2 * L.CHy;       // Y units: 1 per warp
   int o = 0;
-  L.bar = o; o += 16;
+  L.bar = o; o += 8;   // bulk copies of the step's pivots and table
+  L.barF = o; o += 8;  // cluster: forward chunk maps of the lower ranks have landed
+  L.barB = o; o += 8;  // cluster: backward chunk maps of the higher ranks have landed
+  L.barH = o; o += 8;  // cluster: the neighbours' halo rows have landed
   L.A = o; o += up((Ycs + 2) * L.LD * s);  // rows -1 .. Ycs (halo rows at both ends)
   L.B = o; o += up(Ycs * L.LD * s);
   L.w0 = o; o += up(X * s);               // W_k(i), planar
@@ -60,24 +66,22 @@ LVC_HD PairLayout pair_layout(int X, int Ycs, int upw) {
   L.ex = o; o += up(Ycs * s);              // [Ycs] e_j of the current step, planar
   L.tab0 = o; o += up(8 * Ycs * 8);
   L.tab1 = o; o += up(8 * Ycs * 8);
-  L.xf = o; o += up(L.Ux * 64 * s);        // [unit][lane] (a, b) of the forward chunk maps
-  L.xb = o; o += up(L.Ux * 64 * s);        // the same, backward
+  L.xf = o; o += up(L.Ux / upw * 64 * s);  // [warp][lane] (a, b) of the warps' forward chunk maps
+  L.xb = o; o += up(L.Ux / upw * 64 * s);  // the same, backward
   L.yf = o; o += up(L.Uy * 32 * upw * s);
   L.yb = o; o += up(L.Uy * 32 * upw * s);
-  L.blkF = o; o += up(X * s);
-  L.blkB = o; o += up(X * s);
+  // cluster: the chunk maps every other rank pushes here, [rank][column],
+  // and the rank's multiplier product (column-independent), [rank]
+  const int Cc = C > 1 ? C : 0;
+  L.inF = o; o += up(Cc * X * s);
+  L.totF = o; o += up(Cc * s);
+  L.inB = o; o += up(Cc * X * s);
+  L.totB = o; o += up(Cc * s);
   L.zin = o; o += up(X * s);
   L.xin = o; o += up(X * s);
-  L.tot = o; o += up(4 * s);
   L.total = o;
   return L;
 }
-
-// cluster ranks whose block maps are loaded at once (f64; f32 state, whose
-// registers are capped at 128, folds one rank at a time)
-template <typename S> struct FoldBatch {
-  static constexpr int v = sizeof(S) == 8 ? 4 : 1;
-};
 
 template <typename S> struct P2;
 template <> struct P2<double> {
@@ -127,8 +131,8 @@ __global__ void __launch_bounds__(NT, (PairMinBlocks<S, NT, UPW>::v)) lvc_line_p
   static_assert(UPW == 1 || UPW == 2, "one or two units per warp");
   static_assert(sizeof(S) == sizeof(PV), "pivots are copied verbatim into the state buffer");
   static_assert(K % 2 == 0, "columns are walked in pairs");
-  constexpr int FB = FoldBatch<S>::v;
   using V = P2<S>;
+  constexpr int FB = 2;  // warp maps loaded at once in the X folds
   extern __shared__ __align__(16) unsigned char smem[];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int C = args.C;
@@ -137,9 +141,16 @@ __global__ void __launch_bounds__(NT, (PairMinBlocks<S, NT, UPW>::v)) lvc_line_p
   if (clustered) rank = (int)cg::this_cluster().block_rank();
   const int cid = blockIdx.x / C, ncl = gridDim.x / C;
   unsigned sc = 0, phase = 0;
+  unsigned phF = 0, phB = 0, phH = 0;  // parities of the cluster barriers (one completion per use)
   uint64_t* bar = reinterpret_cast<uint64_t*>(smem);
+  uint64_t* barF = bar + 1;
+  uint64_t* barB = bar + 2;
+  uint64_t* barH = bar + 3;
   if (tid == 0) {
     mbar_init(bar, 1);
+    mbar_init(barF, 1);
+    mbar_init(barB, 1);
+    mbar_init(barH, 1);
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
   __syncthreads();
@@ -150,10 +161,10 @@ __global__ void __launch_bounds__(NT, (PairMinBlocks<S, NT, UPW>::v)) lvc_line_p
     const int X = c.numX, Y = c.numY, T = c.numT;
     const int Ycs = c.Ycs;
     const int r0 = rank * Ycs;
-    const PairLayout Ls = pair_layout<S>(X, Ycs, UPW);
+    const PairLayout Ls = pair_layout<S>(X, Ycs, UPW, C);
     // uniform over the cluster (every CTA of a cluster sees the same item)
     if (c.kind != kKindLine || c.C != C || c.ld != Ls.LD || Ls.total > args.smem_elems * (int)sizeof(S) ||
-        Ls.Ux != NU || Ls.Uy != NW || (X % UW) || (Ycs % 32) || Ycs * C != Y) {
+        Ls.Ux != NU || Ls.Uy != NW || (X % UW) || (Ls.CHx % UPW) || (Ycs % 32) || Ycs * C != Y) {
       if (tid == 0) atomicExch(args.err, 5);
       continue;
     }
@@ -172,24 +183,26 @@ __global__ void __launch_bounds__(NT, (PairMinBlocks<S, NT, UPW>::v)) lvc_line_p
     S* xb = reinterpret_cast<S*>(smem + Ls.xb);
     S* yf = reinterpret_cast<S*>(smem + Ls.yf);
     S* yb = reinterpret_cast<S*>(smem + Ls.yb);
-    S* blkF = reinterpret_cast<S*>(smem + Ls.blkF);
-    S* blkB = reinterpret_cast<S*>(smem + Ls.blkB);
+    S* inF = reinterpret_cast<S*>(smem + Ls.inF);
+    S* totF = reinterpret_cast<S*>(smem + Ls.totF);
+    S* inB = reinterpret_cast<S*>(smem + Ls.inB);
+    S* totB = reinterpret_cast<S*>(smem + Ls.totB);
     S* s_zin = reinterpret_cast<S*>(smem + Ls.zin);
     S* s_xin = reinterpret_cast<S*>(smem + Ls.xin);
-    S* s_tot = reinterpret_cast<S*>(smem + Ls.tot);
     const double* tabc = args.tabs + c.tab;
     const TabLayout Lt = tab_layout(X, Y, T, c.Xp, kKindLine);
     const double strike = 0.001 * (double)item.strike;  // strikes (:247)
     const int steps = T > 1 ? T - 1 : 0;
     const PV* piv = args.piv + c.piv;
     const int64_t Y4 = round4(Y);
-    S* halo_prev = nullptr;  // bottom halo row of rank - 1
-    S* halo_next = nullptr;  // top halo row of rank + 1
-    if (clustered) {
-      cg::cluster_group cl = cg::this_cluster();
-      if (rank > 0) halo_prev = cl.map_shared_rank(A + (Ycs + 1) * LD, rank - 1);
-      if (rank < C - 1) halo_next = cl.map_shared_rank(A, rank + 1);
-    }
+    // Cluster pushes (st.async into the other ranks' shared memory, counted
+    // on their barriers): this rank's halo rows go to the bottom halo row of
+    // rank - 1 and the top halo row of rank + 1; its forward chunk maps to
+    // every higher rank, its backward ones to every lower rank, at slot `rank`.
+    const bool has_prev = clustered && rank > 0, has_next = clustered && rank < C - 1;
+    const unsigned halo_bytes = (unsigned)((has_prev + has_next) * X * (int)sizeof(S));
+    const unsigned fold_bytes_F = (unsigned)(rank * (X + 1) * (int)sizeof(S));
+    const unsigned fold_bytes_B = clustered ? (unsigned)((C - 1 - rank) * (X + 1) * (int)sizeof(S)) : 0u;
 
     // The previous instance is done with every buffer, and -- across the
     // cluster -- every neighbour has finished pushing its last halo rows into
@@ -244,8 +257,12 @@ __global__ void __launch_bounds__(NT, (PairMinBlocks<S, NT, UPW>::v)) lvc_line_p
       chx[q] = u - rgx[q] * Ls.CHx;
       jl[q] = rgx[q] * 32 + lane;
     }
-    // the two units of a warp fold their chunk prefixes in one pass
-    const bool xchain = UPW == 2 && rgx[UPW - 1] == rgx[0] && chx[UPW - 1] > chx[0];
+    // A warp's units are consecutive chunks of one row group (numX / 16 is a
+    // multiple of UPW), so the warp composes their chunk maps in registers and
+    // publishes one map per warp; a warp then folds the maps of the warps
+    // before it (forward) or after it (backward) in its row group.
+    const int WPG = Ls.CHx / UPW;           // warps per row group
+    const int wg0 = (warp / WPG) * WPG;     // first warp of this warp's row group
     // Y unit u = warp: columns cgy*UW + UPW*lane (+ h < UPW), rows chy*16 ..
     const int cgy = warp / Ls.CHy, chy = warp - cgy * Ls.CHy;
     const int col0 = cgy * UW + UPW * lane;
@@ -272,17 +289,24 @@ __global__ void __launch_bounds__(NT, (PairMinBlocks<S, NT, UPW>::v)) lvc_line_p
       // sweep; its last readers were the previous step's passes 1 and 2)
       for (int j = tid; j < Ycs; j += NT) sE[j] = (S)tb[j * 8 + kSlotE];
       // Cluster: the neighbours' halo rows of the previous step have landed
-      // (they arrived after pushing them; the arrive/wait pair is split so its
-      // latency overlaps the bulk-copy wait above).  Step 0 reads only the
-      // halo rows this CTA initialised itself.
-      if (clustered && s > 0) asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
+      // (pushed by st.async, counted on barH).  Step 0 reads only the halo
+      // rows this CTA initialised itself.
+      if (clustered && s > 0) {
+        if (tid == 0) mbar_expect_tx(barH, halo_bytes);
+        if (!mbar_wait_cluster(barH, phH, timed_out ? kWaitPollsAfterTimeout : kWaitPolls)) {
+          timed_out = true;
+          atomicExch(args.err, 3);
+        }
+        phH ^= 1u;
+      }
       __syncthreads();
       const S dt = (S)tabc[Lt.dtinv + k];
 
       // -------- X sweep pass 1: explicitX + explicitY, forward recurrence (chunk-local) --------
       S z[UPW][K], PQ[UPW][K];
+      S zl[UPW], Pl[UPW];  // each unit's forward chunk map: z_end = zl + Pl * z_in
       {
-        S e[UPW], g0[UPW], g1[UPW], g2[UPW], Rl[UPW], rbp[UPW], zl[UPW], Pl[UPW];
+        S e[UPW], g0[UPW], g1[UPW], g2[UPW], Rl[UPW], rbp[UPW];
         typename V::T Rc[UPW];
 #pragma unroll
         for (int q = 0; q < UPW; q++) {
@@ -336,35 +360,32 @@ __global__ void __launch_bounds__(NT, (PairMinBlocks<S, NT, UPW>::v)) lvc_line_p
             Rc[q] = Rn;
           }
         }
-#pragma unroll
-        for (int q = 0; q < UPW; q++) {
-          const int u = UPW * warp + q;
-          V::st(xf + (u * 32 + lane) * 2, zl[q], Pl[q]);
-        }
+        // the warp's map (unit 1 after unit 0)
+        if constexpr (UPW == 2)
+          V::st(xf + (warp * 32 + lane) * 2, zl[1] + Pl[1] * zl[0], Pl[1] * Pl[0]);
+        else
+          V::st(xf + (warp * 32 + lane) * 2, zl[0], Pl[0]);
       }
       __syncthreads();
       // -------- pass 2: forward fix-up, backward recurrence (chunk-local) --------
+      S xl[UPW], Ql[UPW];  // each unit's backward chunk map: x_start = xl + Ql * x_in
       {
-        S zin[UPW], xl[UPW], Ql[UPW], e[UPW];
+        S zin[UPW], e[UPW];
         {
           S a = 0;
-          int c2 = 0;
-          for (; c2 < chx[0]; c2++) {
-            const auto f = V::ld(xf + ((rgx[0] * Ls.CHx + c2) * 32 + lane) * 2);
-            a = f.x + f.y * a;
+          // the maps of the warps before this one, in order; loads in batches
+          // of FB so that their latencies overlap
+          for (int w0 = wg0; w0 < warp; w0 += FB) {
+            typename V::T f[FB];
+#pragma unroll
+            for (int t = 0; t < FB; t++)
+              if (w0 + t < warp) f[t] = V::ld(xf + ((w0 + t) * 32 + lane) * 2);
+#pragma unroll
+            for (int t = 0; t < FB; t++)
+              if (w0 + t < warp) a = f[t].x + f[t].y * a;
           }
           zin[0] = a;
-          if constexpr (UPW == 2) {
-            if (!xchain) {
-              a = 0;
-              c2 = 0;
-            }
-            for (; c2 < chx[UPW - 1]; c2++) {
-              const auto f = V::ld(xf + ((rgx[UPW - 1] * Ls.CHx + c2) * 32 + lane) * 2);
-              a = f.x + f.y * a;
-            }
-            zin[UPW - 1] = a;
-          }
+          if constexpr (UPW == 2) zin[1] = zl[0] + Pl[0] * a;
         }
 #pragma unroll
         for (int q = 0; q < UPW; q++) {
@@ -397,11 +418,11 @@ __global__ void __launch_bounds__(NT, (PairMinBlocks<S, NT, UPW>::v)) lvc_line_p
             }
           }
         }
-#pragma unroll
-        for (int q = 0; q < UPW; q++) {
-          const int u = UPW * warp + q;
-          V::st(xb + (u * 32 + lane) * 2, xl[q], Ql[q]);
-        }
+        // the warp's backward map (unit 0 before unit 1)
+        if constexpr (UPW == 2)
+          V::st(xb + (warp * 32 + lane) * 2, xl[0] + Ql[0] * xl[1], Ql[0] * Ql[1]);
+        else
+          V::st(xb + (warp * 32 + lane) * 2, xl[0], Ql[0]);
       }
       __syncthreads();
       // -------- pass 3: backward fix-up; dtInv * u goes to B (:205) --------
@@ -409,23 +430,19 @@ __global__ void __launch_bounds__(NT, (PairMinBlocks<S, NT, UPW>::v)) lvc_line_p
         S xin[UPW];
         {
           S a = 0;
-          int c2 = Ls.CHx - 1;
-          if constexpr (UPW == 2) {
-            for (; c2 > chx[UPW - 1]; c2--) {
-              const auto f = V::ld(xb + ((rgx[UPW - 1] * Ls.CHx + c2) * 32 + lane) * 2);
-              a = f.x + f.y * a;
-            }
-            xin[UPW - 1] = a;
-            if (!xchain) {
-              a = 0;
-              c2 = Ls.CHx - 1;
-            }
+          // the maps of the warps after this one, from the last one down
+          const int wl = wg0 + WPG - 1;
+          for (int w0 = wl; w0 > warp; w0 -= FB) {
+            typename V::T f[FB];
+#pragma unroll
+            for (int t = 0; t < FB; t++)
+              if (w0 - t > warp) f[t] = V::ld(xb + ((w0 - t) * 32 + lane) * 2);
+#pragma unroll
+            for (int t = 0; t < FB; t++)
+              if (w0 - t > warp) a = f[t].x + f[t].y * a;
           }
-          for (; c2 > chx[0]; c2--) {
-            const auto f = V::ld(xb + ((rgx[0] * Ls.CHx + c2) * 32 + lane) * 2);
-            a = f.x + f.y * a;
-          }
-          xin[0] = a;
+          xin[UPW - 1] = a;
+          if constexpr (UPW == 2) xin[0] = xl[1] + Ql[1] * a;
         }
 #pragma unroll
         for (int p = 0; p < K / 2; p++) {
@@ -471,38 +488,30 @@ __global__ void __launch_bounds__(NT, (PairMinBlocks<S, NT, UPW>::v)) lvc_line_p
       __syncthreads();
       if (s + 1 < steps) issue_copies(k - 1, ((sc + 1) & 1) ? sT1 : sT0);
       if (clustered) {
+        // this rank's forward block map of each column, pushed to every
+        // higher rank; then the lower ranks' maps, folded in rank order
         for (int col = tid; col < X; col += NT) {
           const int g = col / UW, w = col - g * UW;
           S a = 0;
           for (int c2 = 0; c2 < Ls.CHy; c2++)
             a = yf[(g * Ls.CHy + c2) * UW + w] + (S)tb[(c2 * K + K - 1) * 8 + kSlotCP] * a;
-          blkF[col] = a;
+          for (int h = rank + 1; h < C; h++)
+            st_async(cluster_addr(inF + rank * X + col, h), a, cluster_addr(barF, h));
         }
         if (tid == 0) {
           S b = 1;
           for (int c2 = 0; c2 < Ls.CHy; c2++) b = (S)tb[(c2 * K + K - 1) * 8 + kSlotCP] * b;
-          s_tot[0] = b;
+          for (int h = rank + 1; h < C; h++) st_async(cluster_addr(totF + rank, h), b, cluster_addr(barF, h));
+          mbar_expect_tx(barF, fold_bytes_F);
         }
-        cg::cluster_group cl = cg::this_cluster();
-        cl.sync();
-        // fold of the lower ranks' block maps, in rank order; the remote
-        // loads of a batch are independent, so they overlap (one distributed
-        // shared-memory round trip per batch instead of one per rank)
+        if (!mbar_wait_cluster(barF, phF, timed_out ? kWaitPollsAfterTimeout : kWaitPolls)) {
+          timed_out = true;
+          atomicExch(args.err, 3);
+        }
+        phF ^= 1u;
         for (int col = tid; col < X; col += NT) {
           S zv = 0;
-          for (int rb0 = 0; rb0 < rank; rb0 += FB) {
-            S f[FB], t[FB];
-#pragma unroll
-            for (int q = 0; q < FB; q++) {
-              if (rb0 + q < rank) {
-                f[q] = cl.map_shared_rank(blkF, rb0 + q)[col];
-                t[q] = cl.map_shared_rank(s_tot, rb0 + q)[0];
-              }
-            }
-#pragma unroll
-            for (int q = 0; q < FB; q++)
-              if (rb0 + q < rank) zv = f[q] + t[q] * zv;
-          }
+          for (int q = 0; q < rank; q++) zv = inF[q * X + col] + totF[q] * zv;
           s_zin[col] = zv;
         }
         __syncthreads();
@@ -538,35 +547,30 @@ __global__ void __launch_bounds__(NT, (PairMinBlocks<S, NT, UPW>::v)) lvc_line_p
       }
       __syncthreads();
       if (clustered) {
+        // the same for the backward maps: pushed to every lower rank, the
+        // higher ranks' folded from the top rank down
         for (int col = tid; col < X; col += NT) {
           const int g = col / UW, w = col - g * UW;
           S a = 0;
           for (int c2 = Ls.CHy - 1; c2 >= 0; c2--)
             a = yb[(g * Ls.CHy + c2) * UW + w] + (S)tb[(c2 * K) * 8 + kSlotCQ] * a;
-          blkB[col] = a;
+          for (int h = 0; h < rank; h++)
+            st_async(cluster_addr(inB + rank * X + col, h), a, cluster_addr(barB, h));
         }
         if (tid == 0) {
           S b = 1;
           for (int c2 = Ls.CHy - 1; c2 >= 0; c2--) b = (S)tb[(c2 * K) * 8 + kSlotCQ] * b;
-          s_tot[1] = b;
+          for (int h = 0; h < rank; h++) st_async(cluster_addr(totB + rank, h), b, cluster_addr(barB, h));
+          mbar_expect_tx(barB, fold_bytes_B);
         }
-        cg::cluster_group cl = cg::this_cluster();
-        cl.sync();
+        if (!mbar_wait_cluster(barB, phB, timed_out ? kWaitPollsAfterTimeout : kWaitPolls)) {
+          timed_out = true;
+          atomicExch(args.err, 3);
+        }
+        phB ^= 1u;
         for (int col = tid; col < X; col += NT) {
           S xv = 0;
-          for (int rb0 = C - 1; rb0 > rank; rb0 -= FB) {
-            S f[FB], t[FB];
-#pragma unroll
-            for (int q = 0; q < FB; q++) {
-              if (rb0 - q > rank) {
-                f[q] = cl.map_shared_rank(blkB, rb0 - q)[col];
-                t[q] = cl.map_shared_rank(s_tot, rb0 - q)[1];
-              }
-            }
-#pragma unroll
-            for (int q = 0; q < FB; q++)
-              if (rb0 - q > rank) xv = f[q] + t[q] * xv;
-          }
+          for (int q = C - 1; q > rank; q--) xv = inB[q * X + col] + totB[q] * xv;
           s_xin[col] = xv;
         }
         __syncthreads();
@@ -595,18 +599,19 @@ __global__ void __launch_bounds__(NT, (PairMinBlocks<S, NT, UPW>::v)) lvc_line_p
           }
           st_cols<S, UPW>(A + (j + 1) * LD + col0, xv);
         }
-        // halo rows of the cluster neighbours, and the price on the last step
-        if (halo_prev && chy == 0) {
-          S t[UPW];
-#pragma unroll
-          for (int h = 0; h < UPW; h++) t[h] = y[h][0];
-          st_cols<S, UPW>(halo_prev + col0, t);
-        }
-        if (halo_next && chy == Ls.CHy - 1) {
-          S t[UPW];
-#pragma unroll
-          for (int h = 0; h < UPW; h++) t[h] = y[h][K - 1];
-          st_cols<S, UPW>(halo_next + col0, t);
+        // halo rows of the cluster neighbours (for the next step), and the
+        // price on the last step
+        if (s + 1 < steps) {
+          if (has_prev && chy == 0) {
+            const unsigned d = cluster_addr(A + (Ycs + 1) * LD + col0, rank - 1);  // its bottom halo row
+            const unsigned hb = cluster_addr(barH, rank - 1);
+            if constexpr (UPW == 2) st_async2(d, y[0][0], y[1][0], hb); else st_async(d, y[0][0], hb);
+          }
+          if (has_next && chy == Ls.CHy - 1) {
+            const unsigned d = cluster_addr(A + col0, rank + 1);  // its top halo row
+            const unsigned hb = cluster_addr(barH, rank + 1);
+            if constexpr (UPW == 2) st_async2(d, y[0][K - 1], y[1][K - 1], hb); else st_async(d, y[0][K - 1], hb);
+          }
         }
         if (s == steps - 1 && out_h >= 0) {
           S pv = 0;
@@ -618,9 +623,6 @@ __global__ void __launch_bounds__(NT, (PairMinBlocks<S, NT, UPW>::v)) lvc_line_p
           args.out[c.out + item.strike] = (double)pv;  // myResult[myYindex, myXindex]
         }
       }
-      // halo rows pushed: release them to the neighbours' next step (the last
-      // step has no next step; the next item starts with a full cluster sync)
-      if (clustered && s + 1 < steps) asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory");
     }
   }
   if (clustered) cg::this_cluster().sync();

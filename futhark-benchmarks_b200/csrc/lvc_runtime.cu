@@ -421,7 +421,7 @@ bool line_pair_cfg(int X, int Y, int C, int max_smem, Config& cf, int upw = 2) {
   const int units = X * Ycs / 512;  // X units of 32 rows x 16 columns
   const int NW = units / upw;
   if (NW * upw != units || NW < 2 || NW > (upw == 2 ? 8 : 16) || (NW & (NW - 1))) return false;
-  const PairLayout F = pair_layout<S>(X, Ycs, upw);
+  const PairLayout F = pair_layout<S>(X, Ycs, upw, C);
   if (F.Ux != units || F.Uy != NW || F.total > max_smem) return false;
   cf.kind = kKindLine;
   cf.full = false;
