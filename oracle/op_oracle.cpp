@@ -218,6 +218,33 @@ void lvc_oracle_op_sums(int contract, int num_bits, int num_models, int num_und,
   }
 }
 
+// The f32 payoffs of paths [first, first + count), [path][model] -- for
+// checks of how the reference's reduce over paths may have been ordered.
+void lvc_oracle_op_payoffs(int contract, int num_bits, int num_models, int num_und, int num_dates, int num_discts,
+                           const int32_t* dir_vs, const float* md_cs, const float* md_vols, const float* md_drifts,
+                           const float* md_sts, const float* md_detvals, const float* md_discts,
+                           const int32_t* bb_inds, const float* bb_data, int64_t first, int64_t count, int threads,
+                           float* out) {
+  OpArgs q{contract, 0, num_bits, num_models, num_und, num_dates, num_discts, dir_vs, md_cs, md_vols, md_drifts,
+           md_sts, md_detvals, md_discts, bb_inds, bb_data};
+  if (threads < 1) threads = 1;
+  auto work = [&](int t) {
+    const int64_t lo = first + count * t / threads, hi = first + count * (t + 1) / threads;
+    const int K = num_dates * num_und;
+    std::vector<float> gauss(K), bbrow(num_dates), bb(K), prices(K);
+    std::vector<double> acc(num_models);
+    for (int64_t it = lo; it < hi; it++) {
+      for (int m = 0; m < num_models; m++) acc[m] = 0.0;
+      op_path(q, (int32_t)(it + 1), gauss.data(), bbrow.data(), bb.data(), prices.data(), acc.data());
+      for (int m = 0; m < num_models; m++) out[(it - first) * num_models + m] = (float)acc[m];
+    }
+  };
+  std::vector<std::thread> pool;
+  for (int t = 1; t < threads; t++) pool.emplace_back(work, t);
+  work(0);
+  for (auto& th : pool) th.join();
+}
+
 // One path's payoff per model (f32, before the mean) -- for per-path checks.
 void lvc_oracle_op_path(int contract, int num_bits, int num_models, int num_und, int num_dates, int num_discts,
                         const int32_t* dir_vs, const float* md_cs, const float* md_vols, const float* md_drifts,

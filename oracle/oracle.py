@@ -166,11 +166,39 @@ def option_pricing_sums(*inputs, first: int = 0, count: int | None = None, threa
     return sums
 
 
-def option_pricing(*inputs, threads: int | None = None) -> np.ndarray:
-    """finpar/OptionPricing.fut's main (f32): [num_models] mean payoffs."""
+def option_pricing(*inputs, threads: int | None = None, order: str = "f64") -> np.ndarray:
+    """finpar/OptionPricing.fut's main (f32): [num_models] mean payoffs.
+
+    order="f64": the sum over paths (a reduce whose order the program leaves
+    open, finpar/OptionPricing.fut:321) accumulated in f64 and rounded once --
+    the order the GPU kernels use.  order="sequential_f32": an f32 running sum
+    in path order, the order that reproduces the reference's own golden
+    outputs (finpar/OptionPricing-data/{small,medium}.out bit for bit)."""
     num_mc_it = int(inputs[1])
+    if order == "sequential_f32":
+        p = option_pricing_payoffs(*inputs, threads=threads)
+        tot = np.cumsum(p, axis=0, dtype=np.float32)[-1] if len(p) else np.zeros(p.shape[1], np.float32)
+        return (tot / np.float32(num_mc_it)).astype(np.float32)
+    if order != "f64":
+        raise ValueError(f"unknown order {order!r}")
     sums = option_pricing_sums(*inputs, threads=threads)
     return (sums.astype(np.float32) / np.float32(num_mc_it)).astype(np.float32)
+
+
+def option_pricing_payoffs(*inputs, first: int = 0, count: int | None = None,
+                           threads: int | None = None) -> np.ndarray:
+    """The f32 payoffs of paths [first, first + count), [path][model]."""
+    num_mc_it, a, dims = _op_arrays(inputs)
+    L = load()
+    fn = L.lvc_oracle_op_payoffs
+    fn.restype = None
+    fn.argtypes = [ctypes.c_int] * 6 + [ctypes.c_void_p] * 9 + [ctypes.c_int64, ctypes.c_int64, ctypes.c_int,
+                                                                  ctypes.c_void_p]
+    count = num_mc_it - first if count is None else count
+    threads = threads or max(1, min(os.cpu_count() or 1, 64))
+    out = np.zeros((count, dims[2]), np.float32)
+    fn(*dims, *[a[k].ctypes.data for k in OP_INPUTS[2:]], first, count, threads, out.ctypes.data)
+    return out
 
 
 def option_pricing_path(*inputs, n: int) -> np.ndarray:
