@@ -32,6 +32,7 @@ struct futhark_context {
   bool ok = false;
   void* scratch = nullptr;  // the entry point's scratch, grown on demand
   size_t scratch_bytes = 0;
+  int reduce_order = 0;        // OptionPricing: 0 f64 accumulation, 1 the reference's f32 running sum
   cudaStream_t aux = nullptr;  // a second stream for work that overlaps `stream`'s,
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;  // forked and joined by these events
 };

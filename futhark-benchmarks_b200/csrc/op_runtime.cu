@@ -63,6 +63,7 @@ struct OpDev {
   const float *md_cs, *md_vols, *md_drifts, *md_sts, *md_detvals, *md_discts;
   const int32_t* bb_inds;
   const float* bb_data;
+  float* pay_out;  // reference order: every path's payoff, [path][model]; null otherwise
 };
 
 __device__ __forceinline__ float f32exp(float x) { return (float)exp((double)x); }
@@ -246,6 +247,7 @@ __global__ void __launch_bounds__(kOpThreads, OpShape<C>::kMinCtas) op_paths_ker
         }
       }
       acc[mm] += (double)pay;
+      if (a.pay_out) a.pay_out[it * a.num_models + m0 + mm] = pay;
     }
   }
   // per-CTA sums in a fixed tree order: partial[mm][blockIdx.x]
@@ -496,7 +498,10 @@ __global__ void __launch_bounds__(kWarpPathWarps * 32, 2) op_paths_warp_kernel(O
           pay = price1 + amt * disc[1];
         }
       }
-      if (lane == 0) acc[mm] += (double)pay;
+      if (lane == 0) {
+        acc[mm] += (double)pay;
+        if (a.pay_out) a.pay_out[it * a.num_models + m0 + mm] = pay;
+      }
       __syncwarp();  // sB is rewritten by the next model or path
     }
   }
@@ -530,6 +535,160 @@ __global__ void __launch_bounds__(kOpReduceThreads) op_reduce_kernel(const doubl
     __syncthreads();
   }
   if (threadIdx.x == 0) out[m0 + mm] = (float)red[0] / (float)num_mc_it;
+}
+
+// ---------------------------------------------------------------------------
+// The reference's own order of the sum over paths (finpar/OptionPricing.fut:321
+// as its golden outputs were produced): an f32 running sum in path order,
+// s_k = fl(s_{k-1} + p_k).  Computed exactly, in parallel, from one fact: while
+// s stays in one binade [2^e, 2^(e+1)) -- f32 grid spacing u = 2^(e-23) -- and
+// p_k >= 0, fl(s + p_k) = s + u * t_k, where t_k is p_k / u rounded to the
+// nearest integer and does not depend on s (except on an exact tie, whose
+// round-to-even goes by the parity of s / u).  So a chunk of payoffs adds the
+// integer sum of its t_k to s / u until the sum would leave the binade; the
+// payoffs where that happens, ties, zero or tiny running sums and anything not
+// a finite nonnegative normal number are added one at a time in f32, exactly
+// as the sequential loop does.
+// ---------------------------------------------------------------------------
+constexpr int kSeqThreads = 1024;
+constexpr int kSeqPer = 16;  // payoffs per thread per chunk
+
+// t = p / 2^(e-23) rounded to nearest; false when p needs a step of its own
+// (a tie, p >= 2^e, p negative, non-finite or subnormal)
+__device__ __forceinline__ bool seq_units(float p, int e, uint32_t& t) {
+  const uint32_t b = __float_as_uint(p);
+  if (b == 0u) {  // +0
+    t = 0;
+    return true;
+  }
+  const int be = (int)((b >> 23) & 0xffu);
+  if ((b >> 31) || be == 0 || be == 0xff) return false;
+  const int d = e - (be - 127);  // p in [2^(e-d), 2^(e-d+1))
+  if (d < 1) return false;
+  const uint32_t m = (b & 0x7fffffu) | 0x800000u;
+  if (d > 31) {
+    t = 0;
+    return true;
+  }
+  t = m >> d;
+  const uint32_t rem = m & ((1u << d) - 1u), half = 1u << (d - 1);
+  if (rem == half) return false;
+  t += rem > half;
+  return true;
+}
+
+__device__ __forceinline__ int64_t warp_excl_scan(int64_t v, int lane) {
+  int64_t x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int64_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  return x - v;
+}
+
+__global__ void __launch_bounds__(kSeqThreads) op_seq_reduce_kernel(const float* __restrict__ pay, int64_t N,
+                                                                    int num_models, int m0, int num_mc_it,
+                                                                    float* __restrict__ out) {
+  const int mm = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const float* p = pay + m0 + mm;  // path k at p[k * num_models]
+  __shared__ float s_sum;
+  __shared__ long long s_next;
+  __shared__ int s_stop;
+  __shared__ long long s_warp[kSeqThreads / 32];
+  __shared__ long long s_base;
+  if (tid == 0) {
+    s_sum = 0.0f;
+    s_next = 0;
+  }
+  __syncthreads();
+  constexpr int CH = kSeqThreads * kSeqPer;
+  while (true) {
+    const int64_t i0 = s_next;
+    const float s = s_sum;
+    if (i0 >= N) break;
+    const uint32_t sb = __float_as_uint(s);
+    const int se = (int)((sb >> 23) & 0xffu);
+    if (se == 0 || se == 0xff || (sb >> 31)) {  // zero, tiny or irregular running sum: one step
+      __syncthreads();
+      if (tid == 0) {
+        s_sum = s + p[i0 * num_models];
+        s_next = i0 + 1;
+      }
+      __syncthreads();
+      continue;
+    }
+    const int e = se - 127;
+    const int64_t S0 = (int64_t)((sb & 0x7fffffu) | 0x800000u);  // s / u
+    const int64_t len = min((int64_t)CH, N - i0);
+    // pass 1: the first payoff of the chunk that needs a step of its own
+    if (tid == 0) s_stop = (int)len;
+    __syncthreads();
+    uint32_t t[kSeqPer];
+    int my_stop = (int)len;
+#pragma unroll
+    for (int j = 0; j < kSeqPer; j++) {
+      const int k = tid * kSeqPer + j;
+      t[j] = 0;
+      if (k < len && my_stop == (int)len && !seq_units(p[(i0 + k) * num_models], e, t[j])) my_stop = k;
+    }
+    if (my_stop < (int)len) atomicMin(&s_stop, my_stop);
+    __syncthreads();
+    const int stop = s_stop;
+    // pass 2: units before the stop, scanned; the first payoff that would
+    // carry the sum out of the binade is a stop too
+    int64_t mine = 0;
+#pragma unroll
+    for (int j = 0; j < kSeqPer; j++)
+      if (tid * kSeqPer + j < stop) mine += t[j];
+    const int64_t wex = warp_excl_scan(mine, lane);
+    if (lane == 31) s_warp[warp] = wex + mine;
+    __syncthreads();
+    if (warp == 0) {
+      const int64_t v = lane < kSeqThreads / 32 ? s_warp[lane] : 0;
+      const int64_t x = warp_excl_scan(v, lane);
+      if (lane < kSeqThreads / 32) s_warp[lane] = x;
+    }
+    __syncthreads();
+    int64_t run = S0 + s_warp[warp] + wex;  // s / u before this thread's first payoff
+    const int64_t lim = (int64_t)1 << 24;   // s / u reaching 2^24 leaves the binade
+    int cross = stop;
+#pragma unroll
+    for (int j = 0; j < kSeqPer; j++) {
+      const int k = tid * kSeqPer + j;
+      if (k < stop && cross == stop) {
+        if (run + t[j] >= lim) cross = k; else run += t[j];
+      }
+    }
+    if (cross < stop) atomicMin(&s_stop, cross);
+    __syncthreads();
+    const int q = s_stop;
+    // the sum before payoff q, from the thread whose range holds q (or the last)
+    const int owner = q < (int)len ? q / kSeqPer : kSeqThreads - 1;
+    if (tid == owner) {
+      int64_t r = S0 + s_warp[warp] + wex;
+#pragma unroll
+      for (int j = 0; j < kSeqPer; j++)
+        if (tid * kSeqPer + j < q) r += t[j];
+      s_base = r;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      float v = ldexpf((float)s_base, e - 23);  // exact: s_base < 2^24
+      int64_t nx = i0 + len;
+      if (q < (int)len) {
+        v = v + p[(i0 + q) * num_models];  // the step the sequential loop takes there
+        nx = i0 + q + 1;
+      }
+      s_sum = v;
+      s_next = nx;
+    }
+    __syncthreads();
+  }
+  if (tid == 0) {
+    const float f64_order = out[m0 + mm];  // NaN when the paths kernel priced nothing (bad bridge)
+    out[m0 + mm] = f64_order != f64_order ? f64_order : s_sum / (float)num_mc_it;
+  }
 }
 
 constexpr size_t kWarpSmem3 = sizeof(float) * OpWarpSmem<3>::kWords;
@@ -570,22 +729,33 @@ int op_validate(futhark_context* ctx, const op_args* q) {
 size_t partial_bytes(const futhark_context* ctx) {
   return (sizeof(double) * (size_t)kOpModels * (size_t)ctx->num_sms * kOpMaxCtasPerSm + 255) & ~(size_t)255;
 }
-size_t scratch_for(const futhark_context* ctx, const op_args* q) {
+size_t dirs_bytes(const op_args* q) {
   const size_t dirs = q->contract_number == 3
                           ? sizeof(int32_t) * (size_t)std::max(0, q->num_dates) * std::max(0, q->num_und) *
                                 std::max(0, q->num_bits)
                           : 0;
-  return partial_bytes(ctx) + dirs + 256;
+  return (dirs + 255) & ~(size_t)255;
+}
+// (reference order) every path's payoff, [path][model]
+size_t payoff_bytes(const futhark_context* ctx, const op_args* q) {
+  if (ctx->reduce_order != 1) return 0;
+  return sizeof(float) * (size_t)std::max(0, q->num_mc_it) * (size_t)std::max(0, q->num_models);
+}
+size_t scratch_for(const futhark_context* ctx, const op_args* q) {
+  return partial_bytes(ctx) + dirs_bytes(q) + payoff_bytes(ctx, q) + 256;
 }
 
 // Enqueues one pricing (lock held, device set, shapes valid, scratch large enough).
 int op_launch(futhark_context* ctx, const op_args* q, float* out, void* scratch) {
   if (q->num_models == 0) return 0;
   const int c = q->contract_number;
-  OpDev a{q->num_mc_it, q->num_bits, q->num_models, q->num_discts, q->dir_vs, q->md_cs, q->md_vols, q->md_drifts,
-          q->md_sts, q->md_detvals, q->md_discts, q->bb_inds, q->bb_data};
-  double* partial = static_cast<double*>(scratch);
   const bool priced = c >= 1 && c <= 3 && q->num_mc_it > 0;
+  float* pay_out = priced && ctx->reduce_order == 1
+                       ? reinterpret_cast<float*>(static_cast<char*>(scratch) + partial_bytes(ctx) + dirs_bytes(q))
+                       : nullptr;
+  OpDev a{q->num_mc_it, q->num_bits, q->num_models, q->num_discts, q->dir_vs, q->md_cs, q->md_vols, q->md_drifts,
+          q->md_sts, q->md_detvals, q->md_discts, q->bb_inds, q->bb_data, pay_out};
+  double* partial = static_cast<double*>(scratch);
   const int64_t T = priced ? op_ctas(ctx, c, q->num_mc_it) : 0;  // CTAs, one partial each
   int32_t* dirT = reinterpret_cast<int32_t*>(static_cast<char*>(scratch) + partial_bytes(ctx));
   if (priced && c == 3) {
@@ -610,8 +780,14 @@ int op_launch(futhark_context* ctx, const op_args* q, float* out, void* scratch)
     }
     // other contracts price every path at 0 (:302); no paths gives 0 / 0
     op_reduce_kernel<<<nm, kOpReduceThreads, 0, ctx->stream>>>(partial, T, m0, q->num_mc_it, out);
-    const cudaError_t e = cudaGetLastError();
+    cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(ctx, e, "option pricing reduction launch");
+    if (pay_out) {  // the reference's order replaces the f64 one (NaN stays NaN)
+      op_seq_reduce_kernel<<<nm, kSeqThreads, 0, ctx->stream>>>(pay_out, q->num_mc_it, q->num_models, m0,
+                                                                 q->num_mc_it, out);
+      e = cudaGetLastError();
+      if (e != cudaSuccess) return cuda_fail(ctx, e, "option pricing ordered reduction launch");
+    }
   }
   return 0;
 }
@@ -714,5 +890,13 @@ int op_check(struct futhark_context* ctx) {
   return e == cudaSuccess ? 0 : cuda_fail(ctx, e, "option pricing");
 }
 void* op_context_stream(struct futhark_context* ctx) { return ctx && ctx->ok ? (void*)ctx->stream : nullptr; }
+int op_context_set_reduction_order(struct futhark_context* ctx, int32_t order) {
+  if (!ctx) return FUTHARK_PROGRAM_ERROR;
+  std::lock_guard<std::mutex> g(ctx->mu);
+  if (order != OP_ORDER_F64 && order != OP_ORDER_SEQUENTIAL_F32)
+    return set_error(ctx, FUTHARK_PROGRAM_ERROR, "option pricing: unknown reduction order");
+  ctx->reduce_order = order;
+  return 0;
+}
 
 }  // extern "C"

@@ -48,6 +48,7 @@ def load_library(path: str = OP_LIB_PATH):
             "op_price_f32": (c_int, [vp, ctypes.POINTER(_OpArgs), vp, vp]),
             "op_check": (c_int, [vp]),
             "op_context_stream": (vp, [vp]),
+            "op_context_set_reduction_order": (c_int, [vp, i32]),
         })
     return _lib
 
@@ -99,6 +100,15 @@ class OpContext(ProgramContext):
         asynchronous on this context's stream."""
         a = self._args(contract, num_mc_it, dims, ptrs)
         self._check(self.lib.op_price_f32(self._ctx, ctypes.byref(a), out, scratch))
+
+    ORDER_F64 = 0
+    ORDER_SEQUENTIAL_F32 = 1
+
+    def set_reduction_order(self, order: int):
+        """Order of the sum over paths for the calls that follow: ORDER_F64
+        (default, f64 accumulation) or ORDER_SEQUENTIAL_F32 (an f32 running sum
+        in path order -- the order of the reference's golden outputs)."""
+        self._check(self.lib.op_context_set_reduction_order(self._ctx, order))
 
     def check(self):
         """Synchronises the context's stream; raises if a launch failed."""

@@ -126,6 +126,18 @@ OP_API int op_price_f32(struct futhark_context *ctx, const struct op_args *args,
 OP_API int op_check(struct futhark_context *ctx);
 /* The context's CUDA stream (a cudaStream_t). */
 OP_API void *op_context_stream(struct futhark_context *ctx);
+/* Order of the sum over paths (no counterpart in the reference's API; the
+ * program leaves the reduce's order open, finpar/OptionPricing.fut:321).
+ * OP_ORDER_F64 (the default): payoffs accumulated in f64 in a fixed tree
+ * order, rounded once -- the more accurate mean.  OP_ORDER_SEQUENTIAL_F32: an
+ * f32 running sum in path order, the order the reference's golden outputs
+ * (the .out files of finpar/OptionPricing-data) were produced in, computed exactly; it
+ * needs num_mc_it * num_models * 4 more bytes of scratch (op_scratch_bytes
+ * counts them) and time for a pass over the stored payoffs.  Applies to the
+ * calls that follow on this context. */
+#define OP_ORDER_F64 0
+#define OP_ORDER_SEQUENTIAL_F32 1
+OP_API int op_context_set_reduction_order(struct futhark_context *ctx, int32_t order);
 
 #ifdef __cplusplus
 }

@@ -166,3 +166,31 @@ def test_device_form_guards_bridge_indices(octx, op, name):
     good, _ = load_op(name)
     good[1] = np.int32(1000)
     assert np.isfinite(octx.main(*good)).all()
+
+
+@pytest.mark.parametrize("name", ["small", "medium", "large"])
+def test_reference_order_reproduces_golden_outputs(op, oracle, name):
+    """OP_ORDER_SEQUENTIAL_F32 (an f32 running sum over paths in path order):
+    the GPU equals the oracle in that order bit for bit, which reproduces the
+    reference's golden small.out and medium.out bit for bit and large.out to
+    3.7e-6."""
+    ins, want = load_op(name)
+    with op.OpContext() as c:
+        c.set_reduction_order(c.ORDER_SEQUENTIAL_F32)
+        got = c.main(*ins)
+    assert np.array_equal(got, oracle.option_pricing(*ins, order="sequential_f32"))
+    tol = 0.0 if name in ("small", "medium") else 4e-6
+    assert close_to(got, want, tol), (got, want)
+
+
+@pytest.mark.parametrize("name,paths", [("small", 1), ("small", 100003), ("medium", 77777), ("large", 4097)])
+def test_reference_order_path_counts(op, oracle, name, paths):
+    ins, _ = load_op(name)
+    ins[1] = np.int32(paths)
+    with op.OpContext() as c:
+        c.set_reduction_order(c.ORDER_SEQUENTIAL_F32)
+        got = c.main(*ins)
+        c.set_reduction_order(c.ORDER_F64)  # back to the default
+        f64 = c.main(*ins)
+    assert np.array_equal(got, oracle.option_pricing(*ins, order="sequential_f32"))
+    assert close_to(f64, oracle.option_pricing(*ins), ORACLE_REL_TOL)
