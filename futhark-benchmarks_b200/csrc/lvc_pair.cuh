@@ -24,6 +24,17 @@
 // lane), so the same block runs on twice the warps at half the registers per
 // thread -- more warps to hide shared-memory and FP64 latency when the grid's
 // shared memory leaves room for only one CTA per SM.
+//
+// Cluster (C CTAs per instance, rank r holding rows r*Ycs ..): the Y
+// recurrences cross the ranks.  Each step, after the forward chunk maps of
+// its block are known, a rank pushes them (st.async) to every higher rank and
+// folds the lower ranks' maps in rank order into its forward input z_in; the
+// same for the backward maps, pushed down and folded from the top into x_in.
+// Every wait is on the receiving CTA's own mbarrier, bounded.  The halo rows
+// the next step's explicit terms need are computed locally from the folds:
+// the row below the block is x_in itself, and the row above is the last row
+// of the rank below, x = (1/b') z_in + nY x_first (Thomas backward step with
+// that row's forward state z_in and this block's first row x_first).
 #pragma once
 
 #include "lvc_line.cuh"
@@ -32,7 +43,7 @@ namespace lvc {
 
 struct PairLayout {
   int LD, Ycs, CHx, Ux, CG2, CHy, Uy;
-  int bar, barF, barB, barH, A, B, w0, w1, w2, grow, gx, ex, tab0, tab1, xf, xb, yf, yb, inF, totF, inB, totB,
+  int bar, barF, barB, A, B, w0, w1, w2, grow, gx, ex, tab0, tab1, tabh, xf, xb, yf, yb, inF, totF, inB, totB,
       zin, xin, total;
 };
 
@@ -54,8 +65,7 @@ LVC_HD PairLayout pair_layout(int X, int Ycs, int upw, int C) {
   int o = 0;
   L.bar = o; o += 8;   // bulk copies of the step's pivots and table
   L.barF = o; o += 8;  // cluster: forward chunk maps of the lower ranks have landed
-  L.barB = o; o += 8;  // cluster: backward chunk maps of the higher ranks have landed
-  L.barH = o; o += 8;  // cluster: the neighbours' halo rows have landed
+  L.barB = o; o += 16; // cluster: backward chunk maps of the higher ranks have landed
   L.A = o; o += up((Ycs + 2) * L.LD * s);  // rows -1 .. Ycs (halo rows at both ends)
   L.B = o; o += up(Ycs * L.LD * s);
   L.w0 = o; o += up(X * s);               // W_k(i), planar
@@ -66,6 +76,7 @@ LVC_HD PairLayout pair_layout(int X, int Ycs, int upw, int C) {
   L.ex = o; o += up(Ycs * s);              // [Ycs] e_j of the current step, planar
   L.tab0 = o; o += up(8 * Ycs * 8);
   L.tab1 = o; o += up(8 * Ycs * 8);
+  L.tabh = o; o += 2 * 64;                 // cluster: the step-table row above the block, double-buffered
   L.xf = o; o += up(L.Ux / upw * 64 * s);  // [warp][lane] (a, b) of the warps' forward chunk maps
   L.xb = o; o += up(L.Ux / upw * 64 * s);  // the same, backward
   L.yf = o; o += up(L.Uy * 32 * upw * s);
@@ -141,16 +152,14 @@ __global__ void __launch_bounds__(NT, (PairMinBlocks<S, NT, UPW>::v)) lvc_line_p
   if (clustered) rank = (int)cg::this_cluster().block_rank();
   const int cid = blockIdx.x / C, ncl = gridDim.x / C;
   unsigned sc = 0, phase = 0;
-  unsigned phF = 0, phB = 0, phH = 0;  // parities of the cluster barriers (one completion per use)
+  unsigned phF = 0, phB = 0;  // parities of the cluster barriers (one completion per use)
   uint64_t* bar = reinterpret_cast<uint64_t*>(smem);
   uint64_t* barF = bar + 1;
   uint64_t* barB = bar + 2;
-  uint64_t* barH = bar + 3;
   if (tid == 0) {
     mbar_init(bar, 1);
     mbar_init(barF, 1);
     mbar_init(barB, 1);
-    mbar_init(barH, 1);
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
   __syncthreads();
@@ -187,6 +196,7 @@ __global__ void __launch_bounds__(NT, (PairMinBlocks<S, NT, UPW>::v)) lvc_line_p
     S* totF = reinterpret_cast<S*>(smem + Ls.totF);
     S* inB = reinterpret_cast<S*>(smem + Ls.inB);
     S* totB = reinterpret_cast<S*>(smem + Ls.totB);
+    double* const sTh = reinterpret_cast<double*>(smem + Ls.tabh);
     S* s_zin = reinterpret_cast<S*>(smem + Ls.zin);
     S* s_xin = reinterpret_cast<S*>(smem + Ls.xin);
     const double* tabc = args.tabs + c.tab;
@@ -196,17 +206,16 @@ __global__ void __launch_bounds__(NT, (PairMinBlocks<S, NT, UPW>::v)) lvc_line_p
     const PV* piv = args.piv + c.piv;
     const int64_t Y4 = round4(Y);
     // Cluster pushes (st.async into the other ranks' shared memory, counted
-    // on their barriers): this rank's halo rows go to the bottom halo row of
-    // rank - 1 and the top halo row of rank + 1; its forward chunk maps to
-    // every higher rank, its backward ones to every lower rank, at slot `rank`.
+    // on their barriers): this rank's forward block maps go to every higher
+    // rank, its backward ones to every lower rank, at slot `rank` -- two
+    // exchanges per step.  The halo rows are not exchanged: each rank computes
+    // its own from the folds' results (see the fix-up).
     const bool has_prev = clustered && rank > 0, has_next = clustered && rank < C - 1;
-    const unsigned halo_bytes = (unsigned)((has_prev + has_next) * X * (int)sizeof(S));
     const unsigned fold_bytes_F = (unsigned)(rank * (X + 1) * (int)sizeof(S));
     const unsigned fold_bytes_B = clustered ? (unsigned)((C - 1 - rank) * (X + 1) * (int)sizeof(S)) : 0u;
 
     // The previous instance is done with every buffer, and -- across the
-    // cluster -- every neighbour has finished pushing its last halo rows into
-    // this CTA before they are re-initialised below.
+    // cluster -- every rank has read the last block maps this CTA pushed to it.
     if (clustered) cg::this_cluster().sync(); else __syncthreads();
     // setPayoff (:46-47) on the block and the halo rows (zero at the global
     // boundary and in the two padding columns)
@@ -235,15 +244,17 @@ __global__ void __launch_bounds__(NT, (PairMinBlocks<S, NT, UPW>::v)) lvc_line_p
     }
     const unsigned piv_bytes = (unsigned)(Ycs * LD * (int)sizeof(S));  // a multiple of 16
     const unsigned tab_bytes = (unsigned)(Ycs * 64);
-    auto issue_copies = [&](int k, double* tdst) {
+    const unsigned tabh_bytes = has_prev ? 64u : 0u;
+    auto issue_copies = [&](int k, unsigned buf) {
       if (tid == 0) {
         asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-        mbar_expect_tx(bar, piv_bytes + tab_bytes);
+        mbar_expect_tx(bar, piv_bytes + tab_bytes + tabh_bytes);
         bulk_g2s(B, piv + ((int64_t)k * Y4 + r0) * LD, piv_bytes, bar);
-        bulk_g2s(tdst, tabc + Lt.stab + ((int64_t)k * Y + r0) * 8, tab_bytes, bar);
+        bulk_g2s(buf ? sT1 : sT0, tabc + Lt.stab + ((int64_t)k * Y + r0) * 8, tab_bytes, bar);
+        if (has_prev) bulk_g2s(sTh + 8 * buf, tabc + Lt.stab + ((int64_t)k * Y + r0 - 1) * 8, 64, bar);
       }
     };
-    issue_copies(steps - 1, (sc & 1) ? sT1 : sT0);
+    issue_copies(steps - 1, sc & 1);
 
     // X units u = UPW * warp + q: rows rgx*32 + lane, columns chx*16 .. -- a
     // warp's two units are neighbouring chunks of the same rows (the number of
@@ -288,17 +299,6 @@ __global__ void __launch_bounds__(NT, (PairMinBlocks<S, NT, UPW>::v)) lvc_line_p
       // e_j of this step, planar (the barrier below orders it before the X
       // sweep; its last readers were the previous step's passes 1 and 2)
       for (int j = tid; j < Ycs; j += NT) sE[j] = (S)tb[j * 8 + kSlotE];
-      // Cluster: the neighbours' halo rows of the previous step have landed
-      // (pushed by st.async, counted on barH).  Step 0 reads only the halo
-      // rows this CTA initialised itself.
-      if (clustered && s > 0) {
-        if (tid == 0) mbar_expect_tx(barH, halo_bytes);
-        if (!mbar_wait_cluster(barH, phH, timed_out ? kWaitPollsAfterTimeout : kWaitPolls)) {
-          timed_out = true;
-          atomicExch(args.err, 3);
-        }
-        phH ^= 1u;
-      }
       __syncthreads();
       const S dt = (S)tabc[Lt.dtinv + k];
 
@@ -486,7 +486,7 @@ __global__ void __launch_bounds__(NT, (PairMinBlocks<S, NT, UPW>::v)) lvc_line_p
         st_cols<S, UPW>(yf + warp * UW + UPW * lane, zz);
       }
       __syncthreads();
-      if (s + 1 < steps) issue_copies(k - 1, ((sc + 1) & 1) ? sT1 : sT0);
+      if (s + 1 < steps) issue_copies(k - 1, (sc + 1) & 1);
       if (clustered) {
         // this rank's forward block map of each column, pushed to every
         // higher rank; then the lower ranks' maps, folded in rank order
@@ -599,20 +599,21 @@ __global__ void __launch_bounds__(NT, (PairMinBlocks<S, NT, UPW>::v)) lvc_line_p
           }
           st_cols<S, UPW>(A + (j + 1) * LD + col0, xv);
         }
-        // halo rows of the cluster neighbours (for the next step), and the
-        // price on the last step
-        if (s + 1 < steps) {
-          if (has_prev && chy == 0) {
-            const unsigned d = cluster_addr(A + (Ycs + 1) * LD + col0, rank - 1);  // its bottom halo row
-            const unsigned hb = cluster_addr(barH, rank - 1);
-            if constexpr (UPW == 2) st_async2(d, y[0][0], y[1][0], hb); else st_async(d, y[0][0], hb);
-          }
-          if (has_next && chy == Ls.CHy - 1) {
-            const unsigned d = cluster_addr(A + col0, rank + 1);  // its top halo row
-            const unsigned hb = cluster_addr(barH, rank + 1);
-            if constexpr (UPW == 2) st_async2(d, y[0][K - 1], y[1][K - 1], hb); else st_async(d, y[0][K - 1], hb);
-          }
+        // Cluster halo rows for the next step, computed here: the row below
+        // the block is the first row of the rank above, which is this rank's
+        // x_in; the row above is the last row of the rank below,
+        // x = (1/b') z_in + nY x_first, with z_in this rank's forward input
+        // (the forward state of that row) and x_first this block's first row.
+        if (has_prev && chy == 0) {
+          const double* th = sTh + 8 * (sc & 1);
+          const S rbh = (S)th[kSlotRB], nyh = (S)th[kSlotNY];
+          S zr[UPW], t[UPW];
+          ld_cols<S, UPW>(s_zin + col0, zr);
+#pragma unroll
+          for (int h = 0; h < UPW; h++) t[h] = rbh * zr[h] + nyh * y[h][0];
+          st_cols<S, UPW>(A + col0, t);
         }
+        if (has_next && chy == Ls.CHy - 1) st_cols<S, UPW>(A + (Ycs + 1) * LD + col0, xin);
         if (s == steps - 1 && out_h >= 0) {
           S pv = 0;
 #pragma unroll
