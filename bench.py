@@ -801,13 +801,17 @@ def run_ours(args):
         c0 = sub[0]
         ctx.main_f64(c0.outer, c0.numX, c0.numY, c0.numT, c0.s0, c0.t, c0.alpha, c0.nu, c0.beta)
         torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        for c in sub:
-            ctx.main_f64(c.outer, c.numX, c.numY, c.numT, c.s0, c.t, c.alpha, c.nu, c.beta)
-        torch.cuda.synchronize()
-        dt = time.perf_counter() - t0
-        plain = {"value": sum(c.outer for c in sub) / dt, "unit": UNIT,
-                 "calls": len(sub), "form": "futhark_entry_main_f64 once per calibration"}
+        passes = []
+        for _ in range(2):  # host-side noise only adds time: the faster pass is reported
+            t0 = time.perf_counter()
+            for c in sub:
+                ctx.main_f64(c.outer, c.numX, c.numY, c.numT, c.s0, c.t, c.alpha, c.nu, c.beta)
+            torch.cuda.synchronize()
+            passes.append(time.perf_counter() - t0)
+        dt = min(passes)
+        plain = {"value": sum(c.outer for c in sub) / dt, "unit": UNIT, "calls": len(sub),
+                 "pass_seconds": passes, "form": "futhark_entry_main_f64 once per calibration, host prices; "
+                                                 "the faster of two passes"}
 
     plain_cfg = None
     if not args.no_plain_configs and rank == 0:

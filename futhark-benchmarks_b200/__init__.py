@@ -188,6 +188,7 @@ def load_library(path: str = LIB_PATH):
         "lvc_tridag_f32": (ctypes.c_int, [vp, i32, i64, i64, vp, vp, vp, vp, vp]),
         "lvc_tridag_check": (ctypes.c_int, [vp]),
         "lvc_wait_selftest": (ctypes.c_int, [vp, i32, i32]),
+        "lvc_entry_main_f64_noalloc_bytes": (i64, [vp, i32, i32, i32, i32]),
         "lvc_probe_peaks": (ctypes.c_int, [vp, ctypes.POINTER(f64), ctypes.POINTER(f64)]),
         "lvc_server_new": (ctypes.c_int, [vp, ctypes.POINTER(_ServerConfig), ctypes.POINTER(vp)]),
         "lvc_server_submit": (ctypes.c_int, [vp, ctypes.POINTER(_Calib), ctypes.POINTER(ctypes.c_uint64)]),

@@ -103,34 +103,73 @@ struct futhark_f32_2d {
 
 namespace {
 
-// Grow-only pool of device memory with a first-fit free list.  Plans built
-// for the entry points and for the serving runtime take their buffers from a
-// pool, so steady-state calls do not reach cudaMalloc/cudaFree (which
-// synchronise the device).  With a budget, allocation fails instead of
-// growing past it -- the serving runtime's HBM admission control.
+// Pool of device memory.  Plans (batch, entry point, serving) take their
+// buffers from a pool, so steady-state calls do not reach cudaMalloc/cudaFree
+// (which synchronise the device; freeing a batch plan's 10 GB of pivot rows
+// took most of a second).  Small requests are carved first-fit out of
+// 256 MB chunks; a request of a chunk or more gets a block of its own, which
+// is kept for later large requests (best fit) when released.  When the
+// device has no room left, blocks that are entirely free are returned to
+// CUDA (trim) and the allocation is retried.  With a budget, allocation fails
+// instead of growing past it -- the serving runtime's HBM admission control.
 struct DevicePool {
   std::mutex mu;
   size_t budget = 0;               // 0: unlimited
   size_t chunk = size_t(256) << 20;
-  std::vector<char*> blocks;
-  std::map<char*, size_t> free_;   // start -> size
+  std::map<char*, size_t> blocks;  // start -> size of every block from cudaMalloc
+  std::map<char*, size_t> large;   // blocks of a single large request (subset of blocks)
+  std::map<char*, size_t> free_;   // start -> size, in chunk blocks
+  std::map<char*, size_t> large_free;
   std::map<char*, size_t> used_;
   size_t reserved = 0, in_use = 0;
 
   ~DevicePool() {
-    for (char* b : blocks) cudaFree(b);
+    for (auto& b : blocks) cudaFree(b.first);
   }
-  bool grow(size_t sz) {
-    if (budget && reserved + sz > budget) return false;
+  char* grow(size_t sz) {
+    if (budget && reserved + sz > budget) return nullptr;
     char* p = nullptr;
     if (cudaMalloc(&p, sz) != cudaSuccess) {
       cudaGetLastError();
-      return false;
+      if (!trim_locked()) return nullptr;
+      if (budget && reserved + sz > budget) return nullptr;
+      if (cudaMalloc(&p, sz) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+      }
     }
-    blocks.push_back(p);
+    blocks[p] = sz;
     reserved += sz;
-    insert_free(p, sz);
-    return true;
+    return p;
+  }
+  // Returns every entirely free block to CUDA; true if any was released.
+  bool trim_locked() {
+    bool any = false;
+    for (auto it = large_free.begin(); it != large_free.end();) {
+      cudaFree(it->first);
+      reserved -= it->second;
+      blocks.erase(it->first);
+      large.erase(it->first);
+      it = large_free.erase(it);
+      any = true;
+    }
+    for (auto it = blocks.begin(); it != blocks.end();) {
+      auto f = free_.find(it->first);
+      if (!large.count(it->first) && f != free_.end() && f->second == it->second) {
+        cudaFree(it->first);
+        reserved -= it->second;
+        free_.erase(f);
+        it = blocks.erase(it);
+        any = true;
+      } else {
+        ++it;
+      }
+    }
+    return any;
+  }
+  void trim() {
+    std::lock_guard<std::mutex> g(mu);
+    trim_locked();
   }
   void insert_free(char* p, size_t sz) {
     auto nx = free_.lower_bound(p);
@@ -150,6 +189,27 @@ struct DevicePool {
   void* alloc(size_t bytes) {
     bytes = (std::max<size_t>(bytes, 1) + 255) & ~size_t(255);
     std::lock_guard<std::mutex> g(mu);
+    if (bytes >= chunk && !budget) {
+      // best fit among the released large blocks, else a block of its own
+      // (a budgeted pool carves everything out of its chunks)
+      auto best = large_free.end();
+      for (auto it = large_free.begin(); it != large_free.end(); ++it)
+        if (it->second >= bytes && (best == large_free.end() || it->second < best->second)) best = it;
+      char* p = nullptr;
+      size_t sz = 0;
+      if (best != large_free.end()) {
+        p = best->first;
+        sz = best->second;
+        large_free.erase(best);
+      } else {
+        sz = (bytes + (size_t(2) << 20) - 1) & ~((size_t(2) << 20) - 1);
+        if (!(p = grow(sz))) return nullptr;
+        large[p] = sz;
+      }
+      used_[p] = sz;
+      in_use += sz;
+      return p;
+    }
     for (int attempt = 0; attempt < 2; attempt++) {
       for (auto it = free_.begin(); it != free_.end(); ++it) {
         if (it->second >= bytes) {
@@ -163,9 +223,11 @@ struct DevicePool {
         }
       }
       if (attempt == 0) {
-        size_t sz = std::max(bytes, chunk);
+        size_t sz = chunk;
         if (budget && reserved + sz > budget) sz = bytes;
-        if (!grow(sz)) return nullptr;
+        char* p = grow(sz);
+        if (!p) return nullptr;
+        insert_free(p, sz);
       }
     }
     return nullptr;
@@ -178,7 +240,10 @@ struct DevicePool {
     const size_t sz = it->second;
     used_.erase(it);
     in_use -= sz;
-    insert_free(static_cast<char*>(vp), sz);
+    if (large.count(static_cast<char*>(vp)))
+      large_free[static_cast<char*>(vp)] = sz;
+    else
+      insert_free(static_cast<char*>(vp), sz);
   }
 };
 
@@ -893,6 +958,18 @@ cudaError_t plan_launch(lvc_plan* P, cudaStream_t s) {
   return plan_enqueue(P, s, nullptr);
 }
 
+// Device memory of the generated API's arrays comes from the context's pool:
+// a freed array's block serves the next one, so an entry-point call does not
+// reach cudaMalloc/cudaFree (cudaFree synchronises the whole device and its
+// cost varies from call to call).  Called with ctx->mu held.
+void* arr_alloc(futhark_context* ctx, size_t bytes) {
+  if (!ctx->pool) ctx->pool = new DevicePool();
+  return ctx->pool->alloc(bytes);
+}
+void arr_free(futhark_context* ctx, void* p) {
+  if (ctx->pool) ctx->pool->release(p);
+}
+
 int check_device_error(futhark_context* ctx, lvc_plan* P) {
   int h = 0;
   LVC_CUDA(ctx, cudaMemcpyAsync(&h, P->d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
@@ -1081,8 +1158,8 @@ int futhark_context_clear_caches(struct futhark_context* ctx) {
   LVC_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   plan_release(ctx->entry_plan);
   ctx->entry_plan = nullptr;
-  delete ctx->pool;
-  ctx->pool = nullptr;
+  // blocks still held by the caller's plans stay; every free one is returned
+  if (ctx->pool) ctx->pool->trim();
   return 0;
 }
 
@@ -1099,7 +1176,7 @@ int futhark_context_clear_caches(struct futhark_context* ctx) {
     if (!a) return nullptr;                                                                      \
     a->shape[0] = dim0;                                                                          \
     a->bytes = sizeof(T) * (size_t)std::max<int64_t>(1, dim0);                                   \
-    if (cudaMalloc(&a->data, a->bytes) != cudaSuccess) {                                         \
+    if (!(a->data = static_cast<T*>(arr_alloc(ctx, a->bytes)))) {                                \
       ctx->error = "out of device memory";                                                       \
       delete a;                                                                                  \
       return nullptr;                                                                            \
@@ -1107,7 +1184,7 @@ int futhark_context_clear_caches(struct futhark_context* ctx) {
     if (dim0 > 0 && data &&                                                                      \
         cudaMemcpyAsync(a->data, data, sizeof(T) * dim0, cudaMemcpyHostToDevice, ctx->stream) != \
             cudaSuccess) {                                                                       \
-      cudaFree(a->data);                                                                         \
+      arr_free(ctx, a->data);                                                                    \
       delete a;                                                                                  \
       ctx->error = "host to device copy failed";                                                 \
       return nullptr;                                                                            \
@@ -1120,7 +1197,7 @@ int futhark_context_clear_caches(struct futhark_context* ctx) {
     std::lock_guard<std::mutex> g(ctx->mu);                                                      \
     cudaSetDevice(ctx->device);                                                                  \
     cudaStreamSynchronize(ctx->stream);                                                          \
-    cudaFree(arr->data);                                                                         \
+    arr_free(ctx, arr->data);                                                                    \
     delete arr;                                                                                  \
     return 0;                                                                                    \
   }                                                                                              \
@@ -1157,19 +1234,19 @@ int futhark_entry_main_f64(struct futhark_context* ctx, struct futhark_f64_1d** 
   if (!a) return set_error(ctx, FUTHARK_OUT_OF_MEMORY, "host allocation failed");
   a->shape[0] = outer;
   a->bytes = sizeof(double) * (size_t)std::max(1, outer);
-  cudaError_t e = cudaMalloc(&a->data, a->bytes);
-  if (e != cudaSuccess) {
+  if (!(a->data = static_cast<double*>(arr_alloc(ctx, a->bytes)))) {
     delete a;
-    return cuda_fail(ctx, e, "cudaMalloc");
+    return set_error(ctx, FUTHARK_OUT_OF_MEMORY, "out of device memory");
   }
+  cudaError_t e;
   if (outer > 0 && (e = cudaMemcpyAsync(a->data, ctx->entry_plan->d_out, sizeof(double) * outer,
                                         cudaMemcpyDeviceToDevice, ctx->stream)) != cudaSuccess) {
-    cudaFree(a->data);
+    arr_free(ctx, a->data);
     delete a;
     return cuda_fail(ctx, e, "cudaMemcpyAsync");
   }
   if (int rc = check_device_error(ctx, ctx->entry_plan)) {
-    cudaFree(a->data);
+    arr_free(ctx, a->data);
     delete a;
     return rc;
   }
@@ -1190,22 +1267,22 @@ int futhark_entry_main(struct futhark_context* ctx, struct futhark_f32_1d** out0
   if (!a) return set_error(ctx, FUTHARK_OUT_OF_MEMORY, "host allocation failed");
   a->shape[0] = outer;
   a->bytes = sizeof(float) * (size_t)std::max(1, outer);
-  cudaError_t e = cudaMalloc(&a->data, a->bytes);
-  if (e != cudaSuccess) {
+  if (!(a->data = static_cast<float*>(arr_alloc(ctx, a->bytes)))) {
     delete a;
-    return cuda_fail(ctx, e, "cudaMalloc");
+    return set_error(ctx, FUTHARK_OUT_OF_MEMORY, "out of device memory");
   }
   if (outer > 0) {
     lvc_to_f32_kernel<<<(outer + 255) / 256, 256, 0, ctx->stream>>>(ctx->entry_plan->d_out, a->data,
                                                                      outer);
+    cudaError_t e;
     if ((e = cudaGetLastError()) != cudaSuccess) {
-      cudaFree(a->data);
+      arr_free(ctx, a->data);
       delete a;
       return cuda_fail(ctx, e, "lvc_to_f32_kernel");
     }
   }
   if (int rc = check_device_error(ctx, ctx->entry_plan)) {
-    cudaFree(a->data);
+    arr_free(ctx, a->data);
     delete a;
     return rc;
   }
@@ -1216,7 +1293,8 @@ int futhark_entry_main(struct futhark_context* ctx, struct futhark_f32_1d** out0
 int lvc_plan_new(struct futhark_context* ctx, const struct lvc_calibration* calibs, int32_t n,
                  int32_t precision, struct lvc_plan** plan) {
   std::lock_guard<std::mutex> g(ctx->mu);
-  return plan_new_locked(ctx, calibs, n, precision, plan);
+  if (ctx->ok && !ctx->pool) ctx->pool = new DevicePool();
+  return plan_new_locked(ctx, calibs, n, precision, plan, ctx->pool);
 }
 
 int lvc_plan_free(struct futhark_context* ctx, struct lvc_plan* plan) {
@@ -1707,11 +1785,21 @@ int lvc_probe_peaks(struct futhark_context* ctx, double* fp64_tflops, double* sm
   std::lock_guard<std::mutex> g(ctx->mu);
   if (!ctx->ok) return set_error(ctx, FUTHARK_PROGRAM_ERROR, "context has no usable CUDA device");
   LVC_CUDA(ctx, cudaSetDevice(ctx->device));
-  void* scratch = nullptr;
-  LVC_CUDA(ctx, cudaMalloc(&scratch, 1 << 20));
-  cudaEvent_t a, b;
-  LVC_CUDA(ctx, cudaEventCreate(&a));
-  LVC_CUDA(ctx, cudaEventCreate(&b));
+  // released on every return, the early error returns of LVC_CUDA included
+  struct Probe {
+    void* scratch = nullptr;
+    cudaEvent_t a = nullptr, b = nullptr;
+    ~Probe() {
+      if (a) cudaEventDestroy(a);
+      if (b) cudaEventDestroy(b);
+      if (scratch) cudaFree(scratch);
+    }
+  } pr;
+  LVC_CUDA(ctx, cudaMalloc(&pr.scratch, 1 << 20));
+  LVC_CUDA(ctx, cudaEventCreate(&pr.a));
+  LVC_CUDA(ctx, cudaEventCreate(&pr.b));
+  void* const scratch = pr.scratch;
+  const cudaEvent_t a = pr.a, b = pr.b;
   const int dgrid = ctx->num_sms * 8, diters = 20000;
   const int sgrid = ctx->num_sms * 4, siters = 20000;
   float best_d = 1e30f, best_s = 1e30f;
@@ -1736,9 +1824,6 @@ int lvc_probe_peaks(struct futhark_context* ctx, double* fp64_tflops, double* sm
   const double bytes = 16.0 * 4.0 * (double)siters * 512.0 * sgrid;
   *fp64_tflops = flops / (best_d * 1e-3) / 1e12;
   *smem_gbs = bytes / (best_s * 1e-3) / 1e9;
-  cudaEventDestroy(a);
-  cudaEventDestroy(b);
-  cudaFree(scratch);
   return 0;
 }
 
@@ -1794,6 +1879,36 @@ size_t up256(size_t n) { return (n + 255) & ~size_t(255); }
 
 }  // namespace
 
+// The scratch carve-up of one call: calibration record, error flag, row
+// table, work list, operator tables and pivot rows, each on a 256-byte boundary.
+struct NoallocCarve {
+  size_t o_calib, o_err, o_rows, o_items, o_tabs, o_piv, need;
+};
+NoallocCarve noalloc_carve(const Config& cf, int outer, int numX, int numY, int numT) {
+  const int Xp = std::max(8, pow2ceil(numX));
+  const int64_t tab_elems = al2(tab_layout(numX, numY, numT, Xp, cf.kind).total);
+  const int64_t piv_n = (piv_elems(numX, numY, numT, Xp, cf.kind, cf.ld) + 3) & ~int64_t(3);
+  NoallocCarve c;
+  c.o_calib = 0;
+  c.o_err = up256(c.o_calib + sizeof(CalibDev));
+  c.o_rows = up256(c.o_err + sizeof(int));
+  c.o_items = up256(c.o_rows + 2 * sizeof(int64_t));
+  c.o_tabs = up256(c.o_items + sizeof(Item) * (size_t)std::max(1, outer));
+  c.o_piv = up256(c.o_tabs + sizeof(double) * (size_t)tab_elems);
+  c.need = c.o_piv + sizeof(double) * (size_t)piv_n;
+  return c;
+}
+
+extern "C" int64_t lvc_entry_main_f64_noalloc_bytes(struct futhark_context* ctx, const int32_t outer,
+                                                    const int32_t numX, const int32_t numY, const int32_t numT) {
+  if (!ctx) return -1;
+  std::lock_guard<std::mutex> g(ctx->mu);
+  if (outer < 0 || numX < 3 || numY < 3 || numT < 1 || numX > kMaxNumX || numY > kMaxNumY) return -1;
+  const Config cf = choose_config<double>(ctx, numX, numY);
+  if (cf.gstate) return -1;
+  return (int64_t)noalloc_carve(cf, outer, numX, numY, numT).need;
+}
+
 extern "C" int lvc_entry_main_f64_noalloc(struct futhark_context* ctx, double* prices,
                                           const int32_t outer, const int32_t numX,
                                           const int32_t numY, const int32_t numT, const double s0,
@@ -1828,16 +1943,9 @@ extern "C" int lvc_entry_main_f64_noalloc(struct futhark_context* ctx, double* p
   d.tab = 0;
   d.piv = 0;
   d.out = 0;
-  const int64_t tab_elems = al2(tab_layout(numX, numY, numT, d.Xp, d.kind).total);
-  const int64_t piv_n = (piv_elems(numX, numY, numT, d.Xp, d.kind, d.ld) + 3) & ~int64_t(3);
-  // scratch carve-up
-  const size_t o_calib = 0;
-  const size_t o_err = up256(o_calib + sizeof(CalibDev));
-  const size_t o_rows = up256(o_err + sizeof(int));
-  const size_t o_items = up256(o_rows + 2 * sizeof(int64_t));
-  const size_t o_tabs = up256(o_items + sizeof(Item) * (size_t)std::max(1, outer));
-  const size_t o_piv = up256(o_tabs + sizeof(double) * (size_t)tab_elems);
-  const size_t need = o_piv + sizeof(double) * (size_t)piv_n;
+  const NoallocCarve cv = noalloc_carve(cf, outer, numX, numY, numT);
+  const size_t o_calib = cv.o_calib, o_err = cv.o_err, o_rows = cv.o_rows, o_items = cv.o_items,
+               o_tabs = cv.o_tabs, o_piv = cv.o_piv, need = cv.need;
   if (need > kNoAllocScratchBytes) {
     char buf[256];
     snprintf(buf, sizeof buf,
@@ -1947,6 +2055,7 @@ double now_s() {
 struct SrvRequest {
   uint64_t ticket = 0;
   lvc_calibration c{};
+  double work = 0;  // option-cell-steps: the admission order's size estimate
   double t_submit = 0, t_done = 0;
   std::vector<double> prices;
   int status = 0;  // 0 pending / running, 1 done, 2 failed
@@ -1956,6 +2065,7 @@ struct SrvRequest {
 struct SrvBatch {
   std::vector<SrvRequest*> reqs;
   lvc_plan* plan = nullptr;
+  bool cached = false;  // a one-request plan that goes back to the plan cache
   int stream = -1;
   cudaEvent_t done = nullptr;
   double sms = 0;
@@ -1973,6 +2083,13 @@ struct lvc_server {
   std::vector<bool> stream_busy;
   std::vector<double*> pinned;  // per stream: staging for prices and the error flag
   std::vector<int64_t> pinned_cap;
+  std::vector<double*> pinned_retired;  // outgrown staging, freed with the server (cudaFreeHost synchronises)
+  int32_t max_batch_configured = 0;     // cfg.max_batch_requests as given; restored after a back-off
+  // one-request plans kept for reuse, keyed by sizes (outer, numX, numY, numT);
+  // idle ones hold pool memory and are evicted when admission needs it
+  std::map<std::tuple<int, int, int, int>, std::vector<lvc_plan*>> plan_cache;
+  std::deque<std::pair<std::tuple<int, int, int, int>, lvc_plan*>> plan_lru;  // idle plans, oldest first
+  int64_t plans_reused = 0;
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
   std::deque<SrvRequest*> pending;
@@ -2026,7 +2143,17 @@ void server_retire(lvc_server* S) {
     if (S->sms_in_use < 1e-9) S->sms_in_use = 0;
     S->stream_busy[b->stream] = false;
     cudaEventDestroy(b->done);
-    plan_release(b->plan);
+    if (b->cached && q == cudaSuccess && !derr) {
+      const lvc_calibration& c = b->reqs[0]->c;
+      auto key = std::make_tuple((int)c.outer, (int)c.numX, (int)c.numY, (int)c.numT);
+      S->plan_cache[key].push_back(b->plan);
+      S->plan_lru.push_back({key, b->plan});
+    } else {
+      plan_release(b->plan);
+    }
+    // a batch completed: grow a backed-off batch size again toward the configured one
+    if (q == cudaSuccess && S->cfg.max_batch_requests < S->max_batch_configured)
+      S->cfg.max_batch_requests = std::min(S->max_batch_configured, 2 * S->cfg.max_batch_requests);
     delete b;
     it = S->inflight.erase(it);
   }
@@ -2058,15 +2185,30 @@ bool server_admit(lvc_server* S, std::unique_lock<std::mutex>& lk) {
       break;
     }
   if (si < 0) return false;
+  // Admission order: shortest job first (option-cell-steps), so that small
+  // requests are not queued behind large ones; a request that has waited
+  // longer than kStarveS goes first (oldest first), so large ones are not
+  // starved.
+  constexpr double kStarveS = 0.05;
+  const double tnow = now_s();
+  auto next_pick = [&]() {
+    auto best = S->pending.end();
+    for (auto it = S->pending.begin(); it != S->pending.end(); ++it) {
+      if (tnow - (*it)->t_submit > kStarveS) return it;  // the deque is in arrival order
+      if (best == S->pending.end() || (*it)->work < (*best)->work) best = it;
+    }
+    return best;
+  };
   std::vector<SrvRequest*> take;
   size_t bytes = 0;
-  const size_t free_bytes = S->pool.budget > S->pool.in_use ? S->pool.budget - S->pool.in_use : 0;
+  auto free_bytes = [&]() { return S->pool.budget > S->pool.in_use ? S->pool.budget - S->pool.in_use : 0; };
   while (!S->pending.empty() && (int)take.size() < S->cfg.max_batch_requests &&
          S->inflight_requests + (int)take.size() < S->cfg.max_inflight_requests) {
-    SrvRequest* r = S->pending.front();
+    auto pit = next_pick();
+    SrvRequest* r = *pit;
     const size_t rb = request_bytes(&S->sctx, r->c, S->cfg.precision);
     if (rb > S->pool.budget) {  // can never fit: fail it now
-      S->pending.pop_front();
+      S->pending.erase(pit);
       r->status = 2;
       r->error = "request needs more device memory than the server's HBM budget";
       r->t_done = now_s();
@@ -2074,33 +2216,71 @@ bool server_admit(lvc_server* S, std::unique_lock<std::mutex>& lk) {
       S->cv_done.notify_all();
       continue;
     }
-    if (bytes + rb > free_bytes) break;
+    // idle cached plans give their memory back before a request is refused
+    while (bytes + rb > free_bytes() && !S->plan_lru.empty()) {
+      auto victim = S->plan_lru.front();
+      S->plan_lru.pop_front();
+      auto& v = S->plan_cache[victim.first];
+      v.erase(std::find(v.begin(), v.end(), victim.second));
+      plan_release(victim.second);
+    }
+    if (bytes + rb > free_bytes()) break;
     take.push_back(r);
     bytes += rb;
-    S->pending.pop_front();
+    S->pending.erase(pit);
   }
   if (take.empty()) return false;
   std::vector<lvc_calibration> cs;
   for (SrvRequest* r : take) cs.push_back(r->c);
   S->stream_busy[si] = true;
-  lk.unlock();
+  // a one-request batch reuses an idle plan of the same sizes when there is one
   lvc_plan* P = nullptr;
-  int rc = plan_new_locked(&S->sctx, cs.data(), (int)cs.size(), S->cfg.precision, &P, &S->pool,
-                           /*use_graph=*/false, /*max_sms=*/-1);
+  if (take.size() == 1) {
+    const lvc_calibration& c = take[0]->c;
+    auto key = std::make_tuple((int)c.outer, (int)c.numX, (int)c.numY, (int)c.numT);
+    auto ci = S->plan_cache.find(key);
+    if (ci != S->plan_cache.end() && !ci->second.empty()) {
+      P = ci->second.back();
+      ci->second.pop_back();
+      for (auto li = S->plan_lru.begin(); li != S->plan_lru.end(); ++li)
+        if (li->second == P) {
+          S->plan_lru.erase(li);
+          break;
+        }
+      S->plans_reused++;
+    }
+  }
+  const bool reused = P != nullptr;
+  lk.unlock();
+  int rc = 0;
   cudaError_t e = cudaSuccess;
+  cudaStream_t st = S->streams[si];
+  if (reused) {
+    // new scalars into the plan's calibration record, uploaded on the batch's stream
+    fill_scalars(P->calibs[0], cs[0]);
+    P->params[0] = cs[0];
+    e = cudaMemcpyAsync(P->d_calibs, P->calibs.data(), sizeof(CalibDev), cudaMemcpyHostToDevice, st);
+  } else {
+    rc = plan_new_locked(&S->sctx, cs.data(), (int)cs.size(), S->cfg.precision, &P, &S->pool,
+                         /*use_graph=*/false, /*max_sms=*/-1);
+  }
   SrvBatch* b = nullptr;
-  if (!rc) {
+  if (!rc && e == cudaSuccess) {
     b = new SrvBatch();
     b->reqs = take;
     b->plan = P;
+    b->cached = take.size() == 1;
     b->stream = si;
     b->sms = P->sms;
     b->t_launch = now_s();
-    cudaStream_t st = S->streams[si];
     if (S->pinned_cap[si] < P->nprices + 1) {
-      if (S->pinned[si]) cudaFreeHost(S->pinned[si]);
-      S->pinned_cap[si] = std::max<int64_t>(P->nprices + 1, 4096);
+      // outgrown staging is kept until the server is freed: cudaFreeHost
+      // would synchronise the device under the running batches
+      if (S->pinned[si]) S->pinned_retired.push_back(S->pinned[si]);
+      S->pinned[si] = nullptr;
+      S->pinned_cap[si] = std::max<int64_t>(2 * (P->nprices + 1), 1 << 16);
       e = cudaMallocHost((void**)&S->pinned[si], sizeof(double) * S->pinned_cap[si]);
+      if (e != cudaSuccess) S->pinned_cap[si] = 0;
     }
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming);
     if (e == cudaSuccess) e = plan_enqueue(P, st, nullptr);
@@ -2118,15 +2298,21 @@ bool server_admit(lvc_server* S, std::unique_lock<std::mutex>& lk) {
     // the budget is taken by running batches (or fragmented): retry with
     // fewer requests, or when running batches complete
     if (P) plan_release(P);
+    // the taken requests go back in arrival order
+    auto requeue = [&]() {
+      for (SrvRequest* r : take) {
+        auto at = std::find_if(S->pending.begin(), S->pending.end(),
+                               [&](const SrvRequest* q) { return q->t_submit > r->t_submit; });
+        S->pending.insert(at, r);
+      }
+    };
+    requeue();
+    S->stream_busy[si] = false;
     if (S->inflight.empty()) {
-      for (size_t i = take.size(); i-- > 1;) S->pending.push_front(take[i]);
-      S->pending.push_front(take[0]);
-      S->stream_busy[si] = false;
+      // back off to half the batch; completed batches restore it (server_retire)
       S->cfg.max_batch_requests = std::max<int32_t>(1, (int32_t)take.size() / 2);
       return true;  // try again at once with the smaller batch size
     }
-    for (auto it = take.rbegin(); it != take.rend(); ++it) S->pending.push_front(*it);
-    S->stream_busy[si] = false;
     return false;
   }
   if (rc || e != cudaSuccess) {
@@ -2192,6 +2378,7 @@ int lvc_server_new(struct futhark_context* ctx, const struct lvc_server_config* 
   lvc_server* S = new lvc_server();
   S->user_ctx = ctx;
   S->cfg = c;
+  S->max_batch_configured = c.max_batch_requests;
   S->sctx.device = ctx->device;
   S->sctx.num_sms = ctx->num_sms;
   S->sctx.max_smem = ctx->max_smem;
@@ -2207,14 +2394,22 @@ int lvc_server_new(struct futhark_context* ctx, const struct lvc_server_config* 
     if (e == cudaSuccess) {
       S->streams.push_back(st);
       S->stream_busy.push_back(false);
-      S->pinned.push_back(nullptr);
-      S->pinned_cap.push_back(0);
+      // staging for 65535 prices and the error flag; a larger batch grows it
+      double* pin = nullptr;
+      e = cudaMallocHost((void**)&pin, sizeof(double) << 16);
+      S->pinned.push_back(e == cudaSuccess ? pin : nullptr);
+      S->pinned_cap.push_back(e == cudaSuccess ? (1 << 16) : 0);
     }
   }
   // reserve the whole budget up front: serving never reaches cudaMalloc
-  if (e == cudaSuccess && !S->pool.grow((size_t)c.hbm_budget_bytes)) e = cudaErrorMemoryAllocation;
+  if (e == cudaSuccess) {
+    char* blk = S->pool.grow((size_t)c.hbm_budget_bytes);
+    if (blk) S->pool.insert_free(blk, (size_t)c.hbm_budget_bytes); else e = cudaErrorMemoryAllocation;
+  }
   if (e != cudaSuccess) {
     for (cudaStream_t st : S->streams) cudaStreamDestroy(st);
+    for (double* pin : S->pinned)
+      if (pin) cudaFreeHost(pin);
     if (S->sctx.stream) cudaStreamDestroy(S->sctx.stream);
     if (S->sctx.capture) cudaStreamDestroy(S->sctx.capture);
     delete S;
@@ -2232,6 +2427,7 @@ int lvc_server_submit(struct lvc_server* S, const struct lvc_calibration* c, uin
   }
   SrvRequest* r = new SrvRequest();
   r->c = *c;
+  r->work = (double)c->outer * c->numX * c->numY * (c->numT > 1 ? c->numT - 1 : 0);
   r->t_submit = now_s();
   {
     std::lock_guard<std::mutex> g(S->mu);
@@ -2330,6 +2526,9 @@ int lvc_server_free(struct lvc_server* S) {
     cudaStreamDestroy(S->streams[i]);
     if (S->pinned[i]) cudaFreeHost(S->pinned[i]);
   }
+  for (double* p : S->pinned_retired) cudaFreeHost(p);
+  for (auto& kv : S->plan_cache)
+    for (lvc_plan* P : kv.second) plan_release(P);
   cudaStreamDestroy(S->sctx.stream);
   cudaStreamDestroy(S->sctx.capture);
   delete S;
@@ -2415,15 +2614,14 @@ int tridag_entry(futhark_context* ctx, futhark_f32_2d** out0, const futhark_f32_
   o->shape[0] = rows;
   o->shape[1] = m;
   o->bytes = sizeof(float) * (size_t)std::max<int64_t>(1, rows * m);
-  if (cudaMalloc(&o->data, o->bytes) != cudaSuccess) {
+  if (!(o->data = static_cast<float*>(arr_alloc(ctx, o->bytes)))) {
     delete o;
-    cudaGetLastError();
     return set_error(ctx, FUTHARK_OUT_OF_MEMORY, "out of device memory");
   }
   int rc = tridag_launch(ctx, form, rows, m, a->data, b->data, c->data, y->data, o->data);
   if (!rc) rc = tridag_check_locked(ctx);
   if (rc) {
-    cudaFree(o->data);
+    arr_free(ctx, o->data);
     delete o;
     return rc;
   }
@@ -2449,15 +2647,14 @@ struct futhark_f32_2d* futhark_new_f32_2d(struct futhark_context* ctx, const flo
   a->shape[1] = dim1;
   const int64_t n = dim0 * dim1;
   a->bytes = sizeof(float) * (size_t)std::max<int64_t>(1, n);
-  if (cudaMalloc(&a->data, a->bytes) != cudaSuccess) {
-    cudaGetLastError();
+  if (!(a->data = static_cast<float*>(arr_alloc(ctx, a->bytes)))) {
     ctx->error = "out of device memory";
     delete a;
     return nullptr;
   }
   if (n > 0 && data &&
       cudaMemcpyAsync(a->data, data, sizeof(float) * n, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess) {
-    cudaFree(a->data);
+    arr_free(ctx, a->data);
     delete a;
     ctx->error = "host to device copy failed";
     return nullptr;
@@ -2471,7 +2668,7 @@ int futhark_free_f32_2d(struct futhark_context* ctx, struct futhark_f32_2d* arr)
   std::lock_guard<std::mutex> g(ctx->mu);
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
-  cudaFree(arr->data);
+  arr_free(ctx, arr->data);
   delete arr;
   return 0;
 }

@@ -192,11 +192,16 @@ LVC_API int lvc_batch(struct futhark_context *ctx, const struct lvc_calibration 
  * and errors as futhark_entry_main_f64, but the prices go to `prices`, a
  * device buffer of outer_loop_count doubles owned by the caller, and all
  * scratch comes from one static device array of LVC_NOALLOC_SCRATCH_BYTES
- * (64 MiB) that every device loading this library holds until exit; the call
- * allocates no device memory.  Calibrations whose scratch exceeds that size
- * (8 * (numX|1) * numY * (numT-1) bytes of pivots plus 64 * numY * (numT-1)
- * bytes of tables; all three reference datasets fit) or whose grid does not
- * fit on chip are rejected with an error.
+ * (64 MiB) that every device loading this library holds until exit -- the
+ * array belongs to the library's device code, so loading the library's
+ * kernels on a device reserves it whether or not this entry point is called
+ * (the serving runtime's HBM budget does not count it); the call allocates no
+ * device memory.  Calibrations whose scratch exceeds that size (the
+ * calibration's pivot rows, about 8 * (numX + 2) * round4(numY) * (numT - 1)
+ * bytes for the paired kernel, plus its tables, about 64 * numY * (numT - 1)
+ * bytes; lvc_entry_main_f64_noalloc_bytes gives the exact figure; all three
+ * reference datasets fit) or whose grid does not fit on chip are rejected
+ * with an error.
  * The first call on each device looks up the array's device address
  * (cudaGetSymbolAddress); make that first call before any stream capture.
  * Runs on the context's stream and returns after the prices are written.
@@ -209,6 +214,13 @@ LVC_API int lvc_entry_main_f64_noalloc(struct futhark_context *ctx, double *pric
                                        const int32_t numY, const int32_t numT, const double s0,
                                        const double t, const double alpha, const double nu,
                                        const double beta);
+/* No counterpart in the reference.  The scratch bytes lvc_entry_main_f64_noalloc
+ * needs for a calibration of these sizes under the context's current shape
+ * for the grid class (the figure it compares with LVC_NOALLOC_SCRATCH_BYTES);
+ * -1 for invalid sizes or a grid that does not fit on chip.  Allocates
+ * nothing. */
+LVC_API int64_t lvc_entry_main_f64_noalloc_bytes(struct futhark_context *ctx, const int32_t outer_loop_count,
+                                                 const int32_t numX, const int32_t numY, const int32_t numT);
 
 /*
  * Serving runtime: continuous batching of calibration requests.  A

@@ -65,3 +65,14 @@ def test_noalloc_rejects_oversized_calibration(pkg):
         # the context is still usable
         rc = fn(ctx._ctx, ctypes.c_void_p(out.data_ptr()), 4, 32, 32, 8, 0.03, 5.0, 0.2, 0.6, 0.5)
         assert rc == 0
+
+
+def test_noalloc_size_query(pkg):
+    # the size query gives the figure the entry point checks: the medium
+    # dataset fits, the oversized calibration above does not, bad sizes are -1
+    with pkg.Context("#0") as ctx:
+        q = pkg.load_library().lvc_entry_main_f64_noalloc_bytes
+        limit = 64 << 20
+        assert 0 < q(ctx._ctx, 128, 256, 32, 64) <= limit
+        assert q(ctx._ctx, 4, 256, 256, 256) > limit
+        assert q(ctx._ctx, 4, 2, 16, 8) == -1
