@@ -47,7 +47,7 @@ F_ALG = 77
 # state precision, from an ncu capture of those launches (the profile named
 # beside each figure); bench.py scales it by the step's option-cell-steps.
 TRAFFIC_PER_CELL_STEP = {
-    "f64": (382.956e9 / 13 / 44624944128, "profiles/launches_bench_uneven.txt"),
+    "f64": (2.027e9 / 4.496e9, "profiles/lvc_rollback_dram_mix64.txt"),
 }
 CALIB_DEV_BYTES = 112  # sizeof(lvc::CalibDev) (static_assert in lvc_layout.h), uploaded per calibration per step
 
@@ -600,12 +600,15 @@ def run_plain_configs(pkg, wl, ctx, args, fp64_peak):
         work = c.work()
         achieved = F_ALG * work / (ms_run * 1e-3) / 1e12
 
-        def cpu(k, nthreads):
+        def cpu(k, nthreads, f32=False):
             ts = []
             ref = None
             for _ in range(5):
                 t0 = time.perf_counter()
-                ref = oracle.main_f64(k, *a9[1:], threads=nthreads)
+                if f32:
+                    ref = oracle.main_f32(k, *a9[1:], threads=nthreads)
+                else:
+                    ref = oracle.main_f64(k, *a9[1:], threads=nthreads)
                 ts.append(time.perf_counter() - t0)
             return k / statistics.median(ts), ref
 
@@ -613,6 +616,7 @@ def run_plain_configs(pkg, wl, ctx, args, fp64_peak):
         v1, ref1 = cpu(k1, 1)
         kn = min(c.outer, k1 * threads)
         vn, refn = cpu(kn, threads)
+        v32, _ = cpu(kn, threads, f32=True)
         rel = np.abs(got[:kn] - refn) / np.abs(refn)
         res[name] = {
             "shape": {"outer": c.outer, "numX": c.numX, "numY": c.numY, "numT": c.numT},
@@ -626,6 +630,8 @@ def run_plain_configs(pkg, wl, ctx, args, fp64_peak):
                          "timing": "whole run (setup + pivot + rollback) with CUDA events"},
             "cpu_baseline": {"all_threads": {"value": vn, "cores": threads, "strikes": kn},
                              "one_thread": {"value": v1, "cores": 1, "strikes": k1},
+                             "all_threads_f32": {"value": v32, "cores": threads, "strikes": kn,
+                                                 "what": "the oracle at the reference's own precision"},
                              "unit": UNIT, "kind": "port",
                              "sample": "the first strikes of the dataset, f64 oracle, median of 5 runs"},
             "max_rel_err_vs_fp64_oracle": float(rel.max()),

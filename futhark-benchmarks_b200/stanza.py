@@ -96,8 +96,25 @@ def _braced(text: str, pos: int):
 _WORD = re.compile(r"\s*(\"[^\"]*\"|[A-Za-z_][\w]*:?|@|\{|==)")
 
 
+def block_of(program: str) -> str:
+    """The test block of a whole program text: its ``-- ==`` line and the rest
+    of that comment block."""
+    lines = program.splitlines()
+    for start, ln in enumerate(lines):
+        if ln.strip() == "-- ==":
+            break
+    else:
+        raise StanzaError("no '-- ==' line")
+    end = start
+    while end < len(lines) and lines[end].lstrip().startswith("--"):
+        end += 1
+    return "\n".join(lines[start:end]) + "\n"
+
+
 def parse(block: str) -> List[Run]:
-    """Parse one test block (the comment lines from ``-- ==`` on)."""
+    """Parse a program's test block; given a whole program text, its block."""
+    if any(ln.strip() and not ln.lstrip().startswith("--") for ln in block.splitlines()):
+        block = block_of(block)
     text = _strip(block)
     pos = 0
     entries = ["main"]

@@ -42,22 +42,11 @@ PROGRAMS = ["finpar/LocVolCalib.fut", "misc/ocean-sim/tridiag-test.fut", "misc/o
             "finpar/OptionPricing.fut"]
 
 
-def stanza_block(text: str) -> str:
-    """The test block of a program: from its ``-- ==`` line to the end of that
-    comment block."""
-    lines = text.splitlines()
-    start = next(i for i, ln in enumerate(lines) if ln.strip() == "-- ==")
-    end = start
-    while end < len(lines) and lines[end].startswith("--"):
-        end += 1
-    return "\n".join(lines[start:end]) + "\n"
-
-
 def main(ref_root: str) -> None:
     stanzas = {}
     for prog in PROGRAMS:
         with open(os.path.join(ref_root, prog)) as f:
-            block = stanza_block(f.read())
+            block = stanza.block_of(f.read())
         stanzas[prog] = block
         for run in stanza.parse(block):
             for rel in (run.input_file, run.output_file):

@@ -48,6 +48,13 @@ def test_every_block_parses():
                     assert os.path.exists(os.path.join(DATASETS, os.path.dirname(prog), rel + ".gz")), rel
 
 
+def test_parse_whole_program_text():
+    # a program's code and its other comments around the block are skipped
+    prog = "-- A program\n-- ==\n-- input { 1i32 }\n-- output { 2i32 }\n\n-- a comment\ndef main (x: i32) = x + 1\n"
+    runs = st.parse(prog)
+    assert len(runs) == 1 and runs[0].output_values.strip() == "2i32"
+
+
 def test_parser_inline_values_and_errors():
     block = """-- ==
 -- entry: f g
