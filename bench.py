@@ -71,6 +71,8 @@ def parse():
     ap.add_argument("--no-f32", action="store_true", help="skip the FP32-state section")
     ap.add_argument("--no-tridiag", action="store_true", help="skip the batched tridiagonal solver section")
     ap.add_argument("--no-tke", action="store_true", help="skip the ocean model's tke step section")
+    ap.add_argument("--only-tridiag", action="store_true",
+                    help="run only the batched tridiagonal solver section (one GPU) and print its JSON object")
     ap.add_argument("--only-tke", action="store_true",
                     help="run only the tke step section (one GPU) and print its JSON object")
     ap.add_argument("--no-op", action="store_true", help="skip the OptionPricing section")
@@ -923,6 +925,13 @@ def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.only_tridiag:
+        pkg = importlib.import_module("futhark-benchmarks_b200")
+        ctx = pkg.Context("#0")
+        try:
+            print(json.dumps(run_tridiag(pkg, importlib.import_module("futhark-benchmarks_b200.workloads"), ctx, args)))
+        finally:
+            ctx.close()
     elif args.only_tke:
         print(json.dumps(run_tke(importlib.import_module("futhark-benchmarks_b200.workloads"), args)))
     elif args.only_op:

@@ -7,9 +7,11 @@
 //           4-tuple matrix scan for the pivots, two linear-function scans --
 //           folded left to right.
 //
-// Two kernels, one thread per system in both: lvc_tridag_block_kernel (m up
-// to 400, the common case) stages a warp's 32 systems through shared memory
-// with coalesced copies; lvc_tridag_kernel (any m) reads rows in place.
+// Three kernels, one thread per system in each: for m up to 400 (the common
+// case) lvc_tridag_block_kernel (FORM 0) stages a warp's 32 systems through
+// shared memory with bulk copies and lvc_tridag_stream_kernel (FORM 1)
+// streams them through a window of columns; lvc_tridag_kernel (any m, both
+// forms) reads rows in place.
 // Each recurrence runs in the reference's operation
 // order with every product, sum and quotient explicitly rounded (no fused
 // multiply-add), so a system's solution is bit for bit the one the CPU
@@ -157,16 +159,18 @@ __global__ void __launch_bounds__(kTriThreads) lvc_tridag_kernel(int64_t rows, i
   }
 }
 
-// Block kernel: one warp per 32 consecutive systems.  In row-major [rows][m]
-// arrays those systems are one contiguous block of 32*m floats per array, so
-// the warp copies the four input blocks into shared memory with coalesced
-// 16-byte loads, each lane then runs its system's recurrences out of shared
-// memory (row stride m: for odd m the 32 lanes hit 32 different banks), and
-// the solution block goes back with coalesced stores.  Every intermediate
-// overwrites an input element that is no longer needed -- FORM 0: cp_i over
-// c_i, yp_i and then x_i over y_i; FORM 1: b'_i over b_i, y'_i and then x_i
-// over y_i -- so the shared memory is exactly the four input blocks.  The
-// arithmetic and its order are those of lvc_tridag_kernel.
+// Block kernel for tridagSeq (FORM 0 of lvc_tridag_kernel): one warp per 32
+// consecutive systems.  In row-major [rows][m] arrays those systems are one
+// contiguous block of 32*m floats per array, so the warp copies the four
+// input blocks into shared memory with coalesced 16-byte loads, each lane
+// then runs its system's recurrences out of shared memory (row stride m: for
+// odd m the 32 lanes hit 32 different banks), and the solution block goes
+// back with coalesced stores.  Every intermediate overwrites an input element
+// that is no longer needed -- cp_i over c_i, yp_i and then x_i over y_i -- so
+// the shared memory is exactly the four input blocks.  The arithmetic and its
+// order are those of lvc_tridag_kernel.  (tridagPar, whose three passes keep
+// b' and y' besides the inputs, streams its inputs instead:
+// lvc_tridag_stream_kernel.)
 // When the arrays are 16-byte aligned and a block's bytes a multiple of 16
 // (every full block: 32 * m * 4 bytes), one thread moves the blocks with TMA
 // bulk copies (four in, one out) -- tens of kilobytes in flight per CTA,
@@ -192,7 +196,6 @@ __device__ __forceinline__ void tri_bulk_s2g(void* dst, const void* src, unsigne
                : "memory");
 }
 
-template <int FORM>
 __global__ void __launch_bounds__(32) lvc_tridag_block_kernel(int64_t rows, int m, const float* __restrict__ a,
                                                              const float* __restrict__ b,
                                                              const float* __restrict__ c,
@@ -244,79 +247,22 @@ __global__ void __launch_bounds__(32) lvc_tridag_block_kernel(int64_t rows, int 
     float* br = sb + (int64_t)lane * m;
     float* cr = scc + (int64_t)lane * m;
     float* yr = sy + (int64_t)lane * m;
-    if constexpr (FORM == 0) {
-      float cp = tri_div(cr[0], br[0]);
-      float yp = tri_div(yr[0], br[0]);
-      cr[0] = cp;
-      yr[0] = yp;
-      for (int i = 1; i < m; i++) {
-        const float ai = ar[i];
-        const float nf = tri_rcp(tri_sub(br[i], tri_mul(ai, cp)));
-        cp = tri_mul(cr[i], nf);
-        yp = tri_mul(tri_sub(yr[i], tri_mul(ai, yp)), nf);
-        cr[i] = cp;
-        yr[i] = yp;
-      }
-      float x = yp;
-      for (int i = m - 2; i >= 0; i--) {
-        x = tri_sub(yr[i], tri_mul(cr[i], x));
-        yr[i] = x;
-      }
-    } else {
-      const float b0 = br[0];
-      float s0 = 1.0f, s1 = 0.0f, s2 = 0.0f, s3 = 1.0f;
-      float cprev = 0.0f;  // c_{i-1}, read before b'_{i-1} replaced b_{i-1} (c is not overwritten)
-      for (int i = 0; i < m; i++) {
-        float m0 = 1.0f, m1 = 0.0f, m2 = 0.0f, m3 = 1.0f;
-        if (0 < i) {
-          m0 = br[i];
-          m1 = tri_sub(0.0f, tri_mul(ar[i], cprev));
-          m2 = 1.0f;
-          m3 = 0.0f;
-        }
-        cprev = cr[i];
-        const float value = tri_rcp(tri_mul(s0, m0));
-        const float n0 = tri_mul(tri_add(tri_mul(m0, s0), tri_mul(m1, s2)), value);
-        const float n1 = tri_mul(tri_add(tri_mul(m0, s1), tri_mul(m1, s3)), value);
-        const float n2 = tri_mul(tri_add(tri_mul(m2, s0), tri_mul(m3, s2)), value);
-        const float n3 = tri_mul(tri_add(tri_mul(m2, s1), tri_mul(m3, s3)), value);
-        s0 = n0;
-        s1 = n1;
-        s2 = n2;
-        s3 = n3;
-        br[i] = tri_div(tri_add(tri_mul(s0, b0), s1), tri_add(tri_mul(s2, b0), s3));  // b'_i
-      }
-      const float y0 = yr[0];
-      float c0 = 0.0f, c1 = 1.0f;
-      for (int i = 0; i < m; i++) {
-        float l0 = 0.0f, l1 = 1.0f;
-        if (0 < i) {
-          l0 = yr[i];
-          l1 = tri_sub(0.0f, tri_div(ar[i], br[i - 1]));
-        }
-        const float n0 = tri_add(l0, tri_mul(l1, c0));
-        const float n1 = tri_mul(c1, l1);
-        c0 = n0;
-        c1 = n1;
-        yr[i] = tri_add(c0, tri_mul(c1, y0));  // y'_i over y_i (y_i already read)
-      }
-      const float yn = tri_div(yr[m - 1], br[m - 1]);
-      c0 = 0.0f;
-      c1 = 1.0f;
-      for (int k = 0; k < m; k++) {
-        const int i = m - k - 1;
-        float l0 = 0.0f, l1 = 1.0f;
-        if (0 < k) {
-          const float bi = br[i];
-          l0 = tri_div(yr[i], bi);
-          l1 = tri_sub(0.0f, tri_div(cr[i], bi));
-        }
-        const float n0 = tri_add(l0, tri_mul(l1, c0));
-        const float n1 = tri_mul(c1, l1);
-        c0 = n0;
-        c1 = n1;
-        yr[i] = tri_add(c0, tri_mul(c1, yn));
-      }
+    float cp = tri_div(cr[0], br[0]);
+    float yp = tri_div(yr[0], br[0]);
+    cr[0] = cp;
+    yr[0] = yp;
+    for (int i = 1; i < m; i++) {
+      const float ai = ar[i];
+      const float nf = tri_rcp(tri_sub(br[i], tri_mul(ai, cp)));
+      cp = tri_mul(cr[i], nf);
+      yp = tri_mul(tri_sub(yr[i], tri_mul(ai, yp)), nf);
+      cr[i] = cp;
+      yr[i] = yp;
+    }
+    float x = yp;
+    for (int i = m - 2; i >= 0; i--) {
+      x = tri_sub(yr[i], tri_mul(cr[i], x));
+      yr[i] = x;
     }
   }
   float* dst = out + off;
@@ -340,6 +286,182 @@ __global__ void __launch_bounds__(32) lvc_tridag_block_kernel(int64_t rows, int 
     for (int64_t k = (n4 << 2) + lane; k < n; k += 32) __stcs(dst + k, sy[k]);
   } else {
     for (int64_t k = lane; k < n; k += 32) __stcs(dst + k, sy[k]);
+  }
+}
+
+// Streaming kernel for tridagPar (FORM 1 of the block kernel): one warp per
+// 32 consecutive systems, lane = system, as the block kernel, but the four
+// input rows are not staged whole.  They pass through a double-buffered
+// window of kTriWin columns (cp.async, 4-byte copies: 8 lanes cover 8
+// consecutive columns of one row, so a warp's copy instruction reads 4 short
+// runs), and shared memory keeps only the two intermediates the backward
+// recurrence needs per row, b'_i and y'_i (c_i comes through the window a
+// second time, last column first) -- about 0.6 of the block kernel's
+// footprint, so more systems are in flight per SM.  The arithmetic and its
+// order are those of lvc_tridag_kernel (recurrences 1 and 2 fused into one
+// forward pass over i: each step reads only values the pass has already
+// produced).  The solution overwrites y'_i and leaves as the block kernel's
+// does.  (The same streaming for tridagSeq measured 4 % slower than the
+// block kernel, whose in-place intermediates need no second pass over c.)
+constexpr int kTriWin = 8;
+
+__device__ __forceinline__ void cp_async4(float* dst, const float* src, bool valid) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(smem_u32(dst)), "l"(src),
+               "r"(valid ? 4 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// Shared floats per warp: the two row arrays (row stride m | 1: lane = row
+// reads conflict-free) and 2 windows x 4 arrays x 32 rows x (kTriWin + 1).
+__host__ __device__ __forceinline__ int tri_stream_ld(int m) { return m | 1; }
+__host__ __device__ __forceinline__ int64_t tri_stream_floats(int m) {
+  return 2LL * 32 * tri_stream_ld(m) + 2LL * 4 * 32 * (kTriWin + 1);
+}
+
+__global__ void __launch_bounds__(32) lvc_tridag_stream_kernel(int64_t rows, int m, const float* __restrict__ a,
+                                                              const float* __restrict__ b,
+                                                              const float* __restrict__ c,
+                                                              const float* __restrict__ y,
+                                                              float* __restrict__ out) {
+  extern __shared__ __align__(16) float tri_s[];
+  const int lane = threadIdx.x;
+  const int64_t r0 = (int64_t)blockIdx.x * 32;
+  const int nr = (int)(rows - r0 < 32 ? rows - r0 : 32);
+  const int ld = tri_stream_ld(m);
+  float* P = tri_s;            // b'_i, [32][ld]
+  float* Q = P + 32 * ld;      // y'_i, then x_i
+  float* Wn = Q + 32 * ld;     // [2][4][32][kTriWin + 1]
+  constexpr int WS = kTriWin + 1, WA = 32 * WS, WB = 4 * WA;
+  const float* src[4] = {a, b, c, y};
+  const int nq = (m + kTriWin - 1) / kTriWin;
+  // chunk q of the arrays in `mask` into window buffer `buf`: 8 lanes per row
+  // segment, 4 rows per copy instruction
+  auto fetch = [&](int q, int buf, int mask) {
+#pragma unroll
+    for (int arr = 0; arr < 4; arr++) {
+      if (!((mask >> arr) & 1)) continue;
+#pragma unroll
+      for (int t = 0; t < 32 * kTriWin / 32; t++) {
+        const int idx = t * 32 + lane, row = idx / kTriWin, col = idx % kTriWin;
+        const int gcol = q * kTriWin + col;
+        const bool valid = row < nr && gcol < m;
+        const float* g = valid ? src[arr] + (r0 + row) * (int64_t)m + gcol : src[arr];
+        cp_async4(Wn + buf * WB + arr * WA + row * WS + col, g, valid);
+      }
+    }
+    cp_async_commit();
+  };
+  // Recurrences 1 and 2 in one forward pass: b'_i from the 4-tuple scan of
+  // (b_i, -a_i c_{i-1}, 1, 0), then y'_i from the 2-tuple scan of
+  // (y_i, -a_i / b'_{i-1}); both as lvc_tridag_kernel computes them.
+  float s0 = 1.0f, s1 = 0.0f, s2 = 0.0f, s3 = 1.0f, b0 = 0.0f, cprev = 0.0f;
+  float y0 = 0.0f, c0 = 0.0f, c1 = 1.0f, bprev = 0.0f;
+  fetch(0, 0, 15);
+  for (int q = 0; q < nq; q++) {
+    if (q + 1 < nq) {
+      fetch(q + 1, (q + 1) & 1, 15);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncwarp();
+    const float* w = Wn + (q & 1) * WB + lane * WS;
+    if (lane < nr) {
+#pragma unroll
+      for (int k = 0; k < kTriWin; k++) {
+        const int i = q * kTriWin + k;
+        if (i < m) {
+          const float ai = w[k], bi = w[WA + k], ci = w[2 * WA + k], yi = w[3 * WA + k];
+          if (i == 0) {
+            b0 = bi;
+            y0 = yi;
+          }
+          float m0 = 1.0f, m1 = 0.0f, m2 = 0.0f, m3 = 1.0f;
+          if (0 < i) {
+            m0 = bi;
+            m1 = tri_sub(0.0f, tri_mul(ai, cprev));
+            m2 = 1.0f;
+            m3 = 0.0f;
+          }
+          cprev = ci;
+          const float value = tri_rcp(tri_mul(s0, m0));
+          const float n0 = tri_mul(tri_add(tri_mul(m0, s0), tri_mul(m1, s2)), value);
+          const float n1 = tri_mul(tri_add(tri_mul(m0, s1), tri_mul(m1, s3)), value);
+          const float n2 = tri_mul(tri_add(tri_mul(m2, s0), tri_mul(m3, s2)), value);
+          const float n3 = tri_mul(tri_add(tri_mul(m2, s1), tri_mul(m3, s3)), value);
+          s0 = n0;
+          s1 = n1;
+          s2 = n2;
+          s3 = n3;
+          const float bpi = tri_div(tri_add(tri_mul(s0, b0), s1), tri_add(tri_mul(s2, b0), s3));  // b'_i
+          float l0 = 0.0f, l1 = 1.0f;
+          if (0 < i) {
+            l0 = yi;
+            l1 = tri_sub(0.0f, tri_div(ai, bprev));
+          }
+          const float e0 = tri_add(l0, tri_mul(l1, c0));
+          const float e1 = tri_mul(c1, l1);
+          c0 = e0;
+          c1 = e1;
+          P[lane * ld + i] = bpi;
+          Q[lane * ld + i] = tri_add(c0, tri_mul(c1, y0));  // y'_i
+          bprev = bpi;
+        }
+      }
+    }
+    __syncwarp();
+  }
+  // Recurrence 3, backward, with c_i through the window again (last chunk first)
+  float yn = 0.0f;
+  if (lane < nr) yn = tri_div(Q[lane * ld + m - 1], P[lane * ld + m - 1]);
+  c0 = 0.0f;
+  c1 = 1.0f;
+  fetch(nq - 1, 0, 4);
+  for (int qq = 0; qq < nq; qq++) {
+    const int q = nq - 1 - qq;
+    if (qq + 1 < nq) {
+      fetch(q - 1, (qq + 1) & 1, 4);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncwarp();
+    const float* w = Wn + (qq & 1) * WB + lane * WS;
+    if (lane < nr) {
+#pragma unroll
+      for (int kk = kTriWin - 1; kk >= 0; kk--) {
+        const int i = q * kTriWin + kk;
+        if (i < m) {
+          float l0 = 0.0f, l1 = 1.0f;
+          if (i < m - 1) {
+            const float bi = P[lane * ld + i];
+            l0 = tri_div(Q[lane * ld + i], bi);
+            l1 = tri_sub(0.0f, tri_div(w[2 * WA + kk], bi));
+          }
+          const float n0 = tri_add(l0, tri_mul(l1, c0));
+          const float n1 = tri_mul(c1, l1);
+          c0 = n0;
+          c1 = n1;
+          Q[lane * ld + i] = tri_add(c0, tri_mul(c1, yn));
+        }
+      }
+    }
+    __syncwarp();
+  }
+  __syncwarp();
+  // the solution rows (Q, stride ld) to out, consecutive lanes on consecutive elements
+  float* dst = out + r0 * (int64_t)m;
+  const int64_t n = (int64_t)nr * m;
+  if (ld == m) {
+    for (int64_t e = lane; e < n; e += 32) __stcs(dst + e, Q[e]);
+  } else {
+    for (int64_t e = lane; e < n; e += 32) {
+      const int rr = (int)(e / m), cc = (int)(e - (int64_t)rr * m);
+      __stcs(dst + e, Q[rr * ld + cc]);
+    }
   }
 }
 
