@@ -429,7 +429,9 @@ def run_op(args):
     (finpar/OptionPricing-data, kept as fixtures under tests/golden): device
     time per pricing through op_price_f32 with the inputs resident, end to end
     through futhark_entry_main with host arrays, agreement with the golden
-    outputs and the oracle, CPU baseline (the oracle on all host threads, a
+    outputs and the oracle, the same in the reference's reduction order (an f32
+    running sum over paths, bit-exact against the golden outputs where the
+    oracle in that order is), CPU baseline (the oracle on all host threads, a
     bounded number of paths)."""
     import numpy as np
     import torch
@@ -479,6 +481,31 @@ def run_op(args):
             oracle.option_pricing_sums(*ins, count=sample, threads=threads)
             cpu_s = time.perf_counter() - t0
             want = oracle.option_pricing(*ins, threads=threads)
+            # the reference's own reduction order (an f32 running sum over the
+            # paths in path order), which reproduces the golden outputs
+            octx.set_reduction_order(octx.ORDER_SEQUENTIAL_F32)
+            scratch_r = torch.empty(octx.scratch_bytes(contract, paths, dims), dtype=torch.uint8, device="cuda")
+            out_r = torch.empty_like(out)
+            for _ in range(max(3, args.warmup)):
+                octx.price(contract, paths, dims, ptrs, out_r.data_ptr(), scratch_r.data_ptr())
+            octx.check()
+            times_r = []
+            for _ in range(max(5, args.steps)):
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(ext)
+                octx.price(contract, paths, dims, ptrs, out_r.data_ptr(), scratch_r.data_ptr())
+                e1.record(ext)
+                octx.check()
+                times_r.append(e0.elapsed_time(e1))
+            got_r = out_r.cpu().numpy()
+            octx.set_reduction_order(octx.ORDER_F64)
+            ms_r = float(np.median(times_r))
+            ref_order = {"device_ms": ms_r, "paths_per_s": paths / (ms_r * 1e-3), "price": float(got_r[0]),
+                         "bit_exact_vs_golden": bool(np.array_equal(got_r.view(np.uint32),
+                                                                    golden.astype(np.float32).view(np.uint32))),
+                         "rel_vs_golden": float(abs(got_r[0] - golden[0]) / abs(golden[0]))}
+            del scratch_r, out_r
             res["datasets"][name] = {
                 "contract": contract, "paths": paths, "dates_x_underlyings": [dims["num_dates"], dims["num_und"]],
                 "device_ms": ms, "paths_per_s": paths / (ms * 1e-3), "e2e_ms": e2e_ms,
@@ -486,6 +513,7 @@ def run_op(args):
                 "rel_vs_golden": float(abs(got[0] - golden[0]) / abs(golden[0])),
                 "rel_vs_oracle": float(abs(got[0] - want[0]) / abs(want[0])),
                 "e2e_equals_device": bool(np.array_equal(e2e, got)),
+                "reference_order": ref_order,
                 "cpu_baseline": {"value": sample / cpu_s, "unit": "paths/s", "cores": threads, "kind": "port",
                                  "sample": f"{sample} of the {paths} paths, oracle"}}
             del dev, out, scratch
