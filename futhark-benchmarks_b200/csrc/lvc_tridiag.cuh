@@ -289,7 +289,7 @@ __global__ void __launch_bounds__(32) lvc_tridag_block_kernel(int64_t rows, int 
   }
 }
 
-// Streaming kernel for tridagPar (FORM 1 of the block kernel): one warp per
+// Streaming kernel for tridagPar (FORM 1 of lvc_tridag_kernel): one warp per
 // 32 consecutive systems, lane = system, as the block kernel, but the four
 // input rows are not staged whole.  They pass through a double-buffered
 // window of kTriWin columns (cp.async, 4-byte copies: 8 lanes cover 8
