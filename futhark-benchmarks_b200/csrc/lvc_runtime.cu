@@ -2546,8 +2546,9 @@ namespace {
 constexpr int64_t kTridagInnerDim = 115;  // INNER_DIM of tridiag-test.fut:4
 
 // Enqueues one batched solve on ctx->stream (device pointers).  Called with
-// ctx->mu held.  m <= 400: the block kernel (tridagSeq) or the streaming
-// kernel (tridagPar), no scratch; larger m: scratch
+// ctx->mu held.  m <= 128: the tensor-memory kernel; m <= 400: the block
+// kernel (tridagSeq) or the streaming kernel (tridagPar), no scratch; larger
+// m: scratch
 // from the context's device pool (stream-ordered: every user of that pool
 // runs on ctx->stream).
 int tridag_check_locked(futhark_context* ctx) {
@@ -2566,6 +2567,17 @@ int tridag_launch(futhark_context* ctx, int form, int64_t rows, int64_t m, const
                   const float* c, const float* y, float* out) {
   if (rows < 0 || m < 0 || m > INT32_MAX) return set_error(ctx, FUTHARK_PROGRAM_ERROR, "bad tridiagonal batch shape");
   if (rows == 0 || m == 0) return 0;
+  if (m <= kTriTmemMaxM) {  // intermediates in tensor memory, four warps per CTA
+    const int64_t nblk = (rows + 32 * kTriTmemWarps - 1) / (32 * kTriTmemWarps);
+    if (nblk > INT32_MAX) return set_error(ctx, FUTHARK_PROGRAM_ERROR, "tridiagonal batch too large");
+    auto fk = form == 0 ? lvc_tridag_tmem_kernel<0> : lvc_tridag_tmem_kernel<1>;
+    LVC_CUDA(ctx, cudaFuncSetAttribute((const void*)fk, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)tri_tmem_smem()));
+    fk<<<(unsigned)nblk, 32 * kTriTmemWarps, tri_tmem_smem(), ctx->stream>>>(rows, (int)m, a, b, c, y, out);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "tridiagonal launch");
+    return 0;
+  }
   if (m <= kTriBlockMaxM && form == 1) {  // tridagPar: inputs streamed through shared memory
     const int64_t nblk = (rows + 31) / 32;
     if (nblk > INT32_MAX) return set_error(ctx, FUTHARK_PROGRAM_ERROR, "tridiagonal batch too large");

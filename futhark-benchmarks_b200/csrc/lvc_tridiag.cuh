@@ -7,11 +7,14 @@
 //           4-tuple matrix scan for the pivots, two linear-function scans --
 //           folded left to right.
 //
-// Three kernels, one thread per system in each: for m up to 400 (the common
-// case) lvc_tridag_block_kernel (FORM 0) stages a warp's 32 systems through
-// shared memory with bulk copies and lvc_tridag_stream_kernel (FORM 1)
-// streams them through a window of columns; lvc_tridag_kernel (any m, both
-// forms) reads rows in place.
+// Four kernels, one thread per system in each: for m up to 128 (the
+// benchmark's 115 among them) lvc_tridag_tmem_kernel (both forms) streams a
+// warp's 32 systems through shared-memory windows and keeps the row
+// intermediates in tensor memory; for m up to 400 lvc_tridag_block_kernel
+// (FORM 0) stages the rows through shared memory with bulk copies and
+// lvc_tridag_stream_kernel (FORM 1) streams them and keeps the intermediates
+// in shared memory; lvc_tridag_kernel (any m, both forms) reads rows in
+// place.
 // Each recurrence runs in the reference's operation
 // order with every product, sum and quotient explicitly rounded (no fused
 // multiply-add), so a system's solution is bit for bit the one the CPU
@@ -463,6 +466,253 @@ __global__ void __launch_bounds__(32) lvc_tridag_stream_kernel(int64_t rows, int
       __stcs(dst + e, Q[rr * ld + cc]);
     }
   }
+}
+
+// ---------------------------------------------------------------------------
+// Tensor-memory kernel (m <= 128): the row intermediates live in TMEM.
+// ---------------------------------------------------------------------------
+// The streaming kernels above are bound by the latency of each system's
+// sequential chain at the few warps per SM that shared memory leaves them
+// (the four input rows, or two intermediate rows, of 32 systems per warp).
+// Here the intermediates go to tensor memory instead -- 256 KB per SM that
+// nothing else of this library uses: thread t of a warp owns TMEM lane
+// 32 (warp % 4) + t of its CTA's allocation, and the two 32-bit values of
+// element i (FORM 0: cp_i, yp_i; FORM 1: the quotients y'_i / b'_i and
+// -c_i / b'_i that the backward recurrence folds) sit in columns 2i, 2i + 1,
+// written and read as 16-column rows by tcgen05.st / tcgen05.ld, one per
+// window of eight elements.  Shared memory keeps only the input ring (three
+// stages of kTriWin-column windows of the four inputs, cp.async) and an
+// output window, so a 4-warp CTA needs 256 TMEM columns and 60 KB: two CTAs,
+// eight warps, per SM (the shared-memory request is padded to 80 KB so that
+// no third CTA waits in tcgen05.alloc).  The arithmetic and its order are
+// lvc_tridag_kernel's, with FORM 1's three recurrences fused into the
+// forward pass and the backward fold.
+constexpr int kTriTmemWarps = 4;
+constexpr int kTriTmemCols = 256;  // TMEM columns per CTA: 16 per window, at most 16 windows
+constexpr int kTriTmemMaxM = 128;
+constexpr int kTriTmemStages = 3;
+__host__ __device__ __forceinline__ size_t tri_tmem_smem() {
+  const size_t need = 16 + sizeof(float) * kTriTmemWarps * (kTriTmemStages * 4 * 32 * (kTriWin + 1) + 32 * (kTriWin + 1));
+  return need > 80 * 1024 ? need : 80 * 1024;
+}
+
+__device__ __forceinline__ void tmem_alloc(uint32_t* dst, int ncols) {  // whole warp
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(dst)), "r"(ncols)
+               : "memory");
+}
+__device__ __forceinline__ void tmem_relinquish() {  // whole warp
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, int ncols) {  // whole warp
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(taddr), "r"(ncols) : "memory");
+}
+__device__ __forceinline__ void tmem_fence_before_sync() {
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+}
+__device__ __forceinline__ void tmem_fence_after_sync() {
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+}
+// 16 consecutive 32-bit columns of this thread's lane (whole warp)
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const float (&v)[16]) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15, %16};\n" ::"r"(taddr),
+      "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])), "r"(__float_as_uint(v[3])),
+      "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])), "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7])),
+      "r"(__float_as_uint(v[8])), "r"(__float_as_uint(v[9])), "r"(__float_as_uint(v[10])),
+      "r"(__float_as_uint(v[11])), "r"(__float_as_uint(v[12])), "r"(__float_as_uint(v[13])),
+      "r"(__float_as_uint(v[14])), "r"(__float_as_uint(v[15]))
+      : "memory");
+}
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;\n" ::: "memory"); }
+// the load and its wait in one statement, so no use of the values can be
+// scheduled before they have arrived (whole warp)
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15}, [%16];\n"
+      "tcgen05.wait::ld.sync.aligned;\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr)
+      : "memory");
+#pragma unroll
+  for (int k = 0; k < 16; k++) v[k] = __uint_as_float(r[k]);
+}
+
+template <int FORM>
+__global__ void __launch_bounds__(32 * kTriTmemWarps) lvc_tridag_tmem_kernel(int64_t rows, int m,
+                                                                             const float* __restrict__ a,
+                                                                             const float* __restrict__ b,
+                                                                             const float* __restrict__ c,
+                                                                             const float* __restrict__ y,
+                                                                             float* __restrict__ out) {
+  extern __shared__ __align__(16) unsigned char tri_raw[];
+  constexpr int WS = kTriWin + 1, WA = 32 * WS, WB = 4 * WA;
+  uint32_t* s_taddr = reinterpret_cast<uint32_t*>(tri_raw);  // written by tcgen05.alloc
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float* const Wn = reinterpret_cast<float*>(tri_raw + 16) + warp * (kTriTmemStages * WB + WA);  // input ring
+  float* const Wo = Wn + kTriTmemStages * WB;                                                    // output window
+  const int64_t r0 = ((int64_t)blockIdx.x * kTriTmemWarps + warp) * 32;
+  // a warp past the last system still takes part in the CTA's allocation
+  // and release of tensor memory
+  const int nr = r0 < rows ? (int)(rows - r0 < 32 ? rows - r0 : 32) : 0;
+  if (warp == 0) {
+    tmem_alloc(s_taddr, kTriTmemCols);
+    tmem_relinquish();
+  }
+  tmem_fence_before_sync();
+  __syncthreads();
+  tmem_fence_after_sync();
+  const uint32_t tl = *s_taddr + ((uint32_t)(32 * (warp & 3)) << 16);  // this warp's lane quarter, column 0
+  if (nr > 0) {
+    const float* src[4] = {a, b, c, y};
+    const int nq = (m + kTriWin - 1) / kTriWin;
+    const bool act = lane < nr;
+    auto fetch = [&](int q) {
+      if (q < nq) {
+        float* const dst = Wn + (q % kTriTmemStages) * WB;
+#pragma unroll
+        for (int arr = 0; arr < 4; arr++) {
+#pragma unroll
+          for (int t = 0; t < kTriWin; t++) {
+            const int idx = t * 32 + lane, row = idx / kTriWin, col = idx % kTriWin;
+            const int gcol = q * kTriWin + col;
+            const bool valid = row < nr && gcol < m;
+            const float* g = valid ? src[arr] + (r0 + row) * (int64_t)m + gcol : src[arr];
+            cp_async4(dst + arr * WA + row * WS + col, g, valid);
+          }
+        }
+      }
+      cp_async_commit();
+    };
+    // -------- forward --------
+    float cp = 0.0f, yp = 0.0f;                                               // FORM 0
+    float s0 = 1.0f, s1 = 0.0f, s2 = 0.0f, s3 = 1.0f, b0 = 0.0f, cprev = 0.0f;  // FORM 1
+    float y0 = 0.0f, c0 = 0.0f, c1 = 1.0f, bprev = 0.0f, yn = 0.0f;
+    fetch(0);
+    fetch(1);
+    for (int q = 0; q < nq; q++) {
+      fetch(q + 2);
+      cp_async_wait<2>();  // window q has landed
+      __syncwarp();
+      const float* w = Wn + (q % kTriTmemStages) * WB + lane * WS;
+      float v[16];
+#pragma unroll
+      for (int k = 0; k < kTriWin; k++) {
+        const int i = q * kTriWin + k;
+        v[2 * k] = 0.0f;
+        v[2 * k + 1] = 0.0f;
+        if (act && i < m) {
+          const float ai = w[k], bi = w[WA + k], ci = w[2 * WA + k], yi = w[3 * WA + k];
+          if constexpr (FORM == 0) {
+            // cp_i = c_i / (b_i - a_i cp_{i-1}), yp_i = (y_i - a_i yp_{i-1}) / (...)  (:82-91)
+            if (i == 0) {
+              cp = tri_div(ci, bi);
+              yp = tri_div(yi, bi);
+            } else {
+              const float nf = tri_rcp(tri_sub(bi, tri_mul(ai, cp)));
+              cp = tri_mul(ci, nf);
+              yp = tri_mul(tri_sub(yi, tri_mul(ai, yp)), nf);
+            }
+            v[2 * k] = cp;
+            v[2 * k + 1] = yp;
+          } else {
+            // recurrence 1 (:9-33): b'_i from the 4-tuple scan of (b_i, -a_i c_{i-1}, 1, 0)
+            if (i == 0) {
+              b0 = bi;
+              y0 = yi;
+            }
+            float m0 = 1.0f, m1 = 0.0f, m2 = 0.0f, m3 = 1.0f;
+            if (0 < i) {
+              m0 = bi;
+              m1 = tri_sub(0.0f, tri_mul(ai, cprev));
+              m2 = 1.0f;
+              m3 = 0.0f;
+            }
+            cprev = ci;
+            const float value = tri_rcp(tri_mul(s0, m0));
+            const float n0 = tri_mul(tri_add(tri_mul(m0, s0), tri_mul(m1, s2)), value);
+            const float n1 = tri_mul(tri_add(tri_mul(m0, s1), tri_mul(m1, s3)), value);
+            const float n2 = tri_mul(tri_add(tri_mul(m2, s0), tri_mul(m3, s2)), value);
+            const float n3 = tri_mul(tri_add(tri_mul(m2, s1), tri_mul(m3, s3)), value);
+            s0 = n0;
+            s1 = n1;
+            s2 = n2;
+            s3 = n3;
+            const float bpi = tri_div(tri_add(tri_mul(s0, b0), s1), tri_add(tri_mul(s2, b0), s3));  // b'_i
+            // recurrence 2 (:38-56): y'_i from the scan of (y_i, -a_i / b'_{i-1})
+            float l0 = 0.0f, l1 = 1.0f;
+            if (0 < i) {
+              l0 = yi;
+              l1 = tri_sub(0.0f, tri_div(ai, bprev));
+            }
+            const float e0 = tri_add(l0, tri_mul(l1, c0));
+            const float e1 = tri_mul(c1, l1);
+            c0 = e0;
+            c1 = e1;
+            const float ypi = tri_add(c0, tri_mul(c1, y0));  // y'_i
+            bprev = bpi;
+            // recurrence 3's elements (:61-79), the last one's first component
+            // its starting value
+            if (i < m - 1) {
+              v[2 * k] = tri_div(ypi, bpi);
+              v[2 * k + 1] = tri_sub(0.0f, tri_div(ci, bpi));
+            } else {
+              yn = tri_div(ypi, bpi);
+            }
+          }
+        }
+      }
+      tmem_st16(tl + 16 * q, v);
+      __syncwarp();  // this ring stage is refilled by the next iteration's fetch
+    }
+    cp_async_wait<0>();
+    tmem_wait_st();
+    // -------- backward --------
+    float x = yp;  // FORM 0: x_{m-1} = yp_{m-1}
+    c0 = 0.0f;
+    c1 = 1.0f;
+    for (int q = nq - 1; q >= 0; q--) {
+      float v[16];
+      tmem_ld16(tl + 16 * q, v);
+#pragma unroll
+      for (int k = kTriWin - 1; k >= 0; k--) {
+        const int i = q * kTriWin + k;
+        if (act && i < m) {
+          if constexpr (FORM == 0) {
+            // x_i = yp_i - cp_i x_{i+1}  (:92-95)
+            if (i < m - 1) x = tri_sub(v[2 * k + 1], tri_mul(v[2 * k], x));
+            Wo[lane * WS + k] = x;
+          } else {
+            float l0 = 0.0f, l1 = 1.0f;
+            if (i < m - 1) {
+              l0 = v[2 * k];
+              l1 = v[2 * k + 1];
+            }
+            const float n0 = tri_add(l0, tri_mul(l1, c0));
+            const float n1 = tri_mul(c1, l1);
+            c0 = n0;
+            c1 = n1;
+            Wo[lane * WS + k] = tri_add(c0, tri_mul(c1, yn));
+          }
+        }
+      }
+      __syncwarp();
+#pragma unroll
+      for (int t = 0; t < kTriWin; t++) {
+        const int idx = t * 32 + lane, row = idx / kTriWin, col = idx % kTriWin;
+        const int gcol = q * kTriWin + col;
+        if (row < nr && gcol < m) __stcs(out + (r0 + row) * (int64_t)m + gcol, Wo[row * WS + col]);
+      }
+      __syncwarp();  // the output window is rewritten next iteration
+    }
+  }
+  tmem_fence_before_sync();
+  __syncthreads();
+  tmem_fence_after_sync();
+  if (warp == 0) tmem_dealloc(*s_taddr, kTriTmemCols);
 }
 
 }  // namespace lvc

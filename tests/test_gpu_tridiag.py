@@ -41,11 +41,12 @@ def test_par_matches_oracle_bit_exact_on_golden_inputs(ctx, oracle, golden_tridi
     assert np.array_equal(got, oracle.tridag(z["a"], z["b"], z["c"], z["y"], form="par4"))
 
 
-# (rows, m): empty, single-element systems, partial warps, the stanza's inner
-# size, odd and even m, the block kernel's limit (400) and the kernel with
-# global scratch above it
-@pytest.mark.parametrize("shape", [(0, 5), (3, 1), (7, 2), (33, 3), (129, 64), (1000, 115), (70, 399),
-                                   (130, 400), (40, 401), (5, 1000)])
+# (rows, m): empty, single-element systems, partial warps and CTAs, the
+# stanza's inner size, the tensor-memory kernel's limit (128) and just above
+# it, odd and even m, the shared-memory kernels' limit (400) and the kernel
+# with global scratch above it
+@pytest.mark.parametrize("shape", [(0, 5), (3, 1), (7, 2), (33, 3), (129, 64), (1000, 115), (257, 128),
+                                   (65, 129), (70, 399), (130, 400), (40, 401), (5, 1000)])
 @pytest.mark.parametrize("form,oform", [("seq", "seq"), ("par", "par4")])
 def test_random_batches_match_oracle_bit_exact(ctx, oracle, shape, form, oform):
     rows, m = shape
@@ -84,11 +85,13 @@ def test_device_pointer_form_matches_entry_point(ctx, oracle):
         assert np.array_equal(out.cpu().numpy(), oracle.tridag(*host, form=oform))
 
 
-def test_device_pointer_form_with_unaligned_arrays(ctx, oracle):
-    # device arrays that start 4 bytes past a 16-byte boundary take the
-    # scalar copy path of the block kernel
+@pytest.mark.parametrize("m", [115, 200])
+def test_device_pointer_form_with_unaligned_arrays(ctx, oracle, m):
+    # device arrays that start 4 bytes past a 16-byte boundary: 4-byte copies
+    # in the tensor-memory kernel (m <= 128), the scalar copy path of the
+    # block kernel above it
     import torch
-    rows, m = 100, 115
+    rows = 100
     host = wl.tridiag_inputs(rows, m, seed=12)
     dev = []
     for v in host:
