@@ -11,11 +11,12 @@
 // done.
 //   tke_advect_kernel  the advection fluxes east, north and top
 //                      (tke.fut:264-319) and dtketau (:320-340).  A thread
-//                      owns one (y, z) of the plane and marches along x over
-//                      a segment, carrying the east flux of x - 1 in a
-//                      register; the north flux of y - 1 and the top flux of
-//                      z - 1 come from the neighbouring threads through shared
-//                      memory, so each flux is evaluated about once.
+//                      owns one (y, z) of a (y, z) tile of the plane and
+//                      marches along x over a segment, carrying the east flux
+//                      of x - 1 in a register; the north flux of y - 1 and the
+//                      top flux of z - 1 come from the neighbouring threads
+//                      through shared memory, so each flux is evaluated about
+//                      once.
 //   tke_column_kernel  everything else, one lane per (x, y) column, a warp per
 //                      32 consecutive columns: the coefficients (:103-210) and
 //                      tridagPar's two forward recurrences
@@ -157,26 +158,33 @@ __device__ __forceinline__ float adv_top(const TkeArgs& p, int x, int y, int z) 
 // ---------------------------------------------------------------------------
 constexpr int kAdvThreads = 256;  // at <= 64 registers two CTAs fit beside two column-kernel CTAs
 
-// Block b.x covers kAdvThreads consecutive (y, z) of the plane (z fastest),
-// block b.y the x segment [b.y * xseg, ...).  A thread keeps tketau and maskW
-// of x - 1 .. x + 2 at its (y, z) in registers (the east flux, :264-281) and
-// publishes those of x in shared memory, where its neighbours (y +- 1, y + 2)
-// and (z +- 1, z + 2) read them for the north (:282-299) and top (:300-319)
-// fluxes -- from global memory where the neighbour is outside the block.  The
-// north flux of (y - 1, z) is thread t - zdim's and the top flux of
-// (y, z - 1) thread t - 1's, again through shared memory; the first zdim
-// threads (resp. thread 0) evaluate that neighbour's flux themselves.
-__global__ void __launch_bounds__(kAdvThreads, 4) tke_advect_kernel(TkeArgs p, int xseg) {
+// Block b.x covers a tile of ty rows (y) x tz levels (z) of the plane --
+// thread t at (t / tz, t % tz), z fastest, ty * tz <= kAdvThreads, the z
+// extent split into nzt tiles of at most 32 -- and block b.y the x segment
+// [b.y * xseg, ...).  A thread keeps tketau and maskW of x - 1 .. x + 2 at
+// its (y, z) in registers (the east flux, :264-281) and publishes those of x
+// in shared memory, where its neighbours (y +- 1, y + 2) and (z +- 1, z + 2)
+// read them for the north (:282-299) and top (:300-319) fluxes -- from
+// global memory where the neighbour is outside the tile.  The north flux of
+// (y - 1, z) is thread t - tz's and the top flux of (y, z - 1) thread
+// t - 1's, again through shared memory; the tile's first row (resp. first
+// level) evaluates that neighbour's flux itself.  Tiles (rather than runs of
+// consecutive (y, z)) keep most north neighbours in the block when zdim is
+// large: with zdim = 100, 2.56 rows of 256 threads held none of them.
+__global__ void __launch_bounds__(kAdvThreads, 4) tke_advect_kernel(TkeArgs p, int xseg, int ty, int tz, int nzt) {
   __shared__ float sT[kAdvThreads], sW[kAdvThreads], sfn[kAdvThreads], sft[kAdvThreads];
   const int t = threadIdx.x;
   const int64_t plane = (int64_t)p.Y * p.Z;
-  const int64_t qi = (int64_t)blockIdx.x * kAdvThreads + t;
-  const bool live = qi < plane;
   const int Z = p.Z;
-  const int y = live ? (int)(qi / Z) : 0, z = live ? (int)(qi % Z) : 0;
+  const int ry = t / tz, rz = t - ry * tz;  // position in the tile
+  const int yt = blockIdx.x / nzt, zt = blockIdx.x - yt * nzt;
+  const int yy = yt * ty + ry, zz = zt * tz + rz;
+  const bool live = ry < ty && yy < p.Y && zz < Z;
+  const int y = live ? yy : 0, z = live ? zz : 0;
+  const int64_t qi = (int64_t)y * Z + z;
   const int xs = blockIdx.y * xseg, xe = min(p.X, xs + xseg);
-  const bool n_in = t - Z >= 0 && t + 2 * Z < kAdvThreads;  // (y - 1 .. y + 2, z) in this block
-  const bool t_in = t >= 1 && t + 2 < kAdvThreads;           // (y, z - 1 .. z + 2) in this block
+  const bool n_in = ry >= 1 && ry + 2 < ty;  // (y - 1 .. y + 2, z) in this tile
+  const bool t_in = rz >= 1 && rz + 2 < tz;  // (y, z - 1 .. z + 2) in this tile
   const bool yint = y >= 2 && y < p.Y - 2;
   const float cy = live ? p.cost[y] : 1.0f, cuy = live ? p.cosu[y] : 1.0f, dyt = live ? p.dyt[y] : 1.0f;
   const float dz = live ? p.dzw[z] : 1.0f;
@@ -202,12 +210,12 @@ __global__ void __launch_bounds__(kAdvThreads, 4) tke_advect_kernel(TkeArgs p, i
       if (y >= 1 && y < p.Y - 2 && xint) {
         float tm, tp1, tp2, wm, wp1, wp2;
         if (n_in) {
-          tm = sT[t - Z];
-          tp1 = sT[t + Z];
-          tp2 = sT[t + 2 * Z];
-          wm = sW[t - Z];
-          wp1 = sW[t + Z];
-          wp2 = sW[t + 2 * Z];
+          tm = sT[t - tz];
+          tp1 = sT[t + tz];
+          tp2 = sT[t + 2 * tz];
+          wm = sW[t - tz];
+          wp1 = sW[t + tz];
+          wp2 = sW[t + 2 * tz];
         } else {
           tm = p.tketau[i - Z];
           tp1 = p.tketau[i + Z];
@@ -252,8 +260,8 @@ __global__ void __launch_bounds__(kAdvThreads, 4) tke_advect_kernel(TkeArgs p, i
     sft[t] = ft;
     __syncthreads();
     if (live) {  // dtketau (:320-340)
-      const float fnm = t >= Z ? sfn[t - Z] : (y >= 1 ? adv_north(p, x, y - 1, z) : 0.0f);
-      const float ftm = t >= 1 ? sft[t - 1] : (z >= 1 ? adv_top(p, x, y, z - 1) : 0.0f);
+      const float fnm = ry >= 1 ? sfn[t - tz] : (y >= 1 ? adv_north(p, x, y - 1, z) : 0.0f);
+      const float ftm = rz >= 1 ? sft[t - 1] : (z >= 1 ? adv_top(p, x, y, z - 1) : 0.0f);
       float tmp;
       if (x >= 2 && x < p.X - 2 && yint)
         tmp = M_(W1, S_(D_(-S_(fe, fe_prev), M_(cy, p.dxt[x])), D_(S_(fn, fnm), M_(cy, dyt))));
@@ -638,15 +646,18 @@ int step_launch(futhark_context* ctx, const tke_step_args* q) {
   tke_column_kernel<<<(unsigned)col_blocks, 32 * kColWarps, kColSmem, s>>>(p);
   e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(ctx, e, "tke column launch");
-  // advection and dtketau: x segments so that about four waves of CTAs run
-  const int64_t plane_blocks = (Y * Z + kAdvThreads - 1) / kAdvThreads;
+  // advection and dtketau: (y, z) tiles of at most 32 levels, x segments so
+  // that about four waves of CTAs run
+  const int64_t nzt = (Z + 31) / 32, tz = (Z + nzt - 1) / nzt, ty = kAdvThreads / tz;
+  const int64_t plane_blocks = ((Y + ty - 1) / ty) * nzt;
   const int64_t want_blocks = 4LL * 4 * ctx->num_sms;  // four CTAs per SM
   const int64_t nseg = std::max<int64_t>(1, std::min<int64_t>(X, (want_blocks + plane_blocks - 1) / plane_blocks));
   const int xseg = (int)((X + nseg - 1) / nseg);
   const int64_t segs = (X + xseg - 1) / xseg;
   if (plane_blocks > INT32_MAX || segs > 65535)
     return set_error(ctx, FUTHARK_PROGRAM_ERROR, "tke step: plane too large");
-  tke_advect_kernel<<<dim3((unsigned)plane_blocks, (unsigned)segs), kAdvThreads, 0, ctx->aux>>>(p, xseg);
+  tke_advect_kernel<<<dim3((unsigned)plane_blocks, (unsigned)segs), kAdvThreads, 0, ctx->aux>>>(p, xseg, (int)ty,
+                                                                                                (int)tz, (int)nzt);
   e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(ctx, e, "tke advection launch");
   e = cudaEventRecord(ctx->ev_join, ctx->aux);
