@@ -2546,7 +2546,7 @@ namespace {
 constexpr int64_t kTridagInnerDim = 115;  // INNER_DIM of tridiag-test.fut:4
 
 // Enqueues one batched solve on ctx->stream (device pointers).  Called with
-// ctx->mu held.  m <= 128: the tensor-memory kernel; m <= 400: the block
+// ctx->mu held.  m <= 256: the tensor-memory kernel; m <= 400: the block
 // kernel (tridagSeq) or the streaming kernel (tridagPar), no scratch; larger
 // m: scratch
 // from the context's device pool (stream-ordered: every user of that pool
@@ -2570,10 +2570,12 @@ int tridag_launch(futhark_context* ctx, int form, int64_t rows, int64_t m, const
   if (m <= kTriTmemMaxM) {  // intermediates in tensor memory, four warps per CTA
     const int64_t nblk = (rows + 32 * kTriTmemWarps - 1) / (32 * kTriTmemWarps);
     if (nblk > INT32_MAX) return set_error(ctx, FUTHARK_PROGRAM_ERROR, "tridiagonal batch too large");
-    auto fk = form == 0 ? lvc_tridag_tmem_kernel<0> : lvc_tridag_tmem_kernel<1>;
-    LVC_CUDA(ctx, cudaFuncSetAttribute((const void*)fk, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)tri_tmem_smem()));
-    fk<<<(unsigned)nblk, 32 * kTriTmemWarps, tri_tmem_smem(), ctx->stream>>>(rows, (int)m, a, b, c, y, out);
+    const int cols = tri_tmem_cols((int)m);
+    auto fk = cols == 256 ? (form == 0 ? lvc_tridag_tmem_kernel<0, 256> : lvc_tridag_tmem_kernel<1, 256>)
+                          : (form == 0 ? lvc_tridag_tmem_kernel<0, 512> : lvc_tridag_tmem_kernel<1, 512>);
+    const size_t smem = tri_tmem_smem(cols);
+    LVC_CUDA(ctx, cudaFuncSetAttribute((const void*)fk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    fk<<<(unsigned)nblk, 32 * kTriTmemWarps, smem, ctx->stream>>>(rows, (int)m, a, b, c, y, out);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(ctx, e, "tridiagonal launch");
     return 0;

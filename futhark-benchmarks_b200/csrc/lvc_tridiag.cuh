@@ -7,7 +7,7 @@
 //           4-tuple matrix scan for the pivots, two linear-function scans --
 //           folded left to right.
 //
-// Four kernels, one thread per system in each: for m up to 128 (the
+// Four kernels, one thread per system in each: for m up to 256 (the
 // benchmark's 115 among them) lvc_tridag_tmem_kernel (both forms) streams a
 // warp's 32 systems through shared-memory windows and keeps the row
 // intermediates in tensor memory; for m up to 400 lvc_tridag_block_kernel
@@ -469,7 +469,7 @@ __global__ void __launch_bounds__(32) lvc_tridag_stream_kernel(int64_t rows, int
 }
 
 // ---------------------------------------------------------------------------
-// Tensor-memory kernel (m <= 128): the row intermediates live in TMEM.
+// Tensor-memory kernel (m <= 256): the row intermediates live in TMEM.
 // ---------------------------------------------------------------------------
 // The streaming kernels above are bound by the latency of each system's
 // sequential chain at the few warps per SM that shared memory leaves them
@@ -482,18 +482,21 @@ __global__ void __launch_bounds__(32) lvc_tridag_stream_kernel(int64_t rows, int
 // written and read as 16-column rows by tcgen05.st / tcgen05.ld, one per
 // window of eight elements.  Shared memory keeps only the input ring (three
 // stages of kTriWin-column windows of the four inputs, cp.async) and an
-// output window, so a 4-warp CTA needs 256 TMEM columns and 60 KB: two CTAs,
-// eight warps, per SM (the shared-memory request is padded to 80 KB so that
-// no third CTA waits in tcgen05.alloc).  The arithmetic and its order are
-// lvc_tridag_kernel's, with FORM 1's three recurrences fused into the
-// forward pass and the backward fold.
+// output window, so a 4-warp CTA needs 60 KB and, for m <= 128, 256 TMEM
+// columns: two CTAs, eight warps, per SM; for m <= 256, 512 columns: one CTA
+// per SM.  The shared-memory request is padded (80 KB, 120 KB) so that no
+// further CTA fits and waits in tcgen05.alloc.  The arithmetic and its
+// order are lvc_tridag_kernel's, with FORM 1's three recurrences fused into
+// the forward pass and the backward fold.
 constexpr int kTriTmemWarps = 4;
-constexpr int kTriTmemCols = 256;  // TMEM columns per CTA: 16 per window, at most 16 windows
-constexpr int kTriTmemMaxM = 128;
+constexpr int kTriTmemMaxM = 256;  // 16 columns per window of 8: 512 columns
 constexpr int kTriTmemStages = 3;
-__host__ __device__ __forceinline__ size_t tri_tmem_smem() {
+// TMEM columns of a CTA for inner size m (a power of two, 256 or 512)
+__host__ __device__ __forceinline__ int tri_tmem_cols(int m) { return m <= 128 ? 256 : 512; }
+__host__ __device__ __forceinline__ size_t tri_tmem_smem(int cols) {
   const size_t need = 16 + sizeof(float) * kTriTmemWarps * (kTriTmemStages * 4 * 32 * (kTriWin + 1) + 32 * (kTriWin + 1));
-  return need > 80 * 1024 ? need : 80 * 1024;
+  const size_t pad = cols > 256 ? 120 * 1024 : 80 * 1024;
+  return need > pad ? need : pad;
 }
 
 __device__ __forceinline__ void tmem_alloc(uint32_t* dst, int ncols) {  // whole warp
@@ -541,7 +544,7 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
   for (int k = 0; k < 16; k++) v[k] = __uint_as_float(r[k]);
 }
 
-template <int FORM>
+template <int FORM, int COLS>
 __global__ void __launch_bounds__(32 * kTriTmemWarps) lvc_tridag_tmem_kernel(int64_t rows, int m,
                                                                              const float* __restrict__ a,
                                                                              const float* __restrict__ b,
@@ -559,7 +562,7 @@ __global__ void __launch_bounds__(32 * kTriTmemWarps) lvc_tridag_tmem_kernel(int
   // and release of tensor memory
   const int nr = r0 < rows ? (int)(rows - r0 < 32 ? rows - r0 : 32) : 0;
   if (warp == 0) {
-    tmem_alloc(s_taddr, kTriTmemCols);
+    tmem_alloc(s_taddr, COLS);
     tmem_relinquish();
   }
   tmem_fence_before_sync();
@@ -712,7 +715,7 @@ __global__ void __launch_bounds__(32 * kTriTmemWarps) lvc_tridag_tmem_kernel(int
   tmem_fence_before_sync();
   __syncthreads();
   tmem_fence_after_sync();
-  if (warp == 0) tmem_dealloc(*s_taddr, kTriTmemCols);
+  if (warp == 0) tmem_dealloc(*s_taddr, COLS);
 }
 
 }  // namespace lvc

@@ -42,11 +42,13 @@ def test_par_matches_oracle_bit_exact_on_golden_inputs(ctx, oracle, golden_tridi
 
 
 # (rows, m): empty, single-element systems, partial warps and CTAs, the
-# stanza's inner size, the tensor-memory kernel's limit (128) and just above
-# it, odd and even m, the shared-memory kernels' limit (400) and the kernel
-# with global scratch above it
+# stanza's inner size, the tensor-memory kernel's two allocation sizes and
+# their limits (128, 256) and just above them, odd and even m, the
+# shared-memory kernels' limit (400) and the kernel with global scratch
+# above it
 @pytest.mark.parametrize("shape", [(0, 5), (3, 1), (7, 2), (33, 3), (129, 64), (1000, 115), (257, 128),
-                                   (65, 129), (70, 399), (130, 400), (40, 401), (5, 1000)])
+                                   (65, 129), (70, 200), (40, 256), (9, 257), (70, 399), (130, 400), (40, 401),
+                                   (5, 1000)])
 @pytest.mark.parametrize("form,oform", [("seq", "seq"), ("par", "par4")])
 def test_random_batches_match_oracle_bit_exact(ctx, oracle, shape, form, oform):
     rows, m = shape
@@ -85,10 +87,10 @@ def test_device_pointer_form_matches_entry_point(ctx, oracle):
         assert np.array_equal(out.cpu().numpy(), oracle.tridag(*host, form=oform))
 
 
-@pytest.mark.parametrize("m", [115, 200])
+@pytest.mark.parametrize("m", [115, 200, 300])
 def test_device_pointer_form_with_unaligned_arrays(ctx, oracle, m):
     # device arrays that start 4 bytes past a 16-byte boundary: 4-byte copies
-    # in the tensor-memory kernel (m <= 128), the scalar copy path of the
+    # in the tensor-memory kernel (m <= 256), the scalar copy path of the
     # block kernel above it
     import torch
     rows = 100
