@@ -2546,19 +2546,18 @@ namespace {
 constexpr int64_t kTridagInnerDim = 115;  // INNER_DIM of tridiag-test.fut:4
 
 // Enqueues one batched solve on ctx->stream (device pointers).  Called with
-// ctx->mu held.  m <= 256: the tensor-memory kernel; m <= 400: the block
-// kernel (tridagSeq) or the streaming kernel (tridagPar), no scratch; larger
-// m: scratch
+// ctx->mu held.  m <= 256: the tensor-memory kernel; m <= 400: the
+// streaming kernel, no scratch; larger m: scratch
 // from the context's device pool (stream-ordered: every user of that pool
 // runs on ctx->stream).
 int tridag_check_locked(futhark_context* ctx) {
-  int flag = 0;  // a bulk copy that never landed (its systems are NaN)
+  int flag = 0;  // a bounded device wait that gave up
   LVC_CUDA(ctx, cudaMemcpyFromSymbolAsync(&flag, lvc_tridag_err, sizeof flag, 0, cudaMemcpyDeviceToHost, ctx->stream));
   LVC_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   if (flag) {
     const int zero = 0;
     cudaMemcpyToSymbol(lvc_tridag_err, &zero, sizeof zero);
-    return set_error(ctx, FUTHARK_PROGRAM_ERROR, "tridiagonal solve: a bulk copy timed out");
+    return set_error(ctx, FUTHARK_PROGRAM_ERROR, "tridiagonal solve: a bounded device wait timed out");
   }
   return 0;
 }
@@ -2580,30 +2579,14 @@ int tridag_launch(futhark_context* ctx, int form, int64_t rows, int64_t m, const
     if (e != cudaSuccess) return cuda_fail(ctx, e, "tridiagonal launch");
     return 0;
   }
-  if (m <= kTriBlockMaxM && form == 1) {  // tridagPar: inputs streamed through shared memory
+  if (m <= kTriMaxM) {  // inputs streamed, intermediates in shared memory
     const int64_t nblk = (rows + 31) / 32;
     if (nblk > INT32_MAX) return set_error(ctx, FUTHARK_PROGRAM_ERROR, "tridiagonal batch too large");
     const size_t smem = sizeof(float) * (size_t)tri_stream_floats((int)m);
-    const size_t smem_max = sizeof(float) * (size_t)tri_stream_floats(kTriBlockMaxM);
-    LVC_CUDA(ctx, cudaFuncSetAttribute((const void*)lvc_tridag_stream_kernel,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max));
-    lvc_tridag_stream_kernel<<<(unsigned)nblk, 32, smem, ctx->stream>>>(rows, (int)m, a, b, c, y, out);
-    const cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return cuda_fail(ctx, e, "tridiagonal launch");
-    return 0;
-  }
-  if (m <= kTriBlockMaxM) {  // tridagSeq: whole input rows staged by bulk copies
-    const int64_t nblk = (rows + kTriBlockRows - 1) / kTriBlockRows;
-    if (nblk > INT32_MAX) return set_error(ctx, FUTHARK_PROGRAM_ERROR, "tridiagonal batch too large");
-    auto aligned = [](const void* p) { return ((uintptr_t)p & 15) == 0; };
-    const int vec = aligned(a) && aligned(b) && aligned(c) && aligned(y) && aligned(out);
-    const size_t bs = (size_t)((kTriBlockRows * m + 3) & ~int64_t(3));
-    const size_t smem_blk = 16 + 4 * bs * sizeof(float);  // mbarrier + four blocks
-    const size_t smem_max = 16 + 4 * (size_t)((kTriBlockRows * kTriBlockMaxM + 3) & ~3) * sizeof(float);
-    LVC_CUDA(ctx, cudaFuncSetAttribute((const void*)lvc_tridag_block_kernel,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max));
-    lvc_tridag_block_kernel<<<(unsigned)nblk, kTriBlockRows, smem_blk, ctx->stream>>>(rows, (int)m, a, b, c, y,
-                                                                                         out, vec);
+    const size_t smem_max = sizeof(float) * (size_t)tri_stream_floats(kTriMaxM);
+    auto fs = form == 0 ? lvc_tridag_stream_kernel<0> : lvc_tridag_stream_kernel<1>;
+    LVC_CUDA(ctx, cudaFuncSetAttribute((const void*)fs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max));
+    fs<<<(unsigned)nblk, 32, smem, ctx->stream>>>(rows, (int)m, a, b, c, y, out);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(ctx, e, "tridiagonal launch");
     return 0;

@@ -7,14 +7,12 @@
 //           4-tuple matrix scan for the pivots, two linear-function scans --
 //           folded left to right.
 //
-// Four kernels, one thread per system in each: for m up to 256 (the
-// benchmark's 115 among them) lvc_tridag_tmem_kernel (both forms) streams a
-// warp's 32 systems through shared-memory windows and keeps the row
-// intermediates in tensor memory; for m up to 400 lvc_tridag_block_kernel
-// (FORM 0) stages the rows through shared memory with bulk copies and
-// lvc_tridag_stream_kernel (FORM 1) streams them and keeps the intermediates
-// in shared memory; lvc_tridag_kernel (any m, both forms) reads rows in
-// place.
+// Three kernels, one thread per system in each: for m up to 256 (the
+// benchmark's 115 among them) lvc_tridag_tmem_kernel streams a warp's 32
+// systems through shared-memory windows and keeps the row intermediates in
+// tensor memory; for m up to 400 lvc_tridag_stream_kernel streams them the
+// same way and keeps the intermediates in shared memory; lvc_tridag_kernel
+// (any m) reads rows in place.  All three take both forms.
 // Each recurrence runs in the reference's operation
 // order with every product, sum and quotient explicitly rounded (no fused
 // multiply-add), so a system's solution is bit for bit the one the CPU
@@ -34,18 +32,19 @@
 
 namespace lvc {
 
-// Set by lvc_tridag_block_kernel when a bulk-copy wait gave up (its systems
-// then come out as NaN); reset and read by the host around each launch.
+// Raised by a bounded wait that gave up (lvc_wait_selftest_kernel below);
+// reset and read by the host after each solve and self-test.
 __device__ int lvc_tridag_err;
 
 constexpr int kTriThreads = 128;  // threads (systems) per CTA of lvc_tridag_kernel
 
-// Self-test of the bounded wait: one warp waits on a fresh mbarrier for at
+// Self-test of the bounded wait that the rollback kernels' bulk-copy and
+// cluster waits use (mbar_wait): one warp waits on a fresh mbarrier for at
 // most `polls` polls.  With arrive == 0 nothing ever completes its phase (no
 // copy targets it and no thread arrives), so the wait runs out and the kernel
-// raises lvc_tridag_err exactly as a solve whose bulk copy never landed
-// does; with arrive != 0 lane 0 arrives first and the wait succeeds.  No
-// asynchronous operation is in flight either way, so the CTA may exit at once.
+// raises lvc_tridag_err, which the host reports as a timed-out wait; with
+// arrive != 0 lane 0 arrives first and the wait succeeds.  No asynchronous
+// operation is in flight either way, so the CTA may exit at once.
 __global__ void lvc_wait_selftest_kernel(int polls, int arrive) {
   __shared__ __align__(8) uint64_t bar;
   if (threadIdx.x == 0) {
@@ -162,150 +161,22 @@ __global__ void __launch_bounds__(kTriThreads) lvc_tridag_kernel(int64_t rows, i
   }
 }
 
-// Block kernel for tridagSeq (FORM 0 of lvc_tridag_kernel): one warp per 32
-// consecutive systems.  In row-major [rows][m] arrays those systems are one
-// contiguous block of 32*m floats per array, so the warp copies the four
-// input blocks into shared memory with coalesced 16-byte loads, each lane
-// then runs its system's recurrences out of shared memory (row stride m: for
-// odd m the 32 lanes hit 32 different banks), and the solution block goes
-// back with coalesced stores.  Every intermediate overwrites an input element
-// that is no longer needed -- cp_i over c_i, yp_i and then x_i over y_i -- so
-// the shared memory is exactly the four input blocks.  The arithmetic and its
-// order are those of lvc_tridag_kernel.  (tridagPar, whose three passes keep
-// b' and y' besides the inputs, streams its inputs instead:
-// lvc_tridag_stream_kernel.)
-// When the arrays are 16-byte aligned and a block's bytes a multiple of 16
-// (every full block: 32 * m * 4 bytes), one thread moves the blocks with TMA
-// bulk copies (four in, one out) -- tens of kilobytes in flight per CTA,
-// which a warp's own loads cannot keep up; otherwise the warp copies.
-constexpr int kTriBlockRows = 32;
-constexpr int kTriBlockMaxM = 400;  // 4 x 32 x 400 floats = 200 KB of shared memory
+constexpr int kTriMaxM = 400;  // the streaming kernel's limit: 2 x 32 x 401 floats + windows = 112 KB
 
-__device__ __forceinline__ void tri_copy_in(float* dst, const float* __restrict__ src, int64_t n, bool vec, int lane) {
-  if (vec) {
-    const int64_t n4 = n >> 2;
-    const float4* s4 = reinterpret_cast<const float4*>(src);
-    float4* d4 = reinterpret_cast<float4*>(dst);
-    for (int64_t k = lane; k < n4; k += 32) d4[k] = __ldcs(s4 + k);  // read once: streaming
-    for (int64_t k = (n4 << 2) + lane; k < n; k += 32) dst[k] = __ldcs(src + k);
-  } else {
-    for (int64_t k = lane; k < n; k += 32) dst[k] = __ldcs(src + k);
-  }
-}
-
-__device__ __forceinline__ void tri_bulk_s2g(void* dst, const void* src, unsigned bytes) {
-  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;\n" ::"l"(dst), "r"(smem_u32(src)),
-               "r"(bytes)
-               : "memory");
-}
-
-__global__ void __launch_bounds__(32) lvc_tridag_block_kernel(int64_t rows, int m, const float* __restrict__ a,
-                                                             const float* __restrict__ b,
-                                                             const float* __restrict__ c,
-                                                             const float* __restrict__ y,
-                                                             float* __restrict__ out, int vec) {
-  extern __shared__ __align__(16) unsigned char tri_raw[];
-  uint64_t* bar = reinterpret_cast<uint64_t*>(tri_raw);
-  float* tri_blk = reinterpret_cast<float*>(tri_raw + 16);
-  const int lane = threadIdx.x;
-  const int64_t r0 = (int64_t)blockIdx.x * kTriBlockRows;
-  const int nr = (int)(rows - r0 < kTriBlockRows ? rows - r0 : kTriBlockRows);
-  const int64_t n = (int64_t)nr * m;
-  const int64_t bs = (int64_t)kTriBlockRows * m + 3 & ~int64_t(3);  // per-array block, 16-byte aligned
-  float* sa = tri_blk;
-  float* sb = sa + bs;
-  float* scc = sb + bs;
-  float* sy = scc + bs;
-  const int64_t off = r0 * m;
-  const unsigned bytes = (unsigned)(n * sizeof(float));
-  const bool bulk = vec && (bytes % 16) == 0;
-  if (bulk) {
-    if (lane == 0) {
-      mbar_init(bar, 1);
-      asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
-      mbar_expect_tx(bar, 4 * bytes);
-      bulk_g2s(sa, a + off, bytes, bar);
-      bulk_g2s(sb, b + off, bytes, bar);
-      bulk_g2s(scc, c + off, bytes, bar);
-      bulk_g2s(sy, y + off, bytes, bar);
-    }
-    __syncwarp();
-    if (!mbar_wait(bar, 0)) {
-      // the copies did not land: flag it, give them one more bounded wait,
-      // and leave NaN where these systems' solutions go
-      if (lane == 0) atomicExch(&lvc_tridag_err, 1);
-      mbar_wait(bar, 0);
-      for (int64_t k = lane; k < n; k += 32) out[off + k] = __int_as_float(0x7fc00000);
-      return;
-    }
-  } else {
-    tri_copy_in(sa, a + off, n, vec, lane);
-    tri_copy_in(sb, b + off, n, vec, lane);
-    tri_copy_in(scc, c + off, n, vec, lane);
-    tri_copy_in(sy, y + off, n, vec, lane);
-  }
-  __syncwarp();
-  if (lane < nr) {
-    const float* ar = sa + (int64_t)lane * m;
-    float* br = sb + (int64_t)lane * m;
-    float* cr = scc + (int64_t)lane * m;
-    float* yr = sy + (int64_t)lane * m;
-    float cp = tri_div(cr[0], br[0]);
-    float yp = tri_div(yr[0], br[0]);
-    cr[0] = cp;
-    yr[0] = yp;
-    for (int i = 1; i < m; i++) {
-      const float ai = ar[i];
-      const float nf = tri_rcp(tri_sub(br[i], tri_mul(ai, cp)));
-      cp = tri_mul(cr[i], nf);
-      yp = tri_mul(tri_sub(yr[i], tri_mul(ai, yp)), nf);
-      cr[i] = cp;
-      yr[i] = yp;
-    }
-    float x = yp;
-    for (int i = m - 2; i >= 0; i--) {
-      x = tri_sub(yr[i], tri_mul(cr[i], x));
-      yr[i] = x;
-    }
-  }
-  float* dst = out + off;
-  if (bulk) {
-    // the lanes' shared-memory writes, then one thread's bulk store
-    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-    __syncwarp();
-    if (lane == 0) {
-      tri_bulk_s2g(dst, sy, bytes);
-      asm volatile("cp.async.bulk.commit_group;\n" ::: "memory");
-      asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory");  // sy read before the CTA exits
-    }
-    return;
-  }
-  __syncwarp();
-  if (vec) {
-    const int64_t n4 = n >> 2;
-    const float4* s4 = reinterpret_cast<const float4*>(sy);
-    float4* d4 = reinterpret_cast<float4*>(dst);
-    for (int64_t k = lane; k < n4; k += 32) __stcs(d4 + k, s4[k]);
-    for (int64_t k = (n4 << 2) + lane; k < n; k += 32) __stcs(dst + k, sy[k]);
-  } else {
-    for (int64_t k = lane; k < n; k += 32) __stcs(dst + k, sy[k]);
-  }
-}
-
-// Streaming kernel for tridagPar (FORM 1 of lvc_tridag_kernel): one warp per
-// 32 consecutive systems, lane = system, as the block kernel, but the four
-// input rows are not staged whole.  They pass through a double-buffered
-// window of kTriWin columns (cp.async, 4-byte copies: 8 lanes cover 8
-// consecutive columns of one row, so a warp's copy instruction reads 4 short
-// runs), and shared memory keeps only the two intermediates the backward
-// recurrence needs per row, b'_i and y'_i (c_i comes through the window a
-// second time, last column first) -- about 0.6 of the block kernel's
-// footprint, so more systems are in flight per SM.  The arithmetic and its
-// order are those of lvc_tridag_kernel (recurrences 1 and 2 fused into one
-// forward pass over i: each step reads only values the pass has already
-// produced).  The solution overwrites y'_i and leaves as the block kernel's
-// does.  (The same streaming for tridagSeq measured 4 % slower than the
-// block kernel, whose in-place intermediates need no second pass over c.)
+// Streaming kernel (both forms of lvc_tridag_kernel; used where the tensor-
+// memory kernel does not fit, 256 < m <= 400): one warp per 32 consecutive
+// systems, lane = system, but the four input rows are not staged whole.
+// They pass through a double-buffered window of kTriWin columns (cp.async,
+// 4-byte copies: 8 lanes cover 8 consecutive columns of one row, so a
+// warp's copy instruction reads 4 short runs), and shared memory keeps only
+// the two intermediates the backward pass needs per row -- FORM 0: cp_i and
+// yp_i; FORM 1: b'_i and y'_i (c_i comes through the window a second time,
+// last column first) -- half of what staging the four input rows would take,
+// so twice the systems are in flight.  The arithmetic and its order are those
+// of lvc_tridag_kernel (FORM 1's recurrences 1 and 2 fused into one forward
+// pass over i: each step reads only values the pass has already produced).
+// The solution overwrites the second intermediate and leaves row by row,
+// consecutive lanes on consecutive elements.
 constexpr int kTriWin = 8;
 
 __device__ __forceinline__ void cp_async4(float* dst, const float* src, bool valid) {
@@ -324,6 +195,7 @@ __host__ __device__ __forceinline__ int64_t tri_stream_floats(int m) {
   return 2LL * 32 * tri_stream_ld(m) + 2LL * 4 * 32 * (kTriWin + 1);
 }
 
+template <int FORM>
 __global__ void __launch_bounds__(32) lvc_tridag_stream_kernel(int64_t rows, int m, const float* __restrict__ a,
                                                               const float* __restrict__ b,
                                                               const float* __restrict__ c,
@@ -334,8 +206,8 @@ __global__ void __launch_bounds__(32) lvc_tridag_stream_kernel(int64_t rows, int
   const int64_t r0 = (int64_t)blockIdx.x * 32;
   const int nr = (int)(rows - r0 < 32 ? rows - r0 : 32);
   const int ld = tri_stream_ld(m);
-  float* P = tri_s;            // b'_i, [32][ld]
-  float* Q = P + 32 * ld;      // y'_i, then x_i
+  float* P = tri_s;            // cp_i (FORM 0) or b'_i (FORM 1), [32][ld]
+  float* Q = P + 32 * ld;      // yp_i or y'_i, then x_i
   float* Wn = Q + 32 * ld;     // [2][4][32][kTriWin + 1]
   constexpr int WS = kTriWin + 1, WA = 32 * WS, WB = 4 * WA;
   const float* src[4] = {a, b, c, y};
@@ -357,102 +229,146 @@ __global__ void __launch_bounds__(32) lvc_tridag_stream_kernel(int64_t rows, int
     }
     cp_async_commit();
   };
-  // Recurrences 1 and 2 in one forward pass: b'_i from the 4-tuple scan of
-  // (b_i, -a_i c_{i-1}, 1, 0), then y'_i from the 2-tuple scan of
-  // (y_i, -a_i / b'_{i-1}); both as lvc_tridag_kernel computes them.
-  float s0 = 1.0f, s1 = 0.0f, s2 = 0.0f, s3 = 1.0f, b0 = 0.0f, cprev = 0.0f;
-  float y0 = 0.0f, c0 = 0.0f, c1 = 1.0f, bprev = 0.0f;
-  fetch(0, 0, 15);
-  for (int q = 0; q < nq; q++) {
-    if (q + 1 < nq) {
-      fetch(q + 1, (q + 1) & 1, 15);
-      cp_async_wait<1>();
-    } else {
-      cp_async_wait<0>();
-    }
-    __syncwarp();
-    const float* w = Wn + (q & 1) * WB + lane * WS;
-    if (lane < nr) {
+  if constexpr (FORM == 0) {
+    // forward: cp_i = c_i / (b_i - a_i cp_{i-1}), yp_i = (y_i - a_i yp_{i-1}) / (...)  (:82-91)
+    float cp = 0.0f, yp = 0.0f;
+    fetch(0, 0, 15);
+    for (int q = 0; q < nq; q++) {
+      if (q + 1 < nq) {
+        fetch(q + 1, (q + 1) & 1, 15);
+        cp_async_wait<1>();
+      } else {
+        cp_async_wait<0>();
+      }
+      __syncwarp();
+      const float* w = Wn + (q & 1) * WB + lane * WS;
+      if (lane < nr) {
 #pragma unroll
-      for (int k = 0; k < kTriWin; k++) {
-        const int i = q * kTriWin + k;
-        if (i < m) {
-          const float ai = w[k], bi = w[WA + k], ci = w[2 * WA + k], yi = w[3 * WA + k];
-          if (i == 0) {
-            b0 = bi;
-            y0 = yi;
+        for (int k = 0; k < kTriWin; k++) {
+          const int i = q * kTriWin + k;
+          if (i < m) {
+            const float ai = w[k], bi = w[WA + k], ci = w[2 * WA + k], yi = w[3 * WA + k];
+            if (i == 0) {
+              cp = tri_div(ci, bi);
+              yp = tri_div(yi, bi);
+            } else {
+              const float nf = tri_rcp(tri_sub(bi, tri_mul(ai, cp)));
+              cp = tri_mul(ci, nf);
+              yp = tri_mul(tri_sub(yi, tri_mul(ai, yp)), nf);
+            }
+            P[lane * ld + i] = cp;
+            Q[lane * ld + i] = yp;
           }
-          float m0 = 1.0f, m1 = 0.0f, m2 = 0.0f, m3 = 1.0f;
-          if (0 < i) {
-            m0 = bi;
-            m1 = tri_sub(0.0f, tri_mul(ai, cprev));
-            m2 = 1.0f;
-            m3 = 0.0f;
-          }
-          cprev = ci;
-          const float value = tri_rcp(tri_mul(s0, m0));
-          const float n0 = tri_mul(tri_add(tri_mul(m0, s0), tri_mul(m1, s2)), value);
-          const float n1 = tri_mul(tri_add(tri_mul(m0, s1), tri_mul(m1, s3)), value);
-          const float n2 = tri_mul(tri_add(tri_mul(m2, s0), tri_mul(m3, s2)), value);
-          const float n3 = tri_mul(tri_add(tri_mul(m2, s1), tri_mul(m3, s3)), value);
-          s0 = n0;
-          s1 = n1;
-          s2 = n2;
-          s3 = n3;
-          const float bpi = tri_div(tri_add(tri_mul(s0, b0), s1), tri_add(tri_mul(s2, b0), s3));  // b'_i
-          float l0 = 0.0f, l1 = 1.0f;
-          if (0 < i) {
-            l0 = yi;
-            l1 = tri_sub(0.0f, tri_div(ai, bprev));
-          }
-          const float e0 = tri_add(l0, tri_mul(l1, c0));
-          const float e1 = tri_mul(c1, l1);
-          c0 = e0;
-          c1 = e1;
-          P[lane * ld + i] = bpi;
-          Q[lane * ld + i] = tri_add(c0, tri_mul(c1, y0));  // y'_i
-          bprev = bpi;
         }
       }
+      __syncwarp();  // the window is refilled two chunks on
     }
-    __syncwarp();
-  }
-  // Recurrence 3, backward, with c_i through the window again (last chunk first)
-  float yn = 0.0f;
-  if (lane < nr) yn = tri_div(Q[lane * ld + m - 1], P[lane * ld + m - 1]);
-  c0 = 0.0f;
-  c1 = 1.0f;
-  fetch(nq - 1, 0, 4);
-  for (int qq = 0; qq < nq; qq++) {
-    const int q = nq - 1 - qq;
-    if (qq + 1 < nq) {
-      fetch(q - 1, (qq + 1) & 1, 4);
-      cp_async_wait<1>();
-    } else {
-      cp_async_wait<0>();
-    }
-    __syncwarp();
-    const float* w = Wn + (qq & 1) * WB + lane * WS;
+    // backward: x_i = yp_i - cp_i x_{i+1}  (:92-95)
     if (lane < nr) {
-#pragma unroll
-      for (int kk = kTriWin - 1; kk >= 0; kk--) {
-        const int i = q * kTriWin + kk;
-        if (i < m) {
-          float l0 = 0.0f, l1 = 1.0f;
-          if (i < m - 1) {
-            const float bi = P[lane * ld + i];
-            l0 = tri_div(Q[lane * ld + i], bi);
-            l1 = tri_sub(0.0f, tri_div(w[2 * WA + kk], bi));
-          }
-          const float n0 = tri_add(l0, tri_mul(l1, c0));
-          const float n1 = tri_mul(c1, l1);
-          c0 = n0;
-          c1 = n1;
-          Q[lane * ld + i] = tri_add(c0, tri_mul(c1, yn));
-        }
+      float x = Q[lane * ld + m - 1];
+      for (int i = m - 2; i >= 0; i--) {
+        x = tri_sub(Q[lane * ld + i], tri_mul(P[lane * ld + i], x));
+        Q[lane * ld + i] = x;
       }
     }
-    __syncwarp();
+  } else {
+    // Recurrences 1 and 2 in one forward pass: b'_i from the 4-tuple scan of
+    // (b_i, -a_i c_{i-1}, 1, 0), then y'_i from the 2-tuple scan of
+    // (y_i, -a_i / b'_{i-1}); both as lvc_tridag_kernel computes them.
+    float s0 = 1.0f, s1 = 0.0f, s2 = 0.0f, s3 = 1.0f, b0 = 0.0f, cprev = 0.0f;
+    float y0 = 0.0f, c0 = 0.0f, c1 = 1.0f, bprev = 0.0f;
+    fetch(0, 0, 15);
+    for (int q = 0; q < nq; q++) {
+      if (q + 1 < nq) {
+        fetch(q + 1, (q + 1) & 1, 15);
+        cp_async_wait<1>();
+      } else {
+        cp_async_wait<0>();
+      }
+      __syncwarp();
+      const float* w = Wn + (q & 1) * WB + lane * WS;
+      if (lane < nr) {
+  #pragma unroll
+        for (int k = 0; k < kTriWin; k++) {
+          const int i = q * kTriWin + k;
+          if (i < m) {
+            const float ai = w[k], bi = w[WA + k], ci = w[2 * WA + k], yi = w[3 * WA + k];
+            if (i == 0) {
+              b0 = bi;
+              y0 = yi;
+            }
+            float m0 = 1.0f, m1 = 0.0f, m2 = 0.0f, m3 = 1.0f;
+            if (0 < i) {
+              m0 = bi;
+              m1 = tri_sub(0.0f, tri_mul(ai, cprev));
+              m2 = 1.0f;
+              m3 = 0.0f;
+            }
+            cprev = ci;
+            const float value = tri_rcp(tri_mul(s0, m0));
+            const float n0 = tri_mul(tri_add(tri_mul(m0, s0), tri_mul(m1, s2)), value);
+            const float n1 = tri_mul(tri_add(tri_mul(m0, s1), tri_mul(m1, s3)), value);
+            const float n2 = tri_mul(tri_add(tri_mul(m2, s0), tri_mul(m3, s2)), value);
+            const float n3 = tri_mul(tri_add(tri_mul(m2, s1), tri_mul(m3, s3)), value);
+            s0 = n0;
+            s1 = n1;
+            s2 = n2;
+            s3 = n3;
+            const float bpi = tri_div(tri_add(tri_mul(s0, b0), s1), tri_add(tri_mul(s2, b0), s3));  // b'_i
+            float l0 = 0.0f, l1 = 1.0f;
+            if (0 < i) {
+              l0 = yi;
+              l1 = tri_sub(0.0f, tri_div(ai, bprev));
+            }
+            const float e0 = tri_add(l0, tri_mul(l1, c0));
+            const float e1 = tri_mul(c1, l1);
+            c0 = e0;
+            c1 = e1;
+            P[lane * ld + i] = bpi;
+            Q[lane * ld + i] = tri_add(c0, tri_mul(c1, y0));  // y'_i
+            bprev = bpi;
+          }
+        }
+      }
+      __syncwarp();
+    }
+    // Recurrence 3, backward, with c_i through the window again (last chunk first)
+    float yn = 0.0f;
+    if (lane < nr) yn = tri_div(Q[lane * ld + m - 1], P[lane * ld + m - 1]);
+    c0 = 0.0f;
+    c1 = 1.0f;
+    fetch(nq - 1, 0, 4);
+    for (int qq = 0; qq < nq; qq++) {
+      const int q = nq - 1 - qq;
+      if (qq + 1 < nq) {
+        fetch(q - 1, (qq + 1) & 1, 4);
+        cp_async_wait<1>();
+      } else {
+        cp_async_wait<0>();
+      }
+      __syncwarp();
+      const float* w = Wn + (qq & 1) * WB + lane * WS;
+      if (lane < nr) {
+  #pragma unroll
+        for (int kk = kTriWin - 1; kk >= 0; kk--) {
+          const int i = q * kTriWin + kk;
+          if (i < m) {
+            float l0 = 0.0f, l1 = 1.0f;
+            if (i < m - 1) {
+              const float bi = P[lane * ld + i];
+              l0 = tri_div(Q[lane * ld + i], bi);
+              l1 = tri_sub(0.0f, tri_div(w[2 * WA + kk], bi));
+            }
+            const float n0 = tri_add(l0, tri_mul(l1, c0));
+            const float n1 = tri_mul(c1, l1);
+            c0 = n0;
+            c1 = n1;
+            Q[lane * ld + i] = tri_add(c0, tri_mul(c1, yn));
+          }
+        }
+      }
+      __syncwarp();
+    }
   }
   __syncwarp();
   // the solution rows (Q, stride ld) to out, consecutive lanes on consecutive elements

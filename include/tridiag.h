@@ -63,16 +63,18 @@ LVC_API int futhark_entry_tridagNestedSeqConst(struct futhark_context *ctx, stru
 LVC_API int lvc_tridag_f32(struct futhark_context *ctx, int32_t form, int64_t rows, int64_t m,
                            const float *a, const float *b, const float *c, const float *y, float *out);
 /* Synchronises the context's stream and reports (FUTHARK_PROGRAM_ERROR) a
- * solve since the last check whose input copy timed out -- its systems were
- * written as NaN.  The entry points check on every call. */
+ * bounded device wait that gave up since the last check, and any CUDA error
+ * of the solves.  The entry points check on every call.  (The solvers
+ * themselves wait on nothing but their own asynchronous copies; the flag is
+ * shared with lvc_wait_selftest.) */
 LVC_API int lvc_tridag_check(struct futhark_context *ctx);
-/* Self-test of the kernels' bounded waits (no counterpart in the reference):
- * one warp waits at most `polls` polls (1 .. 2^22) on a fresh mbarrier that
+/* Self-test of the bounded mbarrier wait the rollback kernels use for their
+ * bulk copies and cluster exchanges (no counterpart in the reference): one
+ * warp waits at most `polls` polls (1 .. 2^22) on a fresh mbarrier that
  * nothing completes (arrive == 0) or that it completes itself first
- * (arrive != 0).  A wait that runs out raises the same device flag as a solve
- * whose copy never landed, so this returns what lvc_tridag_check reports:
- * FUTHARK_PROGRAM_ERROR ("... timed out") for arrive == 0, 0 otherwise.  The
- * context stays usable either way. */
+ * (arrive != 0).  A wait that runs out raises a device flag, so this returns
+ * what lvc_tridag_check reports: FUTHARK_PROGRAM_ERROR ("... timed out") for
+ * arrive == 0, 0 otherwise.  The context stays usable either way. */
 LVC_API int lvc_wait_selftest(struct futhark_context *ctx, int32_t polls, int32_t arrive);
 
 #ifdef __cplusplus

@@ -89,9 +89,9 @@ def test_device_pointer_form_matches_entry_point(ctx, oracle):
 
 @pytest.mark.parametrize("m", [115, 200, 300])
 def test_device_pointer_form_with_unaligned_arrays(ctx, oracle, m):
-    # device arrays that start 4 bytes past a 16-byte boundary: 4-byte copies
-    # in the tensor-memory kernel (m <= 256), the scalar copy path of the
-    # block kernel above it
+    # device arrays that start 4 bytes past a 16-byte boundary (the kernels'
+    # window copies are 4-byte copies: no alignment beyond the element's);
+    # the tensor-memory kernel (m <= 256) and the streaming kernel above it
     import torch
     rows = 100
     host = wl.tridiag_inputs(rows, m, seed=12)
