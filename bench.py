@@ -759,11 +759,16 @@ def run_ours(args):
     if not args.no_autotune:
         t0 = time.perf_counter()
         entries = ctx.autotune(calibs, precision=precision, probe_steps=8)
+        changed = [e for e in entries
+                   if e.us_per_step_default > 0 and e.us_per_step_best < e.us_per_step_default * 0.999]
+        # the plan-level pass keeps a class's change only if the whole plan
+        # is faster with it
         plan_params = ctx.autotune_plan(calibs, precision=precision)
+        kept = [e for e in changed
+                if ctx.tuning_get(e.numX, e.numY, precision=precision).shape.key() == e.shape.key()]
         tune = {"seconds": time.perf_counter() - t0, "classes": len(entries),
-                "changed_from_builtin": [f"{e.numX}x{e.numY}: {e.shape}" for e in entries
-                                         if e.us_per_step_default > 0
-                                         and e.us_per_step_best < e.us_per_step_default * 0.999],
+                "changed_by_class_probe": [f"{e.numX}x{e.numY}: {e.shape}" for e in changed],
+                "changed_from_builtin": [f"{e.numX}x{e.numY}: {e.shape}" for e in kept],
                 "plan_params": plan_params}
     t0 = time.perf_counter()
     plan = ctx.plan(calibs, precision=precision)

@@ -328,7 +328,10 @@ LVC_API int lvc_autotune(struct futhark_context *ctx, const struct lvc_calibrati
 /* Plan-level autotuner: runs the workload's whole plan, with its time lines
  * capped at max_steps (<= 0: 32), under lvc.grid 0/1 x lvc.streams 2/4, and
  * keeps the fastest as the context's tuning parameters (reported through the
- * optional pointers, with the capped plan's time in ms).  Synchronous. */
+ * optional pointers, with the capped plan's time in ms).  Then, for every
+ * grid class of the workload whose table shape is not the built-in one, it
+ * times the plan with that class back on the built-in shape and keeps
+ * whichever plan was faster.  Synchronous. */
 LVC_API int lvc_autotune_plan(struct futhark_context *ctx, const struct lvc_calibration *calibs,
                               int32_t n, int32_t precision, int32_t max_steps, int32_t *grid,
                               int32_t *streams, double *ms);

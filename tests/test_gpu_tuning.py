@@ -115,3 +115,20 @@ def test_plan_autotuner_keeps_valid_parameters(pkg, oracle):
             assert res["lvc.grid"] in (0, 1) and res["lvc.streams"] in (2, 4) and res["capped_plan_ms"] > 0
         got = c.batch(calibs)  # plans built afterwards run under the chosen parameters
         assert rel_err(got, oracle.batch_f64(calibs)) <= 1e-9
+
+
+def test_plan_autotuner_checks_changed_shapes(pkg, oracle):
+    # a class pinned to a non-built-in shape is checked against the whole
+    # plan: afterwards it holds either that shape or the built-in one, and
+    # plans built afterwards are still right
+    calibs = wl.uneven_mix(8, seed=29, sizes=(64, 128), numT=(6, 12), outer=(2, 5))
+    X, Y = calibs[0].numX, calibs[0].numY
+    with pkg.Context() as c:
+        builtin = c.tuning_get(X, Y).shape.key()
+        other = [s for s in c.shape_candidates(X, Y) if s.key() != builtin]
+        assert other
+        c.tuning_set(X, Y, 0, other[0])
+        c.autotune_plan(calibs, precision=0, max_steps=4)
+        assert c.tuning_get(X, Y).shape.key() in (builtin, other[0].key())
+        got = c.batch(calibs)
+        assert rel_err(got, oracle.batch_f64(calibs)) <= 1e-9
