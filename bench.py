@@ -763,7 +763,7 @@ def run_ours(args):
                    if e.us_per_step_default > 0 and e.us_per_step_best < e.us_per_step_default * 0.999]
         # the plan-level pass keeps a class's change only if the whole plan
         # is faster with it
-        plan_params = ctx.autotune_plan(calibs, precision=precision)
+        plan_params = ctx.autotune_plan(calibs, precision=precision, max_steps=256)
         kept = [e for e in changed
                 if ctx.tuning_get(e.numX, e.numY, precision=precision).shape.key() == e.shape.key()]
         tune = {"seconds": time.perf_counter() - t0, "classes": len(entries),

@@ -309,7 +309,9 @@ class Context:
         return self.tuning_entries()
 
     def autotune_plan(self, calibs: Sequence[Calibration], precision: int = F64, max_steps: int = 32) -> dict:
-        """Time the whole plan under lvc.grid 0/1 x lvc.streams 2/4; keep the fastest."""
+        """Time the whole plan (time lines capped at max_steps) under lvc.grid 0/1 x
+        lvc.streams 2/4 and keep the fastest; then keep each class shape the
+        per-class autotuner changed only if the plan is faster with it."""
         arr = _calib_array(calibs)
         g, st, ms = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_double()
         self._check(self.lib.lvc_autotune_plan(self._ctx, arr, len(calibs), precision, max_steps,
