@@ -387,9 +387,9 @@ __global__ void __launch_bounds__(32) lvc_tridag_stream_kernel(int64_t rows, int
 // ---------------------------------------------------------------------------
 // Tensor-memory kernel (m <= 256): the row intermediates live in TMEM.
 // ---------------------------------------------------------------------------
-// The streaming kernels above are bound by the latency of each system's
-// sequential chain at the few warps per SM that shared memory leaves them
-// (the four input rows, or two intermediate rows, of 32 systems per warp).
+// The streaming kernel above is bound by the latency of each system's
+// sequential chain at the few warps per SM that shared memory leaves it (two
+// intermediate rows of 32 systems per warp).
 // Here the intermediates go to tensor memory instead -- 256 KB per SM that
 // nothing else of this library uses: thread t of a warp owns TMEM lane
 // 32 (warp % 4) + t of its CTA's allocation, and the two 32-bit values of
