@@ -400,8 +400,10 @@ __global__ void __launch_bounds__(32) lvc_tridag_stream_kernel(int64_t rows, int
 // stages of kTriWin-column windows of the four inputs, cp.async) and an
 // output window, so a 4-warp CTA needs 60 KB and, for m <= 128, 256 TMEM
 // columns: two CTAs, eight warps, per SM; for m <= 256, 512 columns: one CTA
-// per SM.  The shared-memory request is padded (80 KB, 120 KB) so that no
-// further CTA fits and waits in tcgen05.alloc.  The arithmetic and its
+// per SM.  The shared-memory request is padded -- 80 KB for 256 columns,
+// 150 KB for 512 -- so that whatever mix of these CTAs an SM holds, even
+// from concurrent launches, asks for at most its 512 columns and no CTA
+// waits in tcgen05.alloc.  The arithmetic and its
 // order are lvc_tridag_kernel's, with FORM 1's three recurrences fused into
 // the forward pass and the backward fold.
 constexpr int kTriTmemWarps = 4;
@@ -411,7 +413,7 @@ constexpr int kTriTmemStages = 3;
 __host__ __device__ __forceinline__ int tri_tmem_cols(int m) { return m <= 128 ? 256 : 512; }
 __host__ __device__ __forceinline__ size_t tri_tmem_smem(int cols) {
   const size_t need = 16 + sizeof(float) * kTriTmemWarps * (kTriTmemStages * 4 * 32 * (kTriWin + 1) + 32 * (kTriWin + 1));
-  const size_t pad = cols > 256 ? 120 * 1024 : 80 * 1024;
+  const size_t pad = cols > 256 ? 150 * 1024 : 80 * 1024;  // 150 + 80 KB exceed an SM's 228 KB
   return need > pad ? need : pad;
 }
 
