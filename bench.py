@@ -671,11 +671,20 @@ def run_plain_configs(pkg, wl, ctx, args, fp64_peak):
 
 
 def run_f32_state(pkg, wl, ctx, calibs, args, ref, sample):
-    """The FP32-state variant: the uneven mix (device-resident and end to end)
-    and the large dataset, each with its error against the FP64 oracle."""
+    """The FP32-state variant on a context of its own, autotuned for it: the
+    uneven mix (device-resident and end to end) and the large dataset, each
+    with its error against the FP64 oracle."""
     import numpy as np
     from oracle import oracle
     F32 = pkg.F32_STATE
+    # a context of its own, autotuned for this precision like the main one
+    # (its tuning parameters would otherwise carry over to later f64 plans)
+    ctx = pkg.Context(f"#{dist_env()[2]}")
+    tune = None
+    if not args.no_autotune:
+        t0 = time.perf_counter()
+        ctx.autotune(calibs, precision=F32, probe_steps=8)
+        tune = dict(ctx.autotune_plan(calibs, precision=F32, max_steps=256), seconds=time.perf_counter() - t0)
     plan = ctx.plan(calibs, precision=F32)
     ext = torch_stream(ctx)
     import torch
@@ -712,8 +721,9 @@ def run_f32_state(pkg, wl, ctx, calibs, args, ref, sample):
         lref = np.array(list(ex.map(lambda i: oracle.value_f64(big.numX, big.numY, big.numT, big.s0, 0.001 * i,
                                                                 big.t, big.alpha, big.nu, big.beta), idx)))
     lrel = np.abs(lprices[idx] - lref) / np.abs(lref)
+    ctx.close()
     return {"mix": {"value": n_opts / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms, "e2e_value": e2e,
-                    "error_vs_fp64_oracle": mix_err},
+                    "error_vs_fp64_oracle": mix_err, "autotune": tune},
             "large": {"value": big.outer / (lms * 1e-3), "unit": UNIT, "device_ms": lms,
                       "max_rel_err_vs_fp64_oracle": float(lrel.max()), "oracle_strikes_checked": len(idx)},
             "contract": "1e-4 relative on prices above 1e-3 of their calibration's largest, 1e-7 absolute below"}
