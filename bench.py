@@ -605,16 +605,22 @@ def run_plain_configs(pkg, wl, ctx, args, fp64_peak):
     futhark_entry_main_f64 (prices copied to host), the FP64 roofline, the CPU
     baseline (the oracle on all host threads and on one, median of 5 runs over
     a sample of the strikes) and the error against the oracle on the strikes it
-    priced."""
+    priced.  The datasets run on a context of their own, its shape table
+    autotuned for each dataset's grid class at that dataset's strike count
+    (the mix's table is tuned for the mix's instance counts)."""
     import numpy as np
     from oracle import oracle
     threads = oracle.max_threads()
     # strikes per one-thread sample: about half a second of oracle time each
     one_thread_strikes = {"small": 4, "medium": 16, "large": 2}
     res = {}
+    ctx = pkg.Context(f"#{dist_env()[2]}")
     for name in ("small", "medium", "large"):
         c = wl.DATASETS[name]
         a9 = (c.outer, c.numX, c.numY, c.numT, c.s0, c.t, c.alpha, c.nu, c.beta)
+        if not args.no_autotune:
+            ctx.autotune([c], precision=pkg.F64, probe_steps=8)
+        tuned_shape = str(ctx.tuning_get(c.numX, c.numY).shape)
         got = ctx.main_f64(*a9)  # builds and keeps the entry point's plan
         e2e = []
         for _ in range(5):
@@ -666,7 +672,9 @@ def run_plain_configs(pkg, wl, ctx, args, fp64_peak):
                              "sample": "the first strikes of the dataset, f64 oracle, median of 5 runs"},
             "max_rel_err_vs_fp64_oracle": float(rel.max()),
             "oracle_strikes_checked": kn,
+            "rollback_shape": tuned_shape,
         }
+    ctx.close()
     return res
 
 
