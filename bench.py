@@ -587,7 +587,9 @@ def run_serving(pkg, wl, ctx, args, rank, precision):
         ref = oracle.batch_f64([reqs[i] for i in idx])
         got = np.concatenate([check[i] for i in idx])
         err = float(np.max(np.abs(got - ref) / np.abs(ref)))
+    cells_per_option = sum(c.work() for c in reqs) / max(1, sum(c.outer for c in reqs))
     return {"capacity_req_per_s": cap, "capacity_options_per_s": sat["throughput_options_per_s"],
+            "capacity_option_cell_steps_per_s": (sat["throughput_options_per_s"] or 0.0) * cells_per_option,
             "saturating_stream": sat, "sweep": out,
             "solo_latency_ms": {"p50": solo_p50, "p99": float(np.percentile(solo, 99)),
                                 "what": "each request submitted alone into an idle server"},
