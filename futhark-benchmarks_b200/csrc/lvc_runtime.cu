@@ -2588,11 +2588,8 @@ namespace {
 
 constexpr int64_t kTridagInnerDim = 115;  // INNER_DIM of tridiag-test.fut:4
 
-// Enqueues one batched solve on ctx->stream (device pointers).  Called with
-// ctx->mu held.  m <= 256: the tensor-memory kernel; m <= 400: the
-// streaming kernel, no scratch; larger m: scratch
-// from the context's device pool (stream-ordered: every user of that pool
-// runs on ctx->stream).
+// Synchronises ctx->stream and reports a bounded device wait that gave up.
+// Called with ctx->mu held.
 int tridag_check_locked(futhark_context* ctx) {
   int flag = 0;  // a bounded device wait that gave up
   LVC_CUDA(ctx, cudaMemcpyFromSymbolAsync(&flag, lvc_tridag_err, sizeof flag, 0, cudaMemcpyDeviceToHost, ctx->stream));
@@ -2605,6 +2602,10 @@ int tridag_check_locked(futhark_context* ctx) {
   return 0;
 }
 
+// Enqueues one batched solve on ctx->stream (device pointers).  Called with
+// ctx->mu held.  m <= 256: the tensor-memory kernel; m <= 400: the
+// streaming kernel, no scratch; larger m: scratch from the context's device
+// pool (stream-ordered: every user of that pool runs on ctx->stream).
 int tridag_launch(futhark_context* ctx, int form, int64_t rows, int64_t m, const float* a, const float* b,
                   const float* c, const float* y, float* out) {
   if (rows < 0 || m < 0 || m > INT32_MAX) return set_error(ctx, FUTHARK_PROGRAM_ERROR, "bad tridiagonal batch shape");
