@@ -193,18 +193,25 @@ __global__ void __launch_bounds__(kAdvThreads, 4) tke_advect_kernel(TkeArgs p, i
   float T0 = ldT(xs - 1), T1 = ldT(xs), T2 = ldT(xs + 1), T3 = ldT(xs + 2);  // x - 1 .. x + 2
   float W0 = ldW(xs - 1), W1 = ldW(xs), W2 = ldW(xs + 1), W3 = ldW(xs + 2);
   float fe_prev = (live && xs >= 1) ? adv_east(p, xs - 1, y, z) : 0.0f;
+  // the velocities of this thread's cell, one step ahead
+  auto ldU = [&](const float* f, int xx) { return (live && xx < xe) ? f[xx * plane + qi] : 0.0f; };
+  float uN = ldU(p.utau, xs), vN = ldU(p.vtau, xs), wN = ldU(p.wtau, xs);
   for (int x = xs; x < xe; x++) {
     const int64_t i = x * plane + qi;
     sT[t] = T1;
     sW[t] = W1;
     const float nT = ldT(x + 3), nW = ldW(x + 3);  // next step's window end
+    const float uC = uN, vC = vN, wC = wN;
+    uN = ldU(p.utau, x + 1);
+    vN = ldU(p.vtau, x + 1);
+    wN = ldU(p.wtau, x + 1);
     __syncthreads();
     float fe = 0.0f, fn = 0.0f, ft = 0.0f;
     if (live) {
       const bool xint = x >= 2 && x < p.X - 2;
       if (x >= 1 && x < p.X - 2 && yint) {
         const bool in = x < p.X - 1;
-        fe = calcflux(1.0f, p.utau[i], kDtTracer, M_(cy, p.dxt[x]), T1, T0, T2, T3, in ? M_(W1, W2) : 0.0f,
+        fe = calcflux(1.0f, uC, kDtTracer, M_(cy, p.dxt[x]), T1, T0, T2, T3, in ? M_(W1, W2) : 0.0f,
                       in ? M_(W0, W1) : 0.0f, in ? M_(W2, W3) : 0.0f);
       }
       if (y >= 1 && y < p.Y - 2 && xint) {
@@ -225,7 +232,7 @@ __global__ void __launch_bounds__(kAdvThreads, 4) tke_advect_kernel(TkeArgs p, i
           wp2 = p.maskW[i + 2 * Z];
         }
         const bool in = y < p.Y - 1;
-        fn = calcflux(cuy, p.vtau[i], kDtTracer, M_(cy, dyt), T1, tm, tp1, tp2, in ? M_(W1, wp1) : 0.0f,
+        fn = calcflux(cuy, vC, kDtTracer, M_(cy, dyt), T1, tm, tp1, tp2, in ? M_(W1, wp1) : 0.0f,
                       in ? M_(wm, W1) : 0.0f, in ? M_(wp1, wp2) : 0.0f);
       }
       if (z < Z - 1 && xint && yint) {
@@ -253,7 +260,7 @@ __global__ void __launch_bounds__(kAdvThreads, 4) tke_advect_kernel(TkeArgs p, i
             wp2 = p.maskW[i + 2];
           }
         }
-        ft = calcflux(1.0f, p.wtau[i], kDtTracer, dz, T1, tm, tp1, tp2, M_(W1, wp1), M_(wm, W1), M_(wp1, wp2));
+        ft = calcflux(1.0f, wC, kDtTracer, dz, T1, tm, tp1, tp2, M_(W1, wp1), M_(wm, W1), M_(wp1, wp2));
       }
     }
     sfn[t] = fn;
