@@ -130,29 +130,6 @@ __device__ __forceinline__ float adv_east(const TkeArgs& p, int x, int y, int z)
                   p.tketau[i3(p, x + 1, y, z)], p.tketau[i3(p, x + 2, y, z)], in ? M_(mWs, mWp1) : 0.0f,
                   in ? M_(mWm1, mWs) : 0.0f, in ? M_(mWp1, mWp2) : 0.0f);
 }
-__device__ __forceinline__ float adv_north(const TkeArgs& p, int x, int y, int z) {
-  if (!(y >= 1 && y < p.Y - 2 && x >= 2 && x < p.X - 2)) return 0.0f;
-  const int64_t i = i3(p, x, y, z);
-  const float dx = M_(p.cost[y], p.dyt[y]);
-  const float mWm1 = p.maskW[i3(p, x, y - 1, z)], mWs = p.maskW[i], mWp1 = p.maskW[i3(p, x, y + 1, z)],
-              mWp2 = p.maskW[i3(p, x, y + 2, z)];
-  const bool in = y < p.Y - 1;
-  return calcflux(p.cosu[y], p.vtau[i], kDtTracer, dx, p.tketau[i], p.tketau[i3(p, x, y - 1, z)],
-                  p.tketau[i3(p, x, y + 1, z)], p.tketau[i3(p, x, y + 2, z)], in ? M_(mWs, mWp1) : 0.0f,
-                  in ? M_(mWm1, mWs) : 0.0f, in ? M_(mWp1, mWp2) : 0.0f);
-}
-__device__ __forceinline__ float adv_top(const TkeArgs& p, int x, int y, int z) {
-  if (!(z < p.Z - 1 && interior(p, x, y))) return 0.0f;
-  const int64_t i = i3(p, x, y, z);
-  const float varSM1 = z != 0 ? p.tketau[i - 1] : 0.0f;
-  const float varSP2 = z < p.Z - 2 ? p.tketau[i + 2] : 0.0f;
-  const float mWm1 = z != 0 ? p.maskW[i - 1] : 0.0f;
-  const float mWs = p.maskW[i], mWp1 = p.maskW[i + 1];
-  const float mWp2 = z < p.Z - 2 ? p.maskW[i + 2] : 0.0f;
-  return calcflux(1.0f, p.wtau[i], kDtTracer, p.dzw[z], p.tketau[i], varSM1, p.tketau[i + 1], varSP2,
-                  M_(mWs, mWp1), M_(mWm1, mWs), M_(mWp1, mWp2));
-}
-
 // ---------------------------------------------------------------------------
 // tke_advect_kernel
 // ---------------------------------------------------------------------------
@@ -160,17 +137,19 @@ constexpr int kAdvThreads = 256;  // at <= 64 registers two CTAs fit beside two 
 
 // Block b.x covers a tile of ty rows (y) x tz levels (z) of the plane --
 // thread t at (t / tz, t % tz), z fastest, ty * tz <= kAdvThreads, the z
-// extent split into nzt tiles of at most 32 -- and block b.y the x segment
+// extent split into nzt tiles of at most 31 owned levels, row 0 and level 0
+// of a tile being halo -- and block b.y the x segment
 // [b.y * xseg, ...).  A thread keeps tketau and maskW of x - 1 .. x + 2 at
 // its (y, z) in registers (the east flux, :264-281) and publishes those of x
 // in shared memory, where its neighbours (y +- 1, y + 2) and (z +- 1, z + 2)
 // read them for the north (:282-299) and top (:300-319) fluxes -- from
 // global memory where the neighbour is outside the tile.  The north flux of
 // (y - 1, z) is thread t - tz's and the top flux of (y, z - 1) thread
-// t - 1's, again through shared memory; the tile's first row (resp. first
-// level) evaluates that neighbour's flux itself.  Tiles (rather than runs of
-// consecutive (y, z)) keep most north neighbours in the block when zdim is
-// large: with zdim = 100, 2.56 rows of 256 threads held none of them.
+// t - 1's, again through shared memory, for every owned cell: the halo row
+// and level compute those fluxes in the same code as everyone else.  Tiles
+// (rather than runs of consecutive (y, z)) keep most north neighbours in the
+// block when zdim is large: with zdim = 100, 2.56 rows of 256 threads held
+// none of them.
 __global__ void __launch_bounds__(kAdvThreads, 4) tke_advect_kernel(TkeArgs p, int xseg, int ty, int tz, int nzt) {
   __shared__ float sT[kAdvThreads], sW[kAdvThreads], sfn[kAdvThreads], sft[kAdvThreads];
   const int t = threadIdx.x;
@@ -178,8 +157,13 @@ __global__ void __launch_bounds__(kAdvThreads, 4) tke_advect_kernel(TkeArgs p, i
   const int Z = p.Z;
   const int ry = t / tz, rz = t - ry * tz;  // position in the tile
   const int yt = blockIdx.x / nzt, zt = blockIdx.x - yt * nzt;
-  const int yy = yt * ty + ry, zz = zt * tz + rz;
-  const bool live = ry < ty && yy < p.Y && zz < Z;
+  // row 0 and level 0 of the tile are halo: the cells just below the owned
+  // (ty - 1) x (tz - 1) ones, whose north and top fluxes the owned cells
+  // need; they run the same flux code, so no warp evaluates a neighbour's
+  // flux on a divergent path
+  const int yy = yt * (ty - 1) + ry - 1, zz = zt * (tz - 1) + rz - 1;
+  const bool live = ry < ty && yy >= 0 && yy < p.Y && zz >= 0 && zz < Z;
+  const bool owned = live && ry >= 1 && rz >= 1;
   const int y = live ? yy : 0, z = live ? zz : 0;
   const int64_t qi = (int64_t)y * Z + z;
   const int xs = blockIdx.y * xseg, xe = min(p.X, xs + xseg);
@@ -266,9 +250,9 @@ __global__ void __launch_bounds__(kAdvThreads, 4) tke_advect_kernel(TkeArgs p, i
     sfn[t] = fn;
     sft[t] = ft;
     __syncthreads();
-    if (live) {  // dtketau (:320-340)
-      const float fnm = ry >= 1 ? sfn[t - tz] : (y >= 1 ? adv_north(p, x, y - 1, z) : 0.0f);
-      const float ftm = rz >= 1 ? sft[t - 1] : (z >= 1 ? adv_top(p, x, y, z - 1) : 0.0f);
+    if (owned) {  // dtketau (:320-340)
+      const float fnm = sfn[t - tz];  // the north flux of (y - 1, z): 0 outside the domain
+      const float ftm = sft[t - 1];   // the top flux of (y, z - 1)
       float tmp;
       if (x >= 2 && x < p.X - 2 && yint)
         tmp = M_(W1, S_(D_(-S_(fe, fe_prev), M_(cy, p.dxt[x])), D_(S_(fn, fnm), M_(cy, dyt))));
@@ -653,10 +637,10 @@ int step_launch(futhark_context* ctx, const tke_step_args* q) {
   tke_column_kernel<<<(unsigned)col_blocks, 32 * kColWarps, kColSmem, s>>>(p);
   e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(ctx, e, "tke column launch");
-  // advection and dtketau: (y, z) tiles of at most 32 levels, x segments so
-  // that about four waves of CTAs run
-  const int64_t nzt = (Z + 31) / 32, tz = (Z + nzt - 1) / nzt, ty = kAdvThreads / tz;
-  const int64_t plane_blocks = ((Y + ty - 1) / ty) * nzt;
+  // advection and dtketau: (y, z) tiles of at most 31 owned levels plus a
+  // halo level and a halo row, x segments so that about four waves of CTAs run
+  const int64_t nzt = (Z + 30) / 31, tz = (Z + nzt - 1) / nzt + 1, ty = kAdvThreads / tz;
+  const int64_t plane_blocks = ((Y + ty - 2) / (ty - 1)) * nzt;
   const int64_t want_blocks = 4LL * 4 * ctx->num_sms;  // four CTAs per SM
   const int64_t nseg = std::max<int64_t>(1, std::min<int64_t>(X, (want_blocks + plane_blocks - 1) / plane_blocks));
   const int xseg = (int)((X + nseg - 1) / nseg);
