@@ -13,6 +13,7 @@
 //     the classes forked over several streams (largest class first) so their
 //     tails overlap, captured once into a CUDA graph.
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>  // the driver's cuTensorMapEncodeTiled signature
 
 #include <algorithm>
 #include <chrono>
@@ -2606,10 +2607,62 @@ int tridag_check_locked(futhark_context* ctx) {
 // ctx->mu held.  m <= 256: the tensor-memory kernel; m <= 400: the
 // streaming kernel, no scratch; larger m: scratch from the context's device
 // pool (stream-ordered: every user of that pool runs on ctx->stream).
+// cuTensorMapEncodeTiled from the driver, looked up once through the runtime
+// (the library does not link against the driver library itself); null where
+// the driver does not offer it.
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  return fn;
+}
+
+// The [rows / 4][4m] group view of one input of a batch with odd m and
+// rows % 4 == 0, in boxes of kTriTmaGroups groups x kTriTmaBox floats
+// (lvc_tridag_tma_kernel); false where it cannot be made (no encoder, a base
+// address off the 16-byte grid the tensor copies need).
+bool tri_group_map(CUtensorMap* map, const float* p, int64_t rows, int64_t m) {
+  const PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  if (!enc || (reinterpret_cast<uintptr_t>(p) & 15u) != 0) return false;
+  const cuuint64_t dims[2] = {(cuuint64_t)(4 * m), (cuuint64_t)(rows / 4)};
+  const cuuint64_t strides[1] = {(cuuint64_t)(4 * m) * sizeof(float)};
+  const cuuint32_t box[2] = {(cuuint32_t)kTriTmaBox, (cuuint32_t)kTriTmaGroups};
+  const cuuint32_t estr[2] = {1, 1};
+  return enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(p), dims, strides, box, estr,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 int tridag_launch(futhark_context* ctx, int form, int64_t rows, int64_t m, const float* a, const float* b,
                   const float* c, const float* y, float* out) {
   if (rows < 0 || m < 0 || m > INT32_MAX) return set_error(ctx, FUTHARK_PROGRAM_ERROR, "bad tridiagonal batch shape");
   if (rows == 0 || m == 0) return 0;
+  if (m <= kTriTmemMaxM && (m & 1) && rows % 4 == 0 && rows / 4 <= INT32_MAX - kTriTmaGroups) {
+    // odd m: inputs staged for the whole CTA by tensor copies of 4-system groups
+    CUtensorMap maps[4];
+    const float* src[4] = {a, b, c, y};
+    bool ok = true;
+    for (int i = 0; i < 4 && ok; i++) ok = tri_group_map(&maps[i], src[i], rows, m);
+    if (ok) {
+      const int64_t nblk = (rows + 32 * kTriTmemWarps - 1) / (32 * kTriTmemWarps);
+      const int cols = tri_tmem_cols((int)m);
+      auto fk = cols == 256 ? (form == 0 ? lvc_tridag_tma_kernel<0, 256> : lvc_tridag_tma_kernel<1, 256>)
+                            : (form == 0 ? lvc_tridag_tma_kernel<0, 512> : lvc_tridag_tma_kernel<1, 512>);
+      const size_t smem = tri_tma_smem(cols);
+      LVC_CUDA(ctx, cudaFuncSetAttribute((const void*)fk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      fk<<<(unsigned)nblk, 32 * kTriTmemWarps, smem, ctx->stream>>>(maps[0], maps[1], maps[2], maps[3], rows,
+                                                                     (int)m, out);
+      const cudaError_t e = cudaGetLastError();
+      if (e != cudaSuccess) return cuda_fail(ctx, e, "tridiagonal launch");
+      return 0;
+    }
+  }
   if (m <= kTriTmemMaxM) {  // intermediates in tensor memory, four warps per CTA
     const int64_t nblk = (rows + 32 * kTriTmemWarps - 1) / (32 * kTriTmemWarps);
     if (nblk > INT32_MAX) return set_error(ctx, FUTHARK_PROGRAM_ERROR, "tridiagonal batch too large");

@@ -7,12 +7,14 @@
 //           4-tuple matrix scan for the pivots, two linear-function scans --
 //           folded left to right.
 //
-// Three kernels, one thread per system in each: for m up to 256 (the
+// Four kernels, one thread per system in each: for m up to 256 (the
 // benchmark's 115 among them) lvc_tridag_tmem_kernel streams a warp's 32
 // systems through shared-memory windows and keeps the row intermediates in
-// tensor memory; for m up to 400 lvc_tridag_stream_kernel streams them the
+// tensor memory, and lvc_tridag_tma_kernel does the same with the windows
+// of the CTA's 128 systems brought in by tensor copies (odd m, rows a
+// multiple of 4); for m up to 400 lvc_tridag_stream_kernel streams them the
 // same way and keeps the intermediates in shared memory; lvc_tridag_kernel
-// (any m) reads rows in place.  All three take both forms.
+// (any m) reads rows in place.  All four take both forms.
 // Each recurrence runs in the reference's operation
 // order with every product, sum and quotient explicitly rounded (no fused
 // multiply-add), so a system's solution is bit for bit the one the CPU
@@ -25,6 +27,8 @@
 // consecutive addresses -- and the right-hand side of the backward pass in the
 // output row itself.
 #pragma once
+
+#include <cuda.h>  // CUtensorMap
 
 #include <cstdint>
 
@@ -462,6 +466,145 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
   for (int k = 0; k < 16; k++) v[k] = __uint_as_float(r[k]);
 }
 
+// The forward state of one system (FORM 0: cp, yp; FORM 1: the 4-tuple
+// scan s, b_0, c_{i-1}, the linear scan (c0, c1), y_0, b'_{i-1}, and the
+// last quotient y'_{m-1} / b'_{m-1} that starts the backward fold).
+struct TriFwd {
+  float cp = 0.0f, yp = 0.0f;
+  float s0 = 1.0f, s1 = 0.0f, s2 = 0.0f, s3 = 1.0f, b0 = 0.0f, cprev = 0.0f;
+  float y0 = 0.0f, c0 = 0.0f, c1 = 1.0f, bprev = 0.0f, yn = 0.0f;
+};
+
+// Window q (elements q * kTriWin + k) of a system's forward pass, its inputs
+// a, b, c, y at w[k], w[as + k], w[2 as + k], w[3 as + k]; the two
+// intermediates of each element go to v[2k], v[2k + 1].  FULL: a window
+// after the first that ends before element m - 1 (tri_full_window), run
+// without a condition per element -- lanes past the last system compute on
+// the zeros their windows hold, and nothing reads their results -- so the
+// window's loads issue ahead of the recurrence instead of one element at a
+// time behind its branch.
+__device__ __forceinline__ bool tri_full_window(int q, int m) { return q >= 1 && q * kTriWin + kTriWin < m; }
+template <int FORM, bool FULL = false>
+__device__ __forceinline__ void tri_forward_window(TriFwd& f, const float* w, int as, int q, int m, bool act,
+                                                   float (&v)[16]) {
+#pragma unroll
+  for (int k = 0; k < kTriWin; k++) {
+    const int i = q * kTriWin + k;
+    v[2 * k] = 0.0f;
+    v[2 * k + 1] = 0.0f;
+    if (FULL || (act && i < m)) {
+      const float ai = w[k], bi = w[as + k], ci = w[2 * as + k], yi = w[3 * as + k];
+      if constexpr (FORM == 0) {
+        // cp_i = c_i / (b_i - a_i cp_{i-1}), yp_i = (y_i - a_i yp_{i-1}) / (...)  (:82-91)
+        if (!FULL && i == 0) {
+          f.cp = tri_div(ci, bi);
+          f.yp = tri_div(yi, bi);
+        } else {
+          const float nf = tri_rcp(tri_sub(bi, tri_mul(ai, f.cp)));
+          f.cp = tri_mul(ci, nf);
+          f.yp = tri_mul(tri_sub(yi, tri_mul(ai, f.yp)), nf);
+        }
+        v[2 * k] = f.cp;
+        v[2 * k + 1] = f.yp;
+      } else {
+        // recurrence 1 (:9-33): b'_i from the 4-tuple scan of (b_i, -a_i c_{i-1}, 1, 0)
+        if (!FULL && i == 0) {
+          f.b0 = bi;
+          f.y0 = yi;
+        }
+        float m0 = 1.0f, m1 = 0.0f, m2 = 0.0f, m3 = 1.0f;
+        if (FULL || 0 < i) {
+          m0 = bi;
+          m1 = tri_sub(0.0f, tri_mul(ai, f.cprev));
+          m2 = 1.0f;
+          m3 = 0.0f;
+        }
+        f.cprev = ci;
+        const float value = tri_rcp(tri_mul(f.s0, m0));
+        const float n0 = tri_mul(tri_add(tri_mul(m0, f.s0), tri_mul(m1, f.s2)), value);
+        const float n1 = tri_mul(tri_add(tri_mul(m0, f.s1), tri_mul(m1, f.s3)), value);
+        const float n2 = tri_mul(tri_add(tri_mul(m2, f.s0), tri_mul(m3, f.s2)), value);
+        const float n3 = tri_mul(tri_add(tri_mul(m2, f.s1), tri_mul(m3, f.s3)), value);
+        f.s0 = n0;
+        f.s1 = n1;
+        f.s2 = n2;
+        f.s3 = n3;
+        const float bpi = tri_div(tri_add(tri_mul(f.s0, f.b0), f.s1), tri_add(tri_mul(f.s2, f.b0), f.s3));  // b'_i
+        // recurrence 2 (:38-56): y'_i from the scan of (y_i, -a_i / b'_{i-1})
+        float l0 = 0.0f, l1 = 1.0f;
+        if (FULL || 0 < i) {
+          l0 = yi;
+          l1 = tri_sub(0.0f, tri_div(ai, f.bprev));
+        }
+        const float e0 = tri_add(l0, tri_mul(l1, f.c0));
+        const float e1 = tri_mul(f.c1, l1);
+        f.c0 = e0;
+        f.c1 = e1;
+        const float ypi = tri_add(f.c0, tri_mul(f.c1, f.y0));  // y'_i
+        f.bprev = bpi;
+        // recurrence 3's elements (:61-79), the last one's first component
+        // its starting value
+        if (FULL || i < m - 1) {
+          v[2 * k] = tri_div(ypi, bpi);
+          v[2 * k + 1] = tri_sub(0.0f, tri_div(ci, bpi));
+        } else {
+          f.yn = tri_div(ypi, bpi);
+        }
+      }
+    }
+  }
+}
+
+// The backward pass of a warp's nr systems (rows r0 ..), the intermediates
+// read back from the warp's lane quarter of tensor memory (tl, column 0) a
+// window at a time; the solution leaves through the output window Wo as
+// 32-byte runs of rows.
+template <int FORM>
+__device__ __forceinline__ void tri_backward(TriFwd& f, uint32_t tl, float* Wo, int lane, int nr, int m, int64_t r0,
+                                             float* __restrict__ out) {
+  constexpr int WS = kTriWin + 1;
+  const bool act = lane < nr;
+  const int nq = (m + kTriWin - 1) / kTriWin;
+  float x = f.yp;  // FORM 0: x_{m-1} = yp_{m-1}
+  f.c0 = 0.0f;
+  f.c1 = 1.0f;
+  for (int q = nq - 1; q >= 0; q--) {
+    float v[16];
+    tmem_ld16(tl + 16 * q, v);
+    const bool full = tri_full_window(q, m);  // no element of the window is past m - 2: no condition per element
+#pragma unroll
+    for (int k = kTriWin - 1; k >= 0; k--) {
+      const int i = q * kTriWin + k;
+      if (full || (act && i < m)) {
+        if constexpr (FORM == 0) {
+          // x_i = yp_i - cp_i x_{i+1}  (:92-95)
+          if (full || i < m - 1) x = tri_sub(v[2 * k + 1], tri_mul(v[2 * k], x));
+          Wo[lane * WS + k] = x;
+        } else {
+          float l0 = 0.0f, l1 = 1.0f;
+          if (full || i < m - 1) {
+            l0 = v[2 * k];
+            l1 = v[2 * k + 1];
+          }
+          const float n0 = tri_add(l0, tri_mul(l1, f.c0));
+          const float n1 = tri_mul(f.c1, l1);
+          f.c0 = n0;
+          f.c1 = n1;
+          Wo[lane * WS + k] = tri_add(f.c0, tri_mul(f.c1, f.yn));
+        }
+      }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int t = 0; t < kTriWin; t++) {
+      const int idx = t * 32 + lane, row = idx / kTriWin, col = idx % kTriWin;
+      const int gcol = q * kTriWin + col;
+      if (row < nr && gcol < m) __stcs(out + (r0 + row) * (int64_t)m + gcol, Wo[row * WS + col]);
+    }
+    __syncwarp();  // the output window is rewritten next iteration
+  }
+}
+
 template <int FORM, int COLS>
 __global__ void __launch_bounds__(32 * kTriTmemWarps) lvc_tridag_tmem_kernel(int64_t rows, int m,
                                                                              const float* __restrict__ a,
@@ -508,128 +651,143 @@ __global__ void __launch_bounds__(32 * kTriTmemWarps) lvc_tridag_tmem_kernel(int
       }
       cp_async_commit();
     };
-    // -------- forward --------
-    float cp = 0.0f, yp = 0.0f;                                               // FORM 0
-    float s0 = 1.0f, s1 = 0.0f, s2 = 0.0f, s3 = 1.0f, b0 = 0.0f, cprev = 0.0f;  // FORM 1
-    float y0 = 0.0f, c0 = 0.0f, c1 = 1.0f, bprev = 0.0f, yn = 0.0f;
+    TriFwd f;
     fetch(0);
     fetch(1);
     for (int q = 0; q < nq; q++) {
       fetch(q + 2);
       cp_async_wait<2>();  // window q has landed
       __syncwarp();
-      const float* w = Wn + (q % kTriTmemStages) * WB + lane * WS;
       float v[16];
-#pragma unroll
-      for (int k = 0; k < kTriWin; k++) {
-        const int i = q * kTriWin + k;
-        v[2 * k] = 0.0f;
-        v[2 * k + 1] = 0.0f;
-        if (act && i < m) {
-          const float ai = w[k], bi = w[WA + k], ci = w[2 * WA + k], yi = w[3 * WA + k];
-          if constexpr (FORM == 0) {
-            // cp_i = c_i / (b_i - a_i cp_{i-1}), yp_i = (y_i - a_i yp_{i-1}) / (...)  (:82-91)
-            if (i == 0) {
-              cp = tri_div(ci, bi);
-              yp = tri_div(yi, bi);
-            } else {
-              const float nf = tri_rcp(tri_sub(bi, tri_mul(ai, cp)));
-              cp = tri_mul(ci, nf);
-              yp = tri_mul(tri_sub(yi, tri_mul(ai, yp)), nf);
-            }
-            v[2 * k] = cp;
-            v[2 * k + 1] = yp;
-          } else {
-            // recurrence 1 (:9-33): b'_i from the 4-tuple scan of (b_i, -a_i c_{i-1}, 1, 0)
-            if (i == 0) {
-              b0 = bi;
-              y0 = yi;
-            }
-            float m0 = 1.0f, m1 = 0.0f, m2 = 0.0f, m3 = 1.0f;
-            if (0 < i) {
-              m0 = bi;
-              m1 = tri_sub(0.0f, tri_mul(ai, cprev));
-              m2 = 1.0f;
-              m3 = 0.0f;
-            }
-            cprev = ci;
-            const float value = tri_rcp(tri_mul(s0, m0));
-            const float n0 = tri_mul(tri_add(tri_mul(m0, s0), tri_mul(m1, s2)), value);
-            const float n1 = tri_mul(tri_add(tri_mul(m0, s1), tri_mul(m1, s3)), value);
-            const float n2 = tri_mul(tri_add(tri_mul(m2, s0), tri_mul(m3, s2)), value);
-            const float n3 = tri_mul(tri_add(tri_mul(m2, s1), tri_mul(m3, s3)), value);
-            s0 = n0;
-            s1 = n1;
-            s2 = n2;
-            s3 = n3;
-            const float bpi = tri_div(tri_add(tri_mul(s0, b0), s1), tri_add(tri_mul(s2, b0), s3));  // b'_i
-            // recurrence 2 (:38-56): y'_i from the scan of (y_i, -a_i / b'_{i-1})
-            float l0 = 0.0f, l1 = 1.0f;
-            if (0 < i) {
-              l0 = yi;
-              l1 = tri_sub(0.0f, tri_div(ai, bprev));
-            }
-            const float e0 = tri_add(l0, tri_mul(l1, c0));
-            const float e1 = tri_mul(c1, l1);
-            c0 = e0;
-            c1 = e1;
-            const float ypi = tri_add(c0, tri_mul(c1, y0));  // y'_i
-            bprev = bpi;
-            // recurrence 3's elements (:61-79), the last one's first component
-            // its starting value
-            if (i < m - 1) {
-              v[2 * k] = tri_div(ypi, bpi);
-              v[2 * k + 1] = tri_sub(0.0f, tri_div(ci, bpi));
-            } else {
-              yn = tri_div(ypi, bpi);
-            }
-          }
-        }
-      }
+      const float* const w = Wn + (q % kTriTmemStages) * WB + lane * WS;
+      if (tri_full_window(q, m))
+        tri_forward_window<FORM, true>(f, w, WA, q, m, act, v);
+      else
+        tri_forward_window<FORM>(f, w, WA, q, m, act, v);
       tmem_st16(tl + 16 * q, v);
       __syncwarp();  // this ring stage is refilled by the next iteration's fetch
     }
     cp_async_wait<0>();
     tmem_wait_st();
-    // -------- backward --------
-    float x = yp;  // FORM 0: x_{m-1} = yp_{m-1}
-    c0 = 0.0f;
-    c1 = 1.0f;
-    for (int q = nq - 1; q >= 0; q--) {
-      float v[16];
-      tmem_ld16(tl + 16 * q, v);
-#pragma unroll
-      for (int k = kTriWin - 1; k >= 0; k--) {
-        const int i = q * kTriWin + k;
-        if (act && i < m) {
-          if constexpr (FORM == 0) {
-            // x_i = yp_i - cp_i x_{i+1}  (:92-95)
-            if (i < m - 1) x = tri_sub(v[2 * k + 1], tri_mul(v[2 * k], x));
-            Wo[lane * WS + k] = x;
-          } else {
-            float l0 = 0.0f, l1 = 1.0f;
-            if (i < m - 1) {
-              l0 = v[2 * k];
-              l1 = v[2 * k + 1];
-            }
-            const float n0 = tri_add(l0, tri_mul(l1, c0));
-            const float n1 = tri_mul(c1, l1);
-            c0 = n0;
-            c1 = n1;
-            Wo[lane * WS + k] = tri_add(c0, tri_mul(c1, yn));
-          }
-        }
-      }
-      __syncwarp();
-#pragma unroll
-      for (int t = 0; t < kTriWin; t++) {
-        const int idx = t * 32 + lane, row = idx / kTriWin, col = idx % kTriWin;
-        const int gcol = q * kTriWin + col;
-        if (row < nr && gcol < m) __stcs(out + (r0 + row) * (int64_t)m + gcol, Wo[row * WS + col]);
-      }
-      __syncwarp();  // the output window is rewritten next iteration
-    }
+    tri_backward<FORM>(f, tl, Wo, lane, nr, m, r0, out);
   }
+  tmem_fence_before_sync();
+  __syncthreads();
+  tmem_fence_after_sync();
+  if (warp == 0) tmem_dealloc(*s_taddr, COLS);
+}
+
+// The same solver with the inputs staged by the tensor-memory accelerator
+// (TMA) for the whole CTA, for odd m (up to kTriTmemMaxM) and rows % 4 == 0.
+// Four consecutive systems of such a batch are one contiguous run of 4m
+// floats whose start is 16-byte aligned (16m bytes apart), so each input is
+// viewed as a 2-D tensor of rows / 4 "groups" of 4m floats.  Window q of
+// system s of a group (elements 8q .. 8q + 7, at 4m-offset m s + 8q) lies
+// inside the 12 floats from the 16-byte boundary at or below it, offset
+// (m s) mod 4; one tensor copy per array and s brings that 12-float box of
+// the CTA's 32 groups into shared memory, [s][group][12] -- sixteen copies
+// per window for the CTA's 128 systems, issued by one thread, against 32
+// four-byte cp.async per lane and array.  Lane l of warp w owns system
+// 4 (8w + l / 4) + l % 4 and reads its elements at group 8w + l / 4 of box
+// l % 4: with m odd the offsets (m s) mod 4 of the four boxes are distinct
+// and 12 (8w + g) mod 32 runs over distinct multiples of 4, so a warp's
+// reads are free of bank conflicts.  Three stages; a stage is refilled
+// after the CTA barrier that follows every warp's last read of it, and
+// each window's copies land on that stage's mbarrier (bounded waits).
+// Every warp runs the forward loop (the barriers need all of them); warps
+// past the last system compute nothing.
+constexpr int kTriTmaBox = 12;                                        // floats per box row
+constexpr int kTriTmaGroups = 8 * kTriTmemWarps;                      // 4-system groups per CTA
+constexpr int kTriTmaStageFloats = 4 * 4 * kTriTmaGroups * kTriTmaBox;  // [array][s][group][box]
+__host__ __device__ __forceinline__ size_t tri_tma_smem(int cols) {
+  const size_t need = 128 /* alignment */ + 128 /* barriers, TMEM address */ +
+                      sizeof(float) * (kTriTmemStages * (size_t)kTriTmaStageFloats + kTriTmemWarps * 32 * (kTriWin + 1));
+  const size_t pad = cols > 256 ? 150 * 1024 : 80 * 1024;  // as tri_tmem_smem: at most 512 columns per SM
+  return need > pad ? need : pad;
+}
+__device__ __forceinline__ void tma_load_2d(float* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n" ::"r"(
+          smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+
+template <int FORM, int COLS>
+__global__ void __launch_bounds__(32 * kTriTmemWarps) lvc_tridag_tma_kernel(const __grid_constant__ CUtensorMap ta,
+                                                                            const __grid_constant__ CUtensorMap tb,
+                                                                            const __grid_constant__ CUtensorMap tc,
+                                                                            const __grid_constant__ CUtensorMap ty,
+                                                                            int64_t rows, int m,
+                                                                            float* __restrict__ out) {
+  extern __shared__ __align__(16) unsigned char tri_raw[];
+  constexpr int WS = kTriWin + 1, AS = 4 * kTriTmaGroups * kTriTmaBox, SS = kTriTmaGroups * kTriTmaBox;
+  const uint32_t raw = smem_u32(tri_raw);
+  unsigned char* const base = tri_raw + (((raw + 127u) & ~127u) - raw);  // 128-byte aligned
+  uint64_t* const full = reinterpret_cast<uint64_t*>(base);                // [kTriTmemStages]
+  uint32_t* const s_taddr = reinterpret_cast<uint32_t*>(base + 64);        // written by tcgen05.alloc
+  float* const stage0 = reinterpret_cast<float*>(base + 128);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float* const Wo = stage0 + kTriTmemStages * kTriTmaStageFloats + warp * 32 * WS;  // output window
+  const int64_t r0 = ((int64_t)blockIdx.x * kTriTmemWarps + warp) * 32;
+  const int nr = r0 < rows ? (int)(rows - r0 < 32 ? rows - r0 : 32) : 0;
+  const int g0 = blockIdx.x * kTriTmaGroups;  // the CTA's first group
+  const int nq = (m + kTriWin - 1) / kTriWin;
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < kTriTmemStages; i++) mbar_init(&full[i], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  if (warp == 0) {
+    tmem_alloc(s_taddr, COLS);
+    tmem_relinquish();
+  }
+  tmem_fence_before_sync();
+  __syncthreads();
+  tmem_fence_after_sync();
+  const uint32_t tl = *s_taddr + ((uint32_t)(32 * (warp & 3)) << 16);  // this warp's lane quarter, column 0
+  const CUtensorMap* maps[4] = {&ta, &tb, &tc, &ty};
+  auto issue = [&](int q) {  // thread 0: window q into stage q % kTriTmemStages
+    if (q < nq) {
+      const int st = q % kTriTmemStages;
+      float* const dst = stage0 + st * kTriTmaStageFloats;
+      mbar_expect_tx(&full[st], (unsigned)(sizeof(float) * kTriTmaStageFloats));
+#pragma unroll
+      for (int arr = 0; arr < 4; arr++)
+#pragma unroll
+        for (int s = 0; s < 4; s++)
+          tma_load_2d(dst + arr * AS + s * SS, maps[arr], (m * s + kTriWin * q) & ~3, g0, &full[st]);
+    }
+  };
+  const int s = lane & 3;
+  const float* const mine = stage0 + s * SS + (8 * warp + (lane >> 2)) * kTriTmaBox + ((m * s) & 3);
+  const bool act = lane < nr;
+  bool timed_out = false;
+  TriFwd f;
+  if (threadIdx.x == 0) {
+    issue(0);
+    issue(1);
+  }
+  for (int q = 0; q < nq; q++) {
+    __syncthreads();  // every warp is done with window q - 1, whose stage window q + 2 refills
+    if (threadIdx.x == 0) issue(q + 2);
+    if (!mbar_wait(&full[q % kTriTmemStages], (unsigned)(q / kTriTmemStages) & 1u,
+                   timed_out ? kWaitPollsAfterTimeout : kWaitPolls)) {
+      timed_out = true;
+      atomicExch(&lvc_tridag_err, 1);
+    }
+    float v[16];
+    const float* const w = mine + (q % kTriTmemStages) * kTriTmaStageFloats;
+    if (tri_full_window(q, m))
+      tri_forward_window<FORM, true>(f, w, AS, q, m, act, v);
+    else
+      tri_forward_window<FORM>(f, w, AS, q, m, act, v);
+    tmem_st16(tl + 16 * q, v);
+  }
+  if (timed_out && threadIdx.x == 0)  // a copy that never landed: give the last ones one more bounded wait
+    for (int q = nq > kTriTmemStages ? nq - kTriTmemStages : 0; q < nq; q++)
+      mbar_wait(&full[q % kTriTmemStages], (unsigned)(q / kTriTmemStages) & 1u, kWaitPolls);
+  tmem_wait_st();
+  if (nr > 0) tri_backward<FORM>(f, tl, Wo, lane, nr, m, r0, out);
   tmem_fence_before_sync();
   __syncthreads();
   tmem_fence_after_sync();

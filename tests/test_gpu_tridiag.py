@@ -45,10 +45,14 @@ def test_par_matches_oracle_bit_exact_on_golden_inputs(ctx, oracle, golden_tridi
 # stanza's inner size, the tensor-memory kernel's two allocation sizes and
 # their limits (128, 256) and just above them, odd and even m, the
 # shared-memory kernels' limit (400) and the kernel with global scratch
-# above it
+# above it; rows % 4 == 0 with odd m (the tensor-copy staging of 4-system
+# groups: m = 1 and 3 with boxes wider than the group, partial and whole
+# CTAs, both allocation sizes) beside odd m with rows % 4 != 0 (the
+# per-lane window copies)
 @pytest.mark.parametrize("shape", [(0, 5), (3, 1), (7, 2), (33, 3), (129, 64), (1000, 115), (257, 128),
                                    (65, 129), (70, 200), (40, 256), (9, 257), (70, 399), (130, 400), (40, 401),
-                                   (5, 1000)])
+                                   (5, 1000), (4, 1), (8, 3), (132, 7), (260, 63), (4096, 115), (512, 129),
+                                   (36, 255), (1001, 115)])
 @pytest.mark.parametrize("form,oform", [("seq", "seq"), ("par", "par4")])
 def test_random_batches_match_oracle_bit_exact(ctx, oracle, shape, form, oform):
     rows, m = shape
