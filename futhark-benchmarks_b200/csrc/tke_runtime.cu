@@ -35,7 +35,10 @@
 // Every operation is explicitly rounded (no fused multiply-add) in the
 // reference's operand order -- the fold order of each recurrence included --
 // so the outputs equal the CPU oracle's, which reproduces the reference's
-// golden outputs, bit for bit.
+// golden outputs, bit for bit.  Quotients by a divisor that stays fixed over
+// many of them (dz of a level, cos * dy of a row, cos * dx of a step) come
+// from its double reciprocal (DR_), which gives the same correctly rounded
+// float as the division.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -63,6 +66,20 @@ __device__ __forceinline__ float D_(float a, float b) {
     return __int_as_float((__float_as_int(a) ^ __float_as_int(b)) & (int)0x80000000);
   return __fdiv_rn(a, b);
 }
+// a / b correctly rounded, from rb = 1 / (double)b correctly rounded in
+// double (Rd_): the float nearest the double product a * rb.  That product
+// is within 2^-52 of a / b relatively, while a quotient of two floats (24-bit
+// significands A, B) is never a point halfway between two floats and never
+// closer to one than 2^-49 relatively (a nonzero multiple of a power of two
+// over B < 2^24, against a result below 2^25 of the same power): the product
+// therefore rounds to float as a / b does -- the argument that makes double
+// rounding harmless when the wider format carries at least 2p + 2 bits.
+// Zeros and infinities and the signs follow from the IEEE operations
+// (0 * rb = +-0, a * inf for b = 0).  One double reciprocal then serves every
+// quotient with that divisor, each at the cost of one double multiply and
+// two conversions.
+__device__ __forceinline__ double Rd_(float b) { return __drcp_rn((double)b); }
+__device__ __forceinline__ float DR_(float a, double rb) { return __double2float_rn(__dmul_rn((double)a, rb)); }
 // std::max / std::min as the oracle evaluates them
 __device__ __forceinline__ float max_(float a, float b) { return (a < b) ? b : a; }
 __device__ __forceinline__ float min_(float a, float b) { return (b < a) ? b : a; }
@@ -91,11 +108,14 @@ __device__ __forceinline__ bool interior(const TkeArgs& p, int x, int y) {
 __device__ __forceinline__ float limiter(float cr) {
   return max_(0.0f, max_(min_(1.0f, M_(2.0f, cr)), min_(2.0f, cr)));
 }
-__device__ __forceinline__ float calcflux(float velfac, float velS, float dt_tracer, float dx, float varS,
-                                          float varSM1, float varSP1, float varSP2, float maskS, float maskSM1,
-                                          float maskSP1) {
+// uCFL is |scaledVel dt_tracer / dx|: from dx itself (RECIP false) or from
+// its double reciprocal rdx (RECIP true, DR_)
+template <bool RECIP>
+__device__ __forceinline__ float calcflux(float velfac, float velS, float dt_tracer, float dx, double rdx,
+                                          float varS, float varSM1, float varSP1, float varSP2, float maskS,
+                                          float maskSM1, float maskSP1) {
   const float scaledVel = M_(velfac, velS);
-  const float uCFL = fabsf(D_(M_(scaledVel, dt_tracer), dx));
+  const float uCFL = fabsf(RECIP ? DR_(M_(scaledVel, dt_tracer), rdx) : D_(M_(scaledVel, dt_tracer), dx));
   const float rjp = M_(S_(varSP2, varSP1), maskSP1);
   const float rj = M_(S_(varSP1, varS), maskS);
   const float rjm = M_(S_(varS, varSM1), maskSM1);
@@ -126,7 +146,7 @@ __device__ __forceinline__ float adv_east(const TkeArgs& p, int x, int y, int z)
   const float mWm1 = p.maskW[i3(p, x - 1, y, z)], mWs = p.maskW[i], mWp1 = p.maskW[i3(p, x + 1, y, z)],
               mWp2 = p.maskW[i3(p, x + 2, y, z)];
   const bool in = x < p.X - 1;
-  return calcflux(1.0f, p.utau[i], kDtTracer, dx, p.tketau[i], p.tketau[i3(p, x - 1, y, z)],
+  return calcflux<false>(1.0f, p.utau[i], kDtTracer, dx, 0.0, p.tketau[i], p.tketau[i3(p, x - 1, y, z)],
                   p.tketau[i3(p, x + 1, y, z)], p.tketau[i3(p, x + 2, y, z)], in ? M_(mWs, mWp1) : 0.0f,
                   in ? M_(mWm1, mWs) : 0.0f, in ? M_(mWp1, mWp2) : 0.0f);
 }
@@ -172,6 +192,8 @@ __global__ void __launch_bounds__(kAdvThreads, 4) tke_advect_kernel(TkeArgs p, i
   const bool yint = y >= 2 && y < p.Y - 2;
   const float cy = live ? p.cost[y] : 1.0f, cuy = live ? p.cosu[y] : 1.0f, dyt = live ? p.dyt[y] : 1.0f;
   const float dz = live ? p.dzw[z] : 1.0f;
+  // the divisors that stay fixed along x, as double reciprocals (DR_)
+  const double rdy = Rd_(M_(cy, dyt)), rdz = Rd_(dz), rhdz = Rd_(M_(0.5f, dz));
   auto ldT = [&](int xx) { return (live && xx >= 0 && xx < p.X) ? p.tketau[xx * plane + qi] : 0.0f; };
   auto ldW = [&](int xx) { return (live && xx >= 0 && xx < p.X) ? p.maskW[xx * plane + qi] : 0.0f; };
   float T0 = ldT(xs - 1), T1 = ldT(xs), T2 = ldT(xs + 1), T3 = ldT(xs + 2);  // x - 1 .. x + 2
@@ -191,11 +213,12 @@ __global__ void __launch_bounds__(kAdvThreads, 4) tke_advect_kernel(TkeArgs p, i
     wN = ldU(p.wtau, x + 1);
     __syncthreads();
     float fe = 0.0f, fn = 0.0f, ft = 0.0f;
+    const double rdx = Rd_(M_(cy, p.dxt[x]));  // the east divisor of this x, for fe and dtketau
     if (live) {
       const bool xint = x >= 2 && x < p.X - 2;
       if (x >= 1 && x < p.X - 2 && yint) {
         const bool in = x < p.X - 1;
-        fe = calcflux(1.0f, uC, kDtTracer, M_(cy, p.dxt[x]), T1, T0, T2, T3, in ? M_(W1, W2) : 0.0f,
+        fe = calcflux<true>(1.0f, uC, kDtTracer, 0.0f, rdx, T1, T0, T2, T3, in ? M_(W1, W2) : 0.0f,
                       in ? M_(W0, W1) : 0.0f, in ? M_(W2, W3) : 0.0f);
       }
       if (y >= 1 && y < p.Y - 2 && xint) {
@@ -216,7 +239,7 @@ __global__ void __launch_bounds__(kAdvThreads, 4) tke_advect_kernel(TkeArgs p, i
           wp2 = p.maskW[i + 2 * Z];
         }
         const bool in = y < p.Y - 1;
-        fn = calcflux(cuy, vC, kDtTracer, M_(cy, dyt), T1, tm, tp1, tp2, in ? M_(W1, wp1) : 0.0f,
+        fn = calcflux<true>(cuy, vC, kDtTracer, 0.0f, rdy, T1, tm, tp1, tp2, in ? M_(W1, wp1) : 0.0f,
                       in ? M_(wm, W1) : 0.0f, in ? M_(wp1, wp2) : 0.0f);
       }
       if (z < Z - 1 && xint && yint) {
@@ -244,7 +267,7 @@ __global__ void __launch_bounds__(kAdvThreads, 4) tke_advect_kernel(TkeArgs p, i
             wp2 = p.maskW[i + 2];
           }
         }
-        ft = calcflux(1.0f, wC, kDtTracer, dz, T1, tm, tp1, tp2, M_(W1, wp1), M_(wm, W1), M_(wp1, wp2));
+        ft = calcflux<true>(1.0f, wC, kDtTracer, 0.0f, rdz, T1, tm, tp1, tp2, M_(W1, wp1), M_(wm, W1), M_(wp1, wp2));
       }
     }
     sfn[t] = fn;
@@ -255,12 +278,12 @@ __global__ void __launch_bounds__(kAdvThreads, 4) tke_advect_kernel(TkeArgs p, i
       const float ftm = sft[t - 1];   // the top flux of (y, z - 1)
       float tmp;
       if (x >= 2 && x < p.X - 2 && yint)
-        tmp = M_(W1, S_(D_(-S_(fe, fe_prev), M_(cy, p.dxt[x])), D_(S_(fn, fnm), M_(cy, dyt))));
+        tmp = M_(W1, S_(DR_(-S_(fe, fe_prev), rdx), DR_(S_(fn, fnm), rdy)));
       else
         tmp = p.dtketau[i];
-      const float z0 = z == 0 ? S_(tmp, D_(ft, dz)) : tmp;
-      const float zm = (z >= 1 && z < Z - 1) ? S_(z0, D_(S_(ft, ftm), dz)) : z0;
-      p.dtketau_out[i] = (z == Z - 1) ? S_(zm, D_(S_(ft, ftm), M_(0.5f, dz))) : zm;
+      const float z0 = z == 0 ? S_(tmp, DR_(ft, rdz)) : tmp;
+      const float zm = (z >= 1 && z < Z - 1) ? S_(z0, DR_(S_(ft, ftm), rdz)) : z0;
+      p.dtketau_out[i] = (z == Z - 1) ? S_(zm, DR_(S_(ft, ftm), rhdz)) : zm;
     }
     fe_prev = fe;
     T0 = T1;
@@ -362,9 +385,11 @@ __global__ void __launch_bounds__(kColWarps * 32, 4) tke_column_kernel(TkeArgs p
   float* q0 = p.q0 + col;
   float* q1 = p.q1 + col;
 
-  // Forward, a chunk of kColCh z at a time: (A) the coefficients (tke.fut:103-210),
-  // independent across z; (B) tridagPar's recurrences 1 (the 4-tuple scan
-  // for b', tridiag.fut:9-33) and 2 (y', :38-56) folded left to right --
+  // Forward, staged a chunk of kColCh z at a time and computed one z at a
+  // time (a rolled loop: the unrolled chunk body cost more than its overlap
+  // of the coefficients of neighbouring z saved): (A) the coefficients
+  // (tke.fut:103-210); (B) tridagPar's recurrences 1 (the 4-tuple scan for
+  // b', tridiag.fut:9-33) and 2 (y', :38-56) folded left to right --
   // recurrence 2 at z needs b' of z - 1 only; (C) the two quotients the
   // backward recurrence folds.  Every lane runs A and B (the shuffles need
   // the whole warp); only interior columns store.
@@ -374,6 +399,15 @@ __global__ void __launch_bounds__(kColWarps * 32, 4) tke_column_kernel(TkeArgs p
   cp_async_commit();
   if (nch > 1) col_stage_chunk(p, st + kColStageFloats, col0, ncol, 1, lane);
   cp_async_commit();
+  // the per-z constants of the next chunk, loaded a chunk ahead: lane l
+  // holds dzw and dzt of z + 1 for z = (chunk) * kColCh + l % kColCh
+  float dzN = 1.0f, dztN = 1.0f;
+  auto ld_consts = [&](int k) {
+    const int zl = k * kColCh + (lane & (kColCh - 1));
+    dzN = zl < Z ? p.dzw[zl] : 1.0f;
+    dztN = zl < Z - 1 ? p.dzt[zl + 1] : 1.0f;
+  };
+  ld_consts(0);
   for (int k = 0; k < nch; k++) {
     if (k + 2 < nch) col_stage_chunk(p, st + ((k + 2) % kColStages) * kColStageFloats, col0, ncol, k + 2, lane);
     cp_async_commit();
@@ -384,17 +418,15 @@ __global__ void __launch_bounds__(kColWarps * 32, 4) tke_column_kernel(TkeArgs p
     const int zbase = k * kColCh;
     const int zn = min(kColCh, Z - zbase);
     // the chunk's per-z constants, lane l holding those of z = zbase + l % kColCh
-    float fac_l = 0.0f, dz_l = 1.0f;
-    {
-      const int zl = zbase + (lane & (kColCh - 1));
-      if (zl < Z) dz_l = p.dzw[zl];
-      if (zl < Z - 1) fac_l = M_(M_(D_(kDtTke, p.dzt[zl + 1]), kAlphaTke), 0.5f);
-    }
-    float av[kColCh], bv[kColCh], cv[kColCh], dv[kColCh];
-#pragma unroll
-    for (int zz = 0; zz < kColCh; zz++) {  // (A)
+    const float dz_l = dzN;
+    const float fac_l = zbase + (lane & (kColCh - 1)) < Z - 1 ? M_(M_(D_(kDtTke, dztN), kAlphaTke), 0.5f) : 0.0f;
+    const double rdz_l = Rd_(dz_l);  // the quotients by dz of the interior levels (DR_)
+    if (k + 1 < nch) ld_consts(k + 1);
+#pragma unroll 1
+    for (int zz = 0; zz < zn; zz++) {  // (A), (B), (C) for one z
       const float fac = __shfl_sync(kAll, fac_l, zz);
       const float dz = __shfl_sync(kAll, dz_l, zz);
+      const double rdz = __shfl_sync(kAll, rdz_l, zz);
       const int z = zbase + zz;
       const float t = cur[zz * kColPad + lane];
       const float kap = cur[(kColCh + zz) * kColPad + lane];
@@ -405,43 +437,29 @@ __global__ void __launch_bounds__(kColWarps * 32, 4) tke_column_kernel(TkeArgs p
       const bool edge = land && z == ks, water = land && z >= ks;
       const float sq = __fsqrt_rn(max_(0.0f, t));
       float a_ = 0.0f, b_ = 0.0f, c_ = 0.0f, d_ = 0.0f;
-      // a_tri (:109-122)
       if (edge || !water) a_ = 0.0f;
-      else if (z > 0 && z < Z - 1) a_ = D_(-dm, dz);
+      else if (z > 0 && z < Z - 1) a_ = DR_(-dm, rdz);
       else if (z == Z - 1) a_ = D_(-dm, M_(0.5f, dz));
-      // b_tri (:123-146)
       if (!water) b_ = 1.0f;
-      else if (edge) b_ = A_(A_(1.0f, D_(d0, dz)), M_(D_(M_(kDtTke, kCEps), mx), sq));
-      else if (z > 0 && z < Z - 1) b_ = A_(A_(1.0f, D_(A_(d0, dm), dz)), D_(M_(M_(kDtTke, kCEps), sq), mx));
+      else if (edge) b_ = A_(A_(1.0f, DR_(d0, rdz)), M_(D_(M_(kDtTke, kCEps), mx), sq));
+      else if (z > 0 && z < Z - 1) b_ = A_(A_(1.0f, DR_(A_(d0, dm), rdz)), D_(M_(M_(kDtTke, kCEps), sq), mx));
       else if (z == Z - 1) b_ = A_(A_(1.0f, D_(dm, M_(0.5f, dz))), M_(D_(M_(kDtTke, kCEps), mx), sq));
-      // c_tri (:187-196)
-      if (z < Z - 1) c_ = water ? D_(-d0, dz) : 0.0f;
-      // d_tri (:197-210)
+      if (z < Z - 1) c_ = water ? DR_(-d0, rdz) : 0.0f;
       if (water) {
         const float tmp = A_(t, M_(kDtTke, fo));
         d_ = (z == Z - 1) ? A_(tmp, D_(M_(kDtTke, fts), M_(0.5f, dz))) : tmp;
       }
-      av[zz] = a_;
-      bv[zz] = b_;
-      cv[zz] = c_;
-      dv[zz] = d_;
       dm = d0;
-    }
-    float bp[kColCh], yp[kColCh];
-#pragma unroll
-    for (int zz = 0; zz < kColCh; zz++) {  // (B)
-      if (zz >= zn) break;
-      const int z = zbase + zz;
       float m0 = 1.0f, m1 = 0.0f, m2 = 0.0f, m3 = 1.0f;
       if (z > 0) {
-        m0 = bv[zz];
-        m1 = S_(0.0f, M_(av[zz], cprev));
+        m0 = b_;
+        m1 = S_(0.0f, M_(a_, cprev));
         m2 = 1.0f;
         m3 = 0.0f;
       } else {
-        b0 = bv[zz];
+        b0 = b_;
       }
-      const float value = __frcp_rn(M_(s0, m0));  // 1 / (s0 m0), correctly rounded
+      const float value = __frcp_rn(M_(s0, m0));
       const float n0 = M_(A_(M_(m0, s0), M_(m1, s2)), value);
       const float n1 = M_(A_(M_(m0, s1), M_(m1, s3)), value);
       const float n2 = M_(A_(M_(m2, s0), M_(m3, s2)), value);
@@ -450,28 +468,24 @@ __global__ void __launch_bounds__(kColWarps * 32, 4) tke_column_kernel(TkeArgs p
       s1 = n1;
       s2 = n2;
       s3 = n3;
-      bp[zz] = D_(A_(M_(s0, b0), s1), A_(M_(s2, b0), s3));
+      const float bpz = D_(A_(M_(s0, b0), s1), A_(M_(s2, b0), s3));
       float l0 = 0.0f, l1 = 1.0f;
       if (z > 0) {
-        l0 = dv[zz];
-        l1 = S_(0.0f, D_(av[zz], bpprev));
+        l0 = d_;
+        l1 = S_(0.0f, D_(a_, bpprev));
       } else {
-        y0 = dv[zz];
+        y0 = d_;
       }
       const float rn0 = A_(l0, M_(l1, r0)), rn1 = M_(r1, l1);
       r0 = rn0;
       r1 = rn1;
-      yp[zz] = A_(r0, M_(r1, y0));
-      cprev = cv[zz];
-      bpprev = bp[zz];
-    }
-    if (inner) {
-#pragma unroll
-      for (int zz = 0; zz < kColCh; zz++) {  // (C) y'/b' and -c/b' (:61-79)
-        if (zz >= zn) break;
-        const int64_t o = (int64_t)(zbase + zz) * qs;
-        q0[o] = D_(yp[zz], bp[zz]);
-        q1[o] = S_(0.0f, D_(cv[zz], bp[zz]));
+      const float ypz = A_(r0, M_(r1, y0));
+      cprev = c_;
+      bpprev = bpz;
+      if (inner) {
+        const int64_t o = (int64_t)z * qs;
+        q0[o] = D_(ypz, bpz);
+        q1[o] = S_(0.0f, D_(c_, bpz));
       }
     }
     __syncwarp();  // the next iteration refills this chunk's stage
@@ -482,37 +496,49 @@ __global__ void __launch_bounds__(kColWarps * 32, 4) tke_column_kernel(TkeArgs p
   // into the tile, then the chunk's cells (coalesced): take the solution or
   // keep tketaup1 (:212-218), the top cell's correction, clip and lateral
   // diffusion (:219-263) -- tketaup1 before the Adams-Bashforth update, which
-  // tke_ab_kernel applies once the advection kernel is done.  The next
-  // chunk's quotients (registers) and tketaup1 (cp.async) load meanwhile.
+  // tke_ab_kernel applies once the advection kernel is done.  The quotients
+  // of the chunk after next (registers) and tketaup1 three chunks on
+  // (cp.async) load meanwhile: a backward chunk is little work, so one chunk
+  // ahead left the loads' latency exposed.
   float* ust = st;
   const float yn = inner ? q0[(int64_t)(Z - 1) * qs] : 0.0f;  // y'_{n-1} / b'_{n-1}
   r0 = 0.0f;
   r1 = 1.0f;
   if (valid && !inner) p.tke_surf_corr_out[col] = 0.0f;
-  float qa0[kColCh], qa1[kColCh];
-  {
-    const int k = nch - 1, zn = Z - k * kColCh;
+  // quotients of chunk k (qa), k - 1 (qb) and k - 2 (loaded this iteration)
+  // in registers; tketaup1 of chunks k .. k - kUpd + 1 in flight (cp.async)
+  constexpr int kUpd = 4;
+  static_assert(kUpd * kColUpdFloats <= kColStages * kColStageFloats, "update stages reuse the forward stages");
+  auto ldq = [&](int k, float (&d0)[kColCh], float (&d1)[kColCh]) {  // element n - 1 folds the neutral (0, 1)
 #pragma unroll
-    for (int zz = 0; zz < kColCh; zz++) {  // element n - 1 folds the neutral (0, 1)
+    for (int zz = 0; zz < kColCh; zz++) {
       const int z = k * kColCh + zz;
-      const bool ld = inner && zz < zn && z < Z - 1;
-      qa0[zz] = ld ? q0[(int64_t)z * qs] : 0.0f;
-      qa1[zz] = ld ? q1[(int64_t)z * qs] : 1.0f;
+      const bool ld = inner && k >= 0 && z < Z - 1;
+      d0[zz] = ld ? q0[(int64_t)z * qs] : 0.0f;
+      d1[zz] = ld ? q1[(int64_t)z * qs] : 1.0f;
     }
+  };
+  float qa0[kColCh], qa1[kColCh], qb0[kColCh], qb1[kColCh];
+  ldq(nch - 1, qa0, qa1);
+  ldq(nch - 2, qb0, qb1);
+  for (int d = 0; d < kUpd - 1; d++) {
+    if (nch - 1 - d >= 0) col_stage_update(p, ust + ((nch - 1 - d) % kUpd) * kColUpdFloats, col0, ncol, nch - 1 - d, lane);
+    cp_async_commit();
   }
-  col_stage_update(p, ust + ((nch - 1) & 1) * kColUpdFloats, col0, ncol, nch - 1, lane);
-  cp_async_commit();
+  int in_c[kColCh], ks_c[kColCh];  // the flags of the columns this lane stores
+#pragma unroll
+  for (int j = 0; j < kColCh; j++) {
+    const int c = j * (32 / kColCh) + lane / kColCh;
+    in_c[j] = __shfl_sync(kAll, (int)inner, c);
+    ks_c[j] = __shfl_sync(kAll, ks, c);
+  }
   for (int k = nch - 1; k >= 0; k--) {
     const int zn = min(kColCh, Z - k * kColCh);
-    float qn0[kColCh], qn1[kColCh];
-    if (k >= 1) col_stage_update(p, ust + ((k - 1) & 1) * kColUpdFloats, col0, ncol, k - 1, lane);
+    float qc0[kColCh], qc1[kColCh];
+    if (k - (kUpd - 1) >= 0)
+      col_stage_update(p, ust + ((k - (kUpd - 1)) % kUpd) * kColUpdFloats, col0, ncol, k - (kUpd - 1), lane);
     cp_async_commit();
-#pragma unroll
-    for (int zz = 0; zz < kColCh; zz++) {  // chunk k - 1 is full and below the top cell
-      const int64_t o = (int64_t)((k - 1) * kColCh + zz) * qs;
-      qn0[zz] = (inner && k >= 1) ? q0[o] : 0.0f;
-      qn1[zz] = (inner && k >= 1) ? q1[o] : 1.0f;
-    }
+    ldq(k - 2, qc0, qc1);
     if (inner) {
 #pragma unroll
       for (int zz = kColCh - 1; zz >= 0; zz--) {
@@ -533,27 +559,27 @@ __global__ void __launch_bounds__(kColWarps * 32, 4) tke_column_kernel(TkeArgs p
         tile[zz * kColPad + lane] = v;
       }
     }
-    cp_async_wait_all_but_one();  // chunk k's update fields have landed
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(kUpd - 1) : "memory");  // chunk k's update fields have landed
     __syncwarp();
-    const float* u = ust + (k & 1) * kColUpdFloats;
+    const float* u = ust + (k % kUpd) * kColUpdFloats;
 #pragma unroll
     for (int j = 0; j < kColCh; j++) {
       const int c = j * (32 / kColCh) + lane / kColCh, zz = lane & (kColCh - 1);
-      const int in_c = __shfl_sync(kAll, (int)inner, c);
-      const int ks_c = __shfl_sync(kAll, ks, c);
       const int64_t cc = col0 + c;
       if (cc < ncol && zz < zn) {
         const int z = k * kColCh + zz;
-        const bool take = in_c && (z == Z - 1 || (ks_c >= 0 && z >= ks_c));
+        const bool take = in_c[j] && (z == Z - 1 || (ks_c[j] >= 0 && z >= ks_c[j]));
         const float* uf = u + zz * kColPad + c;
         p.tketaup1_out[cc * Z + z] = take ? tile[zz * kColPad + c] : uf[0];
       }
     }
-    __syncwarp();  // the tile and this stage are rewritten two chunks on
+    __syncwarp();  // the tile and this stage are rewritten by later chunks
 #pragma unroll
     for (int zz = 0; zz < kColCh; zz++) {
-      qa0[zz] = qn0[zz];
-      qa1[zz] = qn1[zz];
+      qa0[zz] = qb0[zz];
+      qa1[zz] = qb1[zz];
+      qb0[zz] = qc0[zz];
+      qb1[zz] = qc1[zz];
     }
   }
 }
