@@ -2656,7 +2656,7 @@ int tridag_launch(futhark_context* ctx, int form, int64_t rows, int64_t m, const
                             : (form == 0 ? lvc_tridag_tma_kernel<0, 512> : lvc_tridag_tma_kernel<1, 512>);
       const size_t smem = tri_tma_smem(cols);
       LVC_CUDA(ctx, cudaFuncSetAttribute((const void*)fk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      fk<<<(unsigned)nblk, 32 * kTriTmemWarps, smem, ctx->stream>>>(maps[0], maps[1], maps[2], maps[3], rows,
+      fk<<<(unsigned)nblk, kTriTmaThreads, smem, ctx->stream>>>(maps[0], maps[1], maps[2], maps[3], rows,
                                                                      (int)m, out);
       const cudaError_t e = cudaGetLastError();
       if (e != cudaSuccess) return cuda_fail(ctx, e, "tridiagonal launch");

@@ -686,23 +686,30 @@ __global__ void __launch_bounds__(32 * kTriTmemWarps) lvc_tridag_tmem_kernel(int
 // inside the 12 floats from the 16-byte boundary at or below it, offset
 // (m s) mod 4; one tensor copy per array and s brings that 12-float box of
 // the CTA's 32 groups into shared memory, [s][group][12] -- sixteen copies
-// per window for the CTA's 128 systems, issued by one thread, against 32
-// four-byte cp.async per lane and array.  Lane l of warp w owns system
-// 4 (8w + l / 4) + l % 4 and reads its elements at group 8w + l / 4 of box
-// l % 4: with m odd the offsets (m s) mod 4 of the four boxes are distinct
-// and 12 (8w + g) mod 32 runs over distinct multiples of 4, so a warp's
-// reads are free of bank conflicts.  Three stages; a stage is refilled
-// after the CTA barrier that follows every warp's last read of it, and
-// each window's copies land on that stage's mbarrier (bounded waits).
-// Every warp runs the forward loop (the barriers need all of them); warps
-// past the last system compute nothing.
+// per window for the CTA's 128 systems, against 32 four-byte cp.async per
+// lane and array.  Lane l of warp w owns system 4 (8w + l / 4) + l % 4 and
+// reads its elements at group 8w + l / 4 of box l % 4: with m odd the
+// offsets (m s) mod 4 of the four boxes are distinct and 12 (8w + g) mod 32
+// runs over distinct multiples of 4, so a warp's reads are free of bank
+// conflicts.  A fifth warp issues the copies into a ring of kTriTmaStages
+// stages: window q lands on full[q % S]; each solving warp, done with a
+// window, arrives on empty[q % S], and the producer refills that stage with
+// window q + S once all four have -- so a solving warp waits only for its
+// data, never for the other warps (a CTA barrier per window cost the
+// solvers about a fifth of their time).  Every wait is bounded.  All four
+// solving warps run the forward loop (the producer counts on their
+// arrivals); warps past the last system compute on zeros and store nothing.
 constexpr int kTriTmaBox = 12;                                        // floats per box row
 constexpr int kTriTmaGroups = 8 * kTriTmemWarps;                      // 4-system groups per CTA
 constexpr int kTriTmaStageFloats = 4 * 4 * kTriTmaGroups * kTriTmaBox;  // [array][s][group][box]
+constexpr int kTriTmaStages = 4;
+constexpr int kTriTmaThreads = 32 * (kTriTmemWarps + 1);                // four solving warps and the producer
 __host__ __device__ __forceinline__ size_t tri_tma_smem(int cols) {
   const size_t need = 128 /* alignment */ + 128 /* barriers, TMEM address */ +
-                      sizeof(float) * (kTriTmemStages * (size_t)kTriTmaStageFloats + kTriTmemWarps * 32 * (kTriWin + 1));
-  const size_t pad = cols > 256 ? 150 * 1024 : 80 * 1024;  // as tri_tmem_smem: at most 512 columns per SM
+                      sizeof(float) * (kTriTmaStages * (size_t)kTriTmaStageFloats + kTriTmemWarps * 32 * (kTriWin + 1));
+  // 103 KB: three CTAs never share an SM, so at most 512 TMEM columns are
+  // asked for there; for 512-column CTAs, one per SM (as tri_tmem_smem)
+  const size_t pad = cols > 256 ? 150 * 1024 : 0;
   return need > pad ? need : pad;
 }
 __device__ __forceinline__ void tma_load_2d(float* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
@@ -714,27 +721,28 @@ __device__ __forceinline__ void tma_load_2d(float* dst, const CUtensorMap* map, 
 }
 
 template <int FORM, int COLS>
-__global__ void __launch_bounds__(32 * kTriTmemWarps) lvc_tridag_tma_kernel(const __grid_constant__ CUtensorMap ta,
-                                                                            const __grid_constant__ CUtensorMap tb,
-                                                                            const __grid_constant__ CUtensorMap tc,
-                                                                            const __grid_constant__ CUtensorMap ty,
-                                                                            int64_t rows, int m,
-                                                                            float* __restrict__ out) {
+__global__ void __launch_bounds__(kTriTmaThreads, 2) lvc_tridag_tma_kernel(const __grid_constant__ CUtensorMap ta,
+                                                                       const __grid_constant__ CUtensorMap tb,
+                                                                       const __grid_constant__ CUtensorMap tc,
+                                                                       const __grid_constant__ CUtensorMap ty,
+                                                                       int64_t rows, int m, float* __restrict__ out) {
   extern __shared__ __align__(16) unsigned char tri_raw[];
   constexpr int WS = kTriWin + 1, AS = 4 * kTriTmaGroups * kTriTmaBox, SS = kTriTmaGroups * kTriTmaBox;
+  constexpr int S = kTriTmaStages;
   const uint32_t raw = smem_u32(tri_raw);
   unsigned char* const base = tri_raw + (((raw + 127u) & ~127u) - raw);  // 128-byte aligned
-  uint64_t* const full = reinterpret_cast<uint64_t*>(base);                // [kTriTmemStages]
-  uint32_t* const s_taddr = reinterpret_cast<uint32_t*>(base + 64);        // written by tcgen05.alloc
+  uint64_t* const full = reinterpret_cast<uint64_t*>(base);                // [S]
+  uint64_t* const empty = full + S;                                        // [S]
+  uint32_t* const s_taddr = reinterpret_cast<uint32_t*>(base + 16 * S);    // written by tcgen05.alloc
   float* const stage0 = reinterpret_cast<float*>(base + 128);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  float* const Wo = stage0 + kTriTmemStages * kTriTmaStageFloats + warp * 32 * WS;  // output window
-  const int64_t r0 = ((int64_t)blockIdx.x * kTriTmemWarps + warp) * 32;
-  const int nr = r0 < rows ? (int)(rows - r0 < 32 ? rows - r0 : 32) : 0;
   const int g0 = blockIdx.x * kTriTmaGroups;  // the CTA's first group
   const int nq = (m + kTriWin - 1) / kTriWin;
   if (threadIdx.x == 0) {
-    for (int i = 0; i < kTriTmemStages; i++) mbar_init(&full[i], 1);
+    for (int i = 0; i < S; i++) {
+      mbar_init(&full[i], 1);
+      mbar_init(&empty[i], kTriTmemWarps);
+    }
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
   if (warp == 0) {
@@ -744,50 +752,57 @@ __global__ void __launch_bounds__(32 * kTriTmemWarps) lvc_tridag_tma_kernel(cons
   tmem_fence_before_sync();
   __syncthreads();
   tmem_fence_after_sync();
-  const uint32_t tl = *s_taddr + ((uint32_t)(32 * (warp & 3)) << 16);  // this warp's lane quarter, column 0
-  const CUtensorMap* maps[4] = {&ta, &tb, &tc, &ty};
-  auto issue = [&](int q) {  // thread 0: window q into stage q % kTriTmemStages
-    if (q < nq) {
-      const int st = q % kTriTmemStages;
-      float* const dst = stage0 + st * kTriTmaStageFloats;
-      mbar_expect_tx(&full[st], (unsigned)(sizeof(float) * kTriTmaStageFloats));
+  if (warp == kTriTmemWarps) {  // the producer
+    if (lane == 0) {
+      for (int q = 0; q < nq; q++) {
+        const int st = q % S;
+        if (q >= S && !mbar_wait(&empty[st], (unsigned)(q / S - 1) & 1u, kWaitPolls)) {
+          atomicExch(&lvc_tridag_err, 1);  // the solvers' own waits then run out too
+          break;
+        }
+        float* const dst = stage0 + st * kTriTmaStageFloats;
+        mbar_expect_tx(&full[st], (unsigned)(sizeof(float) * kTriTmaStageFloats));
 #pragma unroll
-      for (int arr = 0; arr < 4; arr++)
-#pragma unroll
-        for (int s = 0; s < 4; s++)
-          tma_load_2d(dst + arr * AS + s * SS, maps[arr], (m * s + kTriWin * q) & ~3, g0, &full[st]);
+        for (int s = 0; s < 4; s++) {
+          const int x = (m * s + kTriWin * q) & ~3;
+          tma_load_2d(dst + s * SS, &ta, x, g0, &full[st]);
+          tma_load_2d(dst + AS + s * SS, &tb, x, g0, &full[st]);
+          tma_load_2d(dst + 2 * AS + s * SS, &tc, x, g0, &full[st]);
+          tma_load_2d(dst + 3 * AS + s * SS, &ty, x, g0, &full[st]);
+        }
+      }
     }
-  };
-  const int s = lane & 3;
-  const float* const mine = stage0 + s * SS + (8 * warp + (lane >> 2)) * kTriTmaBox + ((m * s) & 3);
-  const bool act = lane < nr;
-  bool timed_out = false;
-  TriFwd f;
-  if (threadIdx.x == 0) {
-    issue(0);
-    issue(1);
-  }
-  for (int q = 0; q < nq; q++) {
-    __syncthreads();  // every warp is done with window q - 1, whose stage window q + 2 refills
-    if (threadIdx.x == 0) issue(q + 2);
-    if (!mbar_wait(&full[q % kTriTmemStages], (unsigned)(q / kTriTmemStages) & 1u,
-                   timed_out ? kWaitPollsAfterTimeout : kWaitPolls)) {
-      timed_out = true;
-      atomicExch(&lvc_tridag_err, 1);
+  } else {
+    float* const Wo = stage0 + S * kTriTmaStageFloats + warp * 32 * WS;  // output window
+    const int64_t r0 = ((int64_t)blockIdx.x * kTriTmemWarps + warp) * 32;
+    const int nr = r0 < rows ? (int)(rows - r0 < 32 ? rows - r0 : 32) : 0;
+    const uint32_t tl = *s_taddr + ((uint32_t)(32 * (warp & 3)) << 16);  // this warp's lane quarter, column 0
+    const int s = lane & 3;
+    const float* const mine = stage0 + s * SS + (8 * warp + (lane >> 2)) * kTriTmaBox + ((m * s) & 3);
+    const bool act = lane < nr;
+    bool timed_out = false;
+    TriFwd f;
+    for (int q = 0; q < nq; q++) {
+      const int st = q % S;
+      if (!mbar_wait(&full[st], (unsigned)(q / S) & 1u, timed_out ? kWaitPollsAfterTimeout : kWaitPolls)) {
+        timed_out = true;
+        atomicExch(&lvc_tridag_err, 1);
+      }
+      float v[16];
+      const float* const w = mine + st * kTriTmaStageFloats;
+      if (tri_full_window(q, m))
+        tri_forward_window<FORM, true>(f, w, AS, q, m, act, v);
+      else
+        tri_forward_window<FORM>(f, w, AS, q, m, act, v);
+      tmem_st16(tl + 16 * q, v);
+      __syncwarp();  // the whole warp has read the stage
+      if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(&empty[st])) : "memory");
     }
-    float v[16];
-    const float* const w = mine + (q % kTriTmemStages) * kTriTmaStageFloats;
-    if (tri_full_window(q, m))
-      tri_forward_window<FORM, true>(f, w, AS, q, m, act, v);
-    else
-      tri_forward_window<FORM>(f, w, AS, q, m, act, v);
-    tmem_st16(tl + 16 * q, v);
+    if (timed_out && lane == 0)  // copies that never landed: one more bounded wait for the last ones
+      for (int q = nq > S ? nq - S : 0; q < nq; q++) mbar_wait(&full[q % S], (unsigned)(q / S) & 1u, kWaitPolls);
+    tmem_wait_st();
+    if (nr > 0) tri_backward<FORM>(f, tl, Wo, lane, nr, m, r0, out);
   }
-  if (timed_out && threadIdx.x == 0)  // a copy that never landed: give the last ones one more bounded wait
-    for (int q = nq > kTriTmemStages ? nq - kTriTmemStages : 0; q < nq; q++)
-      mbar_wait(&full[q % kTriTmemStages], (unsigned)(q / kTriTmemStages) & 1u, kWaitPolls);
-  tmem_wait_st();
-  if (nr > 0) tri_backward<FORM>(f, tl, Wo, lane, nr, m, r0, out);
   tmem_fence_before_sync();
   __syncthreads();
   tmem_fence_after_sync();
