@@ -155,10 +155,10 @@ __device__ __forceinline__ float adv_east(const TkeArgs& p, int x, int y, int z)
 // ---------------------------------------------------------------------------
 constexpr int kAdvThreads = 256;  // at <= 64 registers two CTAs fit beside two column-kernel CTAs
 
-// Block b.x covers a tile of ty rows (y) x tz levels (z) of the plane --
-// thread t at (t / tz, t % tz), z fastest, ty * tz <= kAdvThreads, the z
-// extent split into nzt tiles of at most 31 owned levels, row 0 and level 0
-// of a tile being halo -- and block b.y the x segment
+// Block b.x covers a tile of ty rows (y) x tz levels (z) of the plane -- the
+// halo row 0 in warp 0, row r >= 1 at threads 32 + (r - 1) tz .., z fastest,
+// the z extent split into nzt tiles of at most 31 owned levels, level 0 of a
+// tile being halo too -- and block b.y the x segment
 // [b.y * xseg, ...).  A thread keeps tketau and maskW of x - 1 .. x + 2 at
 // its (y, z) in registers (the east flux, :264-281) and publishes those of x
 // in shared memory, where its neighbours (y +- 1, y + 2) and (z +- 1, z + 2)
@@ -175,19 +175,24 @@ __global__ void __launch_bounds__(kAdvThreads, 4) tke_advect_kernel(TkeArgs p, i
   const int t = threadIdx.x;
   const int64_t plane = (int64_t)p.Y * p.Z;
   const int Z = p.Z;
-  const int ry = t / tz, rz = t - ry * tz;  // position in the tile
+  // position in the tile: the halo row in warp 0 (lanes 0 .. tz - 1), rows
+  // 1 .. ty - 1 packed from thread 32 on, so the halo row's warp evaluates
+  // only the north flux the row above needs
+  const bool hwarp = t < 32;
+  const int ry = hwarp ? 0 : 1 + (t - 32) / tz, rz = hwarp ? t : (t - 32) % tz;
   const int yt = blockIdx.x / nzt, zt = blockIdx.x - yt * nzt;
   // row 0 and level 0 of the tile are halo: the cells just below the owned
   // (ty - 1) x (tz - 1) ones, whose north and top fluxes the owned cells
   // need; they run the same flux code, so no warp evaluates a neighbour's
   // flux on a divergent path
   const int yy = yt * (ty - 1) + ry - 1, zz = zt * (tz - 1) + rz - 1;
-  const bool live = ry < ty && yy >= 0 && yy < p.Y && zz >= 0 && zz < Z;
+  const bool live = ry < ty && rz < tz && yy >= 0 && yy < p.Y && zz >= 0 && zz < Z;
   const bool owned = live && ry >= 1 && rz >= 1;
   const int y = live ? yy : 0, z = live ? zz : 0;
   const int64_t qi = (int64_t)y * Z + z;
   const int xs = blockIdx.y * xseg, xe = min(p.X, xs + xseg);
   const bool n_in = ry >= 1 && ry + 2 < ty;  // (y - 1 .. y + 2, z) in this tile
+  const int nm = ry == 1 ? t - 32 : t - tz, np1 = hwarp ? t + 32 : t + tz;  // threads of rows y - 1, y + 1
   const bool t_in = rz >= 1 && rz + 2 < tz;  // (y, z - 1 .. z + 2) in this tile
   const bool yint = y >= 2 && y < p.Y - 2;
   const float cy = live ? p.cost[y] : 1.0f, cuy = live ? p.cosu[y] : 1.0f, dyt = live ? p.dyt[y] : 1.0f;
@@ -198,7 +203,7 @@ __global__ void __launch_bounds__(kAdvThreads, 4) tke_advect_kernel(TkeArgs p, i
   auto ldW = [&](int xx) { return (live && xx >= 0 && xx < p.X) ? p.maskW[xx * plane + qi] : 0.0f; };
   float T0 = ldT(xs - 1), T1 = ldT(xs), T2 = ldT(xs + 1), T3 = ldT(xs + 2);  // x - 1 .. x + 2
   float W0 = ldW(xs - 1), W1 = ldW(xs), W2 = ldW(xs + 1), W3 = ldW(xs + 2);
-  float fe_prev = (live && xs >= 1) ? adv_east(p, xs - 1, y, z) : 0.0f;
+  float fe_prev = (live && !hwarp && xs >= 1) ? adv_east(p, xs - 1, y, z) : 0.0f;
   // the velocities of this thread's cell, one step ahead
   auto ldU = [&](const float* f, int xx) { return (live && xx < xe) ? f[xx * plane + qi] : 0.0f; };
   float uN = ldU(p.utau, xs), vN = ldU(p.vtau, xs), wN = ldU(p.wtau, xs);
@@ -216,7 +221,7 @@ __global__ void __launch_bounds__(kAdvThreads, 4) tke_advect_kernel(TkeArgs p, i
     const double rdx = Rd_(M_(cy, p.dxt[x]));  // the east divisor of this x, for fe and dtketau
     if (live) {
       const bool xint = x >= 2 && x < p.X - 2;
-      if (x >= 1 && x < p.X - 2 && yint) {
+      if (!hwarp && x >= 1 && x < p.X - 2 && yint) {
         const bool in = x < p.X - 1;
         fe = calcflux<true>(1.0f, uC, kDtTracer, 0.0f, rdx, T1, T0, T2, T3, in ? M_(W1, W2) : 0.0f,
                       in ? M_(W0, W1) : 0.0f, in ? M_(W2, W3) : 0.0f);
@@ -224,12 +229,12 @@ __global__ void __launch_bounds__(kAdvThreads, 4) tke_advect_kernel(TkeArgs p, i
       if (y >= 1 && y < p.Y - 2 && xint) {
         float tm, tp1, tp2, wm, wp1, wp2;
         if (n_in) {
-          tm = sT[t - tz];
-          tp1 = sT[t + tz];
-          tp2 = sT[t + 2 * tz];
-          wm = sW[t - tz];
-          wp1 = sW[t + tz];
-          wp2 = sW[t + 2 * tz];
+          tm = sT[nm];
+          tp1 = sT[np1];
+          tp2 = sT[np1 + tz];
+          wm = sW[nm];
+          wp1 = sW[np1];
+          wp2 = sW[np1 + tz];
         } else {
           tm = p.tketau[i - Z];
           tp1 = p.tketau[i + Z];
@@ -242,7 +247,7 @@ __global__ void __launch_bounds__(kAdvThreads, 4) tke_advect_kernel(TkeArgs p, i
         fn = calcflux<true>(cuy, vC, kDtTracer, 0.0f, rdy, T1, tm, tp1, tp2, in ? M_(W1, wp1) : 0.0f,
                       in ? M_(wm, W1) : 0.0f, in ? M_(wp1, wp2) : 0.0f);
       }
-      if (z < Z - 1 && xint && yint) {
+      if (!hwarp && z < Z - 1 && xint && yint) {
         float tm = 0.0f, tp1, tp2 = 0.0f, wm = 0.0f, wp1, wp2 = 0.0f;
         if (t_in) {
           if (z != 0) {
@@ -274,7 +279,7 @@ __global__ void __launch_bounds__(kAdvThreads, 4) tke_advect_kernel(TkeArgs p, i
     sft[t] = ft;
     __syncthreads();
     if (owned) {  // dtketau (:320-340)
-      const float fnm = sfn[t - tz];  // the north flux of (y - 1, z): 0 outside the domain
+      const float fnm = sfn[nm];  // the north flux of (y - 1, z): 0 outside the domain
       const float ftm = sft[t - 1];   // the top flux of (y, z - 1)
       float tmp;
       if (x >= 2 && x < p.X - 2 && yint)
@@ -394,7 +399,8 @@ __global__ void __launch_bounds__(kColWarps * 32, 4) tke_column_kernel(TkeArgs p
   // backward recurrence folds.  Every lane runs A and B (the shuffles need
   // the whole warp); only interior columns store.
   float s0 = 1.0f, s1 = 0.0f, s2 = 0.0f, s3 = 1.0f, b0 = 0.0f, y0 = 0.0f, r0 = 0.0f, r1 = 1.0f;
-  float dm = 0.0f, cprev = 0.0f, bpprev = 0.0f;
+  float dm = 0.0f, cprev = 0.0f;
+  double rbpprev = 0.0;  // 1 / b' of z - 1 (DR_)
   col_stage_chunk(p, st, col0, ncol, 0, lane);
   cp_async_commit();
   if (nch > 1) col_stage_chunk(p, st + kColStageFloats, col0, ncol, 1, lane);
@@ -469,10 +475,11 @@ __global__ void __launch_bounds__(kColWarps * 32, 4) tke_column_kernel(TkeArgs p
       s2 = n2;
       s3 = n3;
       const float bpz = D_(A_(M_(s0, b0), s1), A_(M_(s2, b0), s3));
+      const double rbp = Rd_(bpz);  // three quotients by b'_z: y'_z, c_z here, a_{z+1} next
       float l0 = 0.0f, l1 = 1.0f;
       if (z > 0) {
         l0 = d_;
-        l1 = S_(0.0f, D_(a_, bpprev));
+        l1 = S_(0.0f, DR_(a_, rbpprev));
       } else {
         y0 = d_;
       }
@@ -481,11 +488,11 @@ __global__ void __launch_bounds__(kColWarps * 32, 4) tke_column_kernel(TkeArgs p
       r1 = rn1;
       const float ypz = A_(r0, M_(r1, y0));
       cprev = c_;
-      bpprev = bpz;
+      rbpprev = rbp;
       if (inner) {
         const int64_t o = (int64_t)z * qs;
-        q0[o] = D_(ypz, bpz);
-        q1[o] = S_(0.0f, D_(c_, bpz));
+        q0[o] = DR_(ypz, rbp);
+        q1[o] = S_(0.0f, DR_(c_, rbp));
       }
     }
     __syncwarp();  // the next iteration refills this chunk's stage
@@ -665,7 +672,7 @@ int step_launch(futhark_context* ctx, const tke_step_args* q) {
   if (e != cudaSuccess) return cuda_fail(ctx, e, "tke column launch");
   // advection and dtketau: (y, z) tiles of at most 31 owned levels plus a
   // halo level and a halo row, x segments so that about four waves of CTAs run
-  const int64_t nzt = (Z + 30) / 31, tz = (Z + nzt - 1) / nzt + 1, ty = kAdvThreads / tz;
+  const int64_t nzt = (Z + 30) / 31, tz = (Z + nzt - 1) / nzt + 1, ty = 1 + (kAdvThreads - 32) / tz;
   const int64_t plane_blocks = ((Y + ty - 2) / (ty - 1)) * nzt;
   const int64_t want_blocks = 4LL * 4 * ctx->num_sms;  // four CTAs per SM
   const int64_t nseg = std::max<int64_t>(1, std::min<int64_t>(X, (want_blocks + plane_blocks - 1) / plane_blocks));
