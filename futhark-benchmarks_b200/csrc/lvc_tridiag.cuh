@@ -68,6 +68,16 @@ __device__ __forceinline__ float tri_sub(float a, float b) { return __fsub_rn(a,
 __device__ __forceinline__ float tri_div(float a, float b) { return __fdiv_rn(a, b); }
 // 1 / x correctly rounded: the same value as tri_div(1.0f, x), cheaper
 __device__ __forceinline__ float tri_rcp(float x) { return __frcp_rn(x); }
+// a / b correctly rounded from rb = 1 / (double)b correctly rounded in
+// double: the float nearest the double product a * rb.  The product is
+// within 2^-52 of a / b relatively; a quotient of two floats is never a
+// point halfway between two floats nor closer to one than 2^-49 relatively
+// (a nonzero multiple of a power of two over a 24-bit divisor significand),
+// so the product rounds to float as a / b does.  Zeros, infinities and signs
+// follow from the IEEE operations.  One double reciprocal then serves every
+// quotient by the same divisor.
+__device__ __forceinline__ double tri_rcpd(float b) { return __drcp_rn((double)b); }
+__device__ __forceinline__ float tri_divr(float a, double rb) { return __double2float_rn(__dmul_rn((double)a, rb)); }
 
 template <int FORM>
 __global__ void __launch_bounds__(kTriThreads) lvc_tridag_kernel(int64_t rows, int m, const float* __restrict__ a,
@@ -467,12 +477,13 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
 }
 
 // The forward state of one system (FORM 0: cp, yp; FORM 1: the 4-tuple
-// scan s, b_0, c_{i-1}, the linear scan (c0, c1), y_0, b'_{i-1}, and the
+// scan s, b_0, c_{i-1}, the linear scan (c0, c1), y_0, 1 / b'_{i-1}, and the
 // last quotient y'_{m-1} / b'_{m-1} that starts the backward fold).
 struct TriFwd {
   float cp = 0.0f, yp = 0.0f;
   float s0 = 1.0f, s1 = 0.0f, s2 = 0.0f, s3 = 1.0f, b0 = 0.0f, cprev = 0.0f;
-  float y0 = 0.0f, c0 = 0.0f, c1 = 1.0f, bprev = 0.0f, yn = 0.0f;
+  float y0 = 0.0f, c0 = 0.0f, c1 = 1.0f, yn = 0.0f;
+  double rbprev = 0.0;  // 1 / b'_{i-1}, correctly rounded in double (tri_divr)
 };
 
 // Window q (elements q * kTriWin + k) of a system's forward pass, its inputs
@@ -530,25 +541,26 @@ __device__ __forceinline__ void tri_forward_window(TriFwd& f, const float* w, in
         f.s2 = n2;
         f.s3 = n3;
         const float bpi = tri_div(tri_add(tri_mul(f.s0, f.b0), f.s1), tri_add(tri_mul(f.s2, f.b0), f.s3));  // b'_i
+        const double rbp = tri_rcpd(bpi);  // three quotients by b'_i: y'_i, c_i here, a_{i+1} next
         // recurrence 2 (:38-56): y'_i from the scan of (y_i, -a_i / b'_{i-1})
         float l0 = 0.0f, l1 = 1.0f;
         if (FULL || 0 < i) {
           l0 = yi;
-          l1 = tri_sub(0.0f, tri_div(ai, f.bprev));
+          l1 = tri_sub(0.0f, tri_divr(ai, f.rbprev));
         }
         const float e0 = tri_add(l0, tri_mul(l1, f.c0));
         const float e1 = tri_mul(f.c1, l1);
         f.c0 = e0;
         f.c1 = e1;
         const float ypi = tri_add(f.c0, tri_mul(f.c1, f.y0));  // y'_i
-        f.bprev = bpi;
+        f.rbprev = rbp;
         // recurrence 3's elements (:61-79), the last one's first component
         // its starting value
         if (FULL || i < m - 1) {
-          v[2 * k] = tri_div(ypi, bpi);
-          v[2 * k + 1] = tri_sub(0.0f, tri_div(ci, bpi));
+          v[2 * k] = tri_divr(ypi, rbp);
+          v[2 * k + 1] = tri_sub(0.0f, tri_divr(ci, rbp));
         } else {
-          f.yn = tri_div(ypi, bpi);
+          f.yn = tri_divr(ypi, rbp);
         }
       }
     }
