@@ -59,7 +59,10 @@ LVC_API int futhark_entry_tridagNestedSeqConst(struct futhark_context *ctx, stru
 
 /* Solves `rows` systems of size m given as row-major [rows][m] device arrays,
  * asynchronously on the context's stream (lvc_context_stream); out may not
- * alias the inputs.  Same arithmetic as the entry points. */
+ * alias the inputs.  Same arithmetic as the entry points.  Any alignment of
+ * the arrays is accepted; with odd m <= 256, rows a multiple of 4 and the
+ * four inputs on 16-byte boundaries (as every allocation is) the inputs are
+ * staged by tensor copies, the fastest path. */
 LVC_API int lvc_tridag_f32(struct futhark_context *ctx, int32_t form, int64_t rows, int64_t m,
                            const float *a, const float *b, const float *c, const float *y, float *out);
 /* Synchronises the context's stream and reports (FUTHARK_PROGRAM_ERROR) a
