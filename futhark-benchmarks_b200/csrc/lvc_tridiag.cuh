@@ -697,29 +697,33 @@ __global__ void __launch_bounds__(32 * kTriTmemWarps) lvc_tridag_tmem_kernel(int
 // system s of a group (elements 8q .. 8q + 7, at 4m-offset m s + 8q) lies
 // inside the 12 floats from the 16-byte boundary at or below it, offset
 // (m s) mod 4; one tensor copy per array and s brings that 12-float box of
-// the CTA's 32 groups into shared memory, [s][group][12] -- sixteen copies
-// per window for the CTA's 128 systems, against 32 four-byte cp.async per
-// lane and array.  Lane l of warp w owns system 4 (8w + l / 4) + l % 4 and
-// reads its elements at group 8w + l / 4 of box l % 4: with m odd the
-// offsets (m s) mod 4 of the four boxes are distinct and 12 (8w + g) mod 32
-// runs over distinct multiples of 4, so a warp's reads are free of bank
-// conflicts.  A fifth warp issues the copies into a ring of kTriTmaStages
-// stages: window q lands on full[q % S]; each solving warp, done with a
-// window, arrives on empty[q % S], and the producer refills that stage with
-// window q + S once all four have -- so a solving warp waits only for its
-// data, never for the other warps (a CTA barrier per window cost the
-// solvers about a fifth of their time).  Every wait is bounded.  All four
-// solving warps run the forward loop (the producer counts on their
-// arrivals); warps past the last system compute on zeros and store nothing.
-constexpr int kTriTmaBox = 12;                                        // floats per box row
+// the CTA's 32 groups into shared memory -- and the box is 20 floats wide,
+// so that it holds two windows (2j, 2j + 1: 16 elements from offset
+// (m s) mod 4), [s][group][20]: sixteen copies per pair of windows for the
+// CTA's 128 systems, against 32 four-byte cp.async per lane, array and
+// window (boxes of one window, 12 floats, were 6 % slower: twice the box
+// rows for the copy engine).  Lane l of warp w owns system
+// 4 (8w + l / 4) + l % 4 and reads its elements at group 8w + l / 4 of box
+// l % 4: with m odd the offsets (m s) mod 4 of the four boxes are distinct
+// and 20 (8w + g) mod 32 runs over distinct multiples of 4, so a warp's
+// reads are free of bank conflicts.  A fifth warp issues the copies into a
+// ring of kTriTmaStages stages: window pair j lands on full[j % S]; each
+// solving warp, done with a pair, arrives on empty[j % S], and the producer
+// refills that stage with pair j + S once all four have -- so a solving
+// warp waits only for its data, never for the other warps (a CTA barrier
+// per window cost the solvers about a fifth of their time).  Every wait is
+// bounded.  All four solving warps run the forward loop (the producer
+// counts on their arrivals); warps past the last system compute on zeros
+// and store nothing.
+constexpr int kTriTmaBox = 20;                                        // floats per box row: two windows
 constexpr int kTriTmaGroups = 8 * kTriTmemWarps;                      // 4-system groups per CTA
 constexpr int kTriTmaStageFloats = 4 * 4 * kTriTmaGroups * kTriTmaBox;  // [array][s][group][box]
-constexpr int kTriTmaStages = 4;
+constexpr int kTriTmaStages = 2;
 constexpr int kTriTmaThreads = 32 * (kTriTmemWarps + 1);                // four solving warps and the producer
 __host__ __device__ __forceinline__ size_t tri_tma_smem(int cols) {
   const size_t need = 128 /* alignment */ + 128 /* barriers, TMEM address */ +
                       sizeof(float) * (kTriTmaStages * (size_t)kTriTmaStageFloats + kTriTmemWarps * 32 * (kTriWin + 1));
-  // 103 KB: three CTAs never share an SM, so at most 512 TMEM columns are
+  // 87 KB: three CTAs never share an SM, so at most 512 TMEM columns are
   // asked for there; for 512-column CTAs, one per SM (as tri_tmem_smem)
   const size_t pad = cols > 256 ? 150 * 1024 : 0;
   return need > pad ? need : pad;
@@ -766,7 +770,8 @@ __global__ void __launch_bounds__(kTriTmaThreads, 2) lvc_tridag_tma_kernel(const
   tmem_fence_after_sync();
   if (warp == kTriTmemWarps) {  // the producer
     if (lane == 0) {
-      for (int q = 0; q < nq; q++) {
+      const int np = (nq + 1) / 2;
+      for (int q = 0; q < np; q++) {
         const int st = q % S;
         if (q >= S && !mbar_wait(&empty[st], (unsigned)(q / S - 1) & 1u, kWaitPolls)) {
           atomicExch(&lvc_tridag_err, 1);  // the solvers' own waits then run out too
@@ -776,7 +781,7 @@ __global__ void __launch_bounds__(kTriTmaThreads, 2) lvc_tridag_tma_kernel(const
         mbar_expect_tx(&full[st], (unsigned)(sizeof(float) * kTriTmaStageFloats));
 #pragma unroll
         for (int s = 0; s < 4; s++) {
-          const int x = (m * s + kTriWin * q) & ~3;
+          const int x = (m * s + 2 * kTriWin * q) & ~3;
           tma_load_2d(dst + s * SS, &ta, x, g0, &full[st]);
           tma_load_2d(dst + AS + s * SS, &tb, x, g0, &full[st]);
           tma_load_2d(dst + 2 * AS + s * SS, &tc, x, g0, &full[st]);
@@ -795,23 +800,26 @@ __global__ void __launch_bounds__(kTriTmaThreads, 2) lvc_tridag_tma_kernel(const
     bool timed_out = false;
     TriFwd f;
     for (int q = 0; q < nq; q++) {
-      const int st = q % S;
-      if (!mbar_wait(&full[st], (unsigned)(q / S) & 1u, timed_out ? kWaitPollsAfterTimeout : kWaitPolls)) {
+      const int j = q >> 1, st = j % S;
+      if (!(q & 1) && !mbar_wait(&full[st], (unsigned)(j / S) & 1u, timed_out ? kWaitPollsAfterTimeout : kWaitPolls)) {
         timed_out = true;
         atomicExch(&lvc_tridag_err, 1);
       }
       float v[16];
-      const float* const w = mine + st * kTriTmaStageFloats;
+      const float* const w = mine + st * kTriTmaStageFloats + kTriWin * (q & 1);
       if (tri_full_window(q, m))
         tri_forward_window<FORM, true>(f, w, AS, q, m, act, v);
       else
         tri_forward_window<FORM>(f, w, AS, q, m, act, v);
       tmem_st16(tl + 16 * q, v);
       __syncwarp();  // the whole warp has read the stage
-      if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(&empty[st])) : "memory");
+      if (lane == 0 && ((q & 1) || q == nq - 1))
+        asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(&empty[st])) : "memory");
     }
-    if (timed_out && lane == 0)  // copies that never landed: one more bounded wait for the last ones
-      for (int q = nq > S ? nq - S : 0; q < nq; q++) mbar_wait(&full[q % S], (unsigned)(q / S) & 1u, kWaitPolls);
+    if (timed_out && lane == 0) {  // copies that never landed: one more bounded wait for the last ones
+      const int np = (nq + 1) / 2;
+      for (int q = np > S ? np - S : 0; q < np; q++) mbar_wait(&full[q % S], (unsigned)(q / S) & 1u, kWaitPolls);
+    }
     tmem_wait_st();
     if (nr > 0) tri_backward<FORM>(f, tl, Wo, lane, nr, m, r0, out);
   }
