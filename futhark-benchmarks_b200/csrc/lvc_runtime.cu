@@ -335,6 +335,13 @@ struct futhark_context {
   cudaStream_t aux[kMaxAux] = {};  // fork streams of the batch plans
   std::map<std::tuple<int, int, int>, TunedShape> shapes;  // (numX, numY, precision) -> tuned shape
   uint64_t shapes_gen = 0;  // bumped on every change of `shapes`
+  // tridiagonal solves: the tensor maps of the last batch that took the
+  // tensor-copy kernel, reused while its four inputs and shape repeat, and
+  // the kernels whose shared-memory limit is already raised on this device
+  const float* tri_map_src[4] = {};
+  int64_t tri_map_rows = -1, tri_map_m = -1;
+  CUtensorMap tri_maps[4];
+  std::set<const void*> tri_smem_raised;
 };
 
 namespace {
@@ -2639,23 +2646,39 @@ bool tri_group_map(CUtensorMap* map, const float* p, int64_t rows, int64_t m) {
              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// Raises a tridiagonal kernel's dynamic shared-memory limit once per context
+// (each kernel instance always asks for the same size).
+int tri_smem_limit(futhark_context* ctx, const void* fn, size_t bytes) {
+  if (ctx->tri_smem_raised.count(fn)) return 0;
+  LVC_CUDA(ctx, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  ctx->tri_smem_raised.insert(fn);
+  return 0;
+}
+
 int tridag_launch(futhark_context* ctx, int form, int64_t rows, int64_t m, const float* a, const float* b,
                   const float* c, const float* y, float* out) {
   if (rows < 0 || m < 0 || m > INT32_MAX) return set_error(ctx, FUTHARK_PROGRAM_ERROR, "bad tridiagonal batch shape");
   if (rows == 0 || m == 0) return 0;
   if (m <= kTriTmemMaxM && (m & 1) && rows % 4 == 0 && rows / 4 <= INT32_MAX - kTriTmaGroups) {
     // odd m: inputs staged for the whole CTA by tensor copies of 4-system groups
-    CUtensorMap maps[4];
     const float* src[4] = {a, b, c, y};
-    bool ok = true;
-    for (int i = 0; i < 4 && ok; i++) ok = tri_group_map(&maps[i], src[i], rows, m);
+    bool ok = ctx->tri_map_rows == rows && ctx->tri_map_m == m;
+    for (int i = 0; i < 4 && ok; i++) ok = ctx->tri_map_src[i] == src[i];
+    if (!ok) {  // encode the maps of this batch (host work: reused while the batch repeats)
+      ok = true;
+      for (int i = 0; i < 4 && ok; i++) ok = tri_group_map(&ctx->tri_maps[i], src[i], rows, m);
+      ctx->tri_map_rows = ok ? rows : -1;
+      ctx->tri_map_m = ok ? m : -1;
+      for (int i = 0; i < 4; i++) ctx->tri_map_src[i] = ok ? src[i] : nullptr;
+    }
     if (ok) {
+      const CUtensorMap* maps = ctx->tri_maps;
       const int64_t nblk = (rows + 32 * kTriTmemWarps - 1) / (32 * kTriTmemWarps);
       const int cols = tri_tmem_cols((int)m);
       auto fk = cols == 256 ? (form == 0 ? lvc_tridag_tma_kernel<0, 256> : lvc_tridag_tma_kernel<1, 256>)
                             : (form == 0 ? lvc_tridag_tma_kernel<0, 512> : lvc_tridag_tma_kernel<1, 512>);
       const size_t smem = tri_tma_smem(cols);
-      LVC_CUDA(ctx, cudaFuncSetAttribute((const void*)fk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      if (int rc = tri_smem_limit(ctx, (const void*)fk, smem)) return rc;
       fk<<<(unsigned)nblk, kTriTmaThreads, smem, ctx->stream>>>(maps[0], maps[1], maps[2], maps[3], rows,
                                                                      (int)m, out);
       const cudaError_t e = cudaGetLastError();
@@ -2670,7 +2693,7 @@ int tridag_launch(futhark_context* ctx, int form, int64_t rows, int64_t m, const
     auto fk = cols == 256 ? (form == 0 ? lvc_tridag_tmem_kernel<0, 256> : lvc_tridag_tmem_kernel<1, 256>)
                           : (form == 0 ? lvc_tridag_tmem_kernel<0, 512> : lvc_tridag_tmem_kernel<1, 512>);
     const size_t smem = tri_tmem_smem(cols);
-    LVC_CUDA(ctx, cudaFuncSetAttribute((const void*)fk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (int rc = tri_smem_limit(ctx, (const void*)fk, smem)) return rc;
     fk<<<(unsigned)nblk, 32 * kTriTmemWarps, smem, ctx->stream>>>(rows, (int)m, a, b, c, y, out);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(ctx, e, "tridiagonal launch");
@@ -2682,7 +2705,7 @@ int tridag_launch(futhark_context* ctx, int form, int64_t rows, int64_t m, const
     const size_t smem = sizeof(float) * (size_t)tri_stream_floats((int)m);
     const size_t smem_max = sizeof(float) * (size_t)tri_stream_floats(kTriMaxM);
     auto fs = form == 0 ? lvc_tridag_stream_kernel<0> : lvc_tridag_stream_kernel<1>;
-    LVC_CUDA(ctx, cudaFuncSetAttribute((const void*)fs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max));
+    if (int rc = tri_smem_limit(ctx, (const void*)fs, smem_max)) return rc;
     fs<<<(unsigned)nblk, 32, smem, ctx->stream>>>(rows, (int)m, a, b, c, y, out);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(ctx, e, "tridiagonal launch");
