@@ -2132,6 +2132,7 @@ struct lvc_server {
   DevicePool pool;
   std::vector<cudaStream_t> streams;
   std::vector<bool> stream_busy;
+  std::vector<bool> stream_high;  // created at the device's greatest priority: small batches go there
   std::vector<double*> pinned;  // per stream: staging for prices and the error flag
   std::vector<int64_t> pinned_cap;
   std::vector<double*> pinned_retired;  // outgrown staging, freed with the server (cudaFreeHost synchronises)
@@ -2229,18 +2230,14 @@ size_t request_bytes(const futhark_context* ctx, const lvc_calibration& c, int p
 // could be admitted.  Called with S->mu held; releases it while building.
 bool server_admit(lvc_server* S, std::unique_lock<std::mutex>& lk) {
   if (S->pending.empty()) return false;
-  int si = -1;
-  for (size_t i = 0; i < S->streams.size(); i++)
-    if (!S->stream_busy[i]) {
-      si = (int)i;
-      break;
-    }
-  if (si < 0) return false;
+  if (std::find(S->stream_busy.begin(), S->stream_busy.end(), false) == S->stream_busy.end()) return false;
   // Admission order: shortest job first (option-cell-steps), so that small
   // requests are not queued behind large ones; a request that has waited
   // longer than kStarveS goes first (oldest first), so large ones are not
   // starved.
   constexpr double kStarveS = 0.05;
+  constexpr double kBatchSpread = 4.0;     // largest / first request of a batch, by work
+  constexpr double kSmallBatchWork = 1.5e8;  // option-cell-steps (about a millisecond of the GPU)
   const double tnow = now_s();
   auto next_pick = [&]() {
     auto best = S->pending.end();
@@ -2253,10 +2250,14 @@ bool server_admit(lvc_server* S, std::unique_lock<std::mutex>& lk) {
   std::vector<SrvRequest*> take;
   size_t bytes = 0;
   auto free_bytes = [&]() { return S->pool.budget > S->pool.in_use ? S->pool.budget - S->pool.in_use : 0; };
+  double take_work = 0, first_work = 0;
   while (!S->pending.empty() && (int)take.size() < S->cfg.max_batch_requests &&
          S->inflight_requests + (int)take.size() < S->cfg.max_inflight_requests) {
     auto pit = next_pick();
     SrvRequest* r = *pit;
+    // a batch completes with its largest request: a small request joins no
+    // batch of requests much larger than itself
+    if (!take.empty() && r->work > kBatchSpread * first_work) break;
     const size_t rb = request_bytes(&S->sctx, r->c, S->cfg.precision);
     if (rb > S->pool.budget) {  // can never fit: fail it now
       S->pending.erase(pit);
@@ -2276,11 +2277,23 @@ bool server_admit(lvc_server* S, std::unique_lock<std::mutex>& lk) {
       plan_release(victim.second);
     }
     if (bytes + rb > free_bytes()) break;
+    if (take.empty()) first_work = r->work;
     take.push_back(r);
+    take_work += r->work;
     bytes += rb;
     S->pending.erase(pit);
   }
   if (take.empty()) return false;
+  // a free stream: a small batch prefers the high-priority ones, a large one
+  // the others (either takes what is free)
+  const bool small = take_work <= kSmallBatchWork;
+  int si = -1;
+  for (int pass = 0; pass < 2 && si < 0; pass++)
+    for (size_t i = 0; i < S->streams.size(); i++)
+      if (!S->stream_busy[i] && (pass == 1 || S->stream_high[i] == small)) {
+        si = (int)i;
+        break;
+      }
   std::vector<lvc_calibration> cs;
   for (SrvRequest* r : take) cs.push_back(r->c);
   S->stream_busy[si] = true;
@@ -2439,12 +2452,18 @@ int lvc_server_new(struct futhark_context* ctx, const struct lvc_server_config* 
   S->pool.budget = (size_t)c.hbm_budget_bytes;
   cudaError_t e = cudaStreamCreateWithFlags(&S->sctx.stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&S->sctx.capture, cudaStreamNonBlocking);
+  // half the streams at the device's greatest priority: the block scheduler
+  // starts their CTAs ahead of waiting CTAs of the other half's large batches
+  int prio_low = 0, prio_high = 0;
+  if (cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high) != cudaSuccess) prio_low = prio_high = 0;
   for (int i = 0; i < c.num_streams && e == cudaSuccess; i++) {
     cudaStream_t st;
-    e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    const bool high = 2 * i < c.num_streams;
+    e = cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, high ? prio_high : prio_low);
     if (e == cudaSuccess) {
       S->streams.push_back(st);
       S->stream_busy.push_back(false);
+      S->stream_high.push_back(high);
       // staging for 65535 prices and the error flag; a larger batch grows it
       double* pin = nullptr;
       e = cudaMallocHost((void**)&pin, sizeof(double) << 16);

@@ -224,13 +224,16 @@ LVC_API int64_t lvc_entry_main_f64_noalloc_bytes(struct futhark_context *ctx, co
 
 /*
  * Serving runtime: continuous batching of calibration requests.  A
- * scheduler thread admits queued requests in arrival order as batches while
- * a stream is free, the in-flight request cap is not reached and the batch's
- * tables and pivots fit in what is left of the HBM budget (reserved once at
- * creation).  Batches run concurrently on their own streams with one CTA (or
- * cluster) per strike instance, so SMs pass to waiting instances of any
- * in-flight batch as running ones finish.  Latency is measured from submit to
- * the completion of the request's batch.
+ * scheduler thread admits queued requests as batches -- shortest first by
+ * option-cell-steps, a request queued over 50 ms first of all, no request
+ * of more than 4x the work of the batch's first -- while a stream is free,
+ * the in-flight request cap is not reached and the batch's tables and
+ * pivots fit in what is left of the HBM budget (reserved once at creation).
+ * Batches run concurrently on their own streams with one CTA (or cluster)
+ * per strike instance, so SMs pass to waiting instances of any in-flight
+ * batch as running ones finish; half the streams have the device's greatest
+ * priority and take the batches of up to about a millisecond of GPU work.
+ * Latency is measured from submit to the completion of the request's batch.
  */
 struct lvc_server;
 struct lvc_server_config {
