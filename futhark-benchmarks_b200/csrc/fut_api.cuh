@@ -35,6 +35,7 @@ struct futhark_context {
   int reduce_order = 0;        // OptionPricing: 0 f64 accumulation, 1 the reference's f32 running sum
   cudaStream_t aux = nullptr;  // a second stream for work that overlaps `stream`'s,
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;  // forked and joined by these events
+  bool smem_raised = false;    // a kernel's shared-memory limit already raised on this device
 };
 
 namespace {

@@ -447,8 +447,8 @@ __global__ void __launch_bounds__(kColWarps * 32, 4) tke_column_kernel(TkeArgs p
       else if (z > 0 && z < Z - 1) a_ = DR_(-dm, rdz);
       else if (z == Z - 1) a_ = D_(-dm, M_(0.5f, dz));
       if (!water) b_ = 1.0f;
-      else if (edge) b_ = A_(A_(1.0f, DR_(d0, rdz)), M_(D_(M_(kDtTke, kCEps), mx), sq));
-      else if (z > 0 && z < Z - 1) b_ = A_(A_(1.0f, DR_(A_(d0, dm), rdz)), D_(M_(M_(kDtTke, kCEps), sq), mx));
+      else if (edge) b_ = A_(A_(1.0f, DR_(d0, rdz)), M_(__fdiv_rn(M_(kDtTke, kCEps), mx), sq));
+      else if (z > 0 && z < Z - 1) b_ = A_(A_(1.0f, DR_(A_(d0, dm), rdz)), __fdiv_rn(M_(M_(kDtTke, kCEps), sq), mx));
       else if (z == Z - 1) b_ = A_(A_(1.0f, D_(dm, M_(0.5f, dz))), M_(D_(M_(kDtTke, kCEps), mx), sq));
       if (z < Z - 1) c_ = water ? DR_(-d0, rdz) : 0.0f;
       if (water) {
@@ -474,7 +474,8 @@ __global__ void __launch_bounds__(kColWarps * 32, 4) tke_column_kernel(TkeArgs p
       s1 = n1;
       s2 = n2;
       s3 = n3;
-      const float bpz = D_(A_(M_(s0, b0), s1), A_(M_(s2, b0), s3));
+      // (quotients whose dividend is rarely zero skip D_'s test for one)
+      const float bpz = __fdiv_rn(A_(M_(s0, b0), s1), A_(M_(s2, b0), s3));
       const double rbp = Rd_(bpz);  // three quotients by b'_z: y'_z, c_z here, a_{z+1} next
       float l0 = 0.0f, l1 = 1.0f;
       if (z > 0) {
@@ -665,8 +666,12 @@ int step_launch(futhark_context* ctx, const tke_step_args* q) {
   // the columns: coefficients, tridagPar, tketaup1 (tke.fut:103-263)
   const int64_t col_blocks = (X * Y + 32 * kColWarps - 1) / (32 * kColWarps);
   if (col_blocks > INT32_MAX) return set_error(ctx, FUTHARK_PROGRAM_ERROR, "tke step: too many columns");
-  e = cudaFuncSetAttribute((const void*)tke_column_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kColSmem);
-  if (e != cudaSuccess) return cuda_fail(ctx, e, "tke column attributes");
+  if (!ctx->smem_raised) {  // once per context: host time the step need not spend
+    e = cudaFuncSetAttribute((const void*)tke_column_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)kColSmem);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "tke column attributes");
+    ctx->smem_raised = true;
+  }
   tke_column_kernel<<<(unsigned)col_blocks, 32 * kColWarps, kColSmem, s>>>(p);
   e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(ctx, e, "tke column launch");
