@@ -107,6 +107,38 @@ def test_device_step_matches_entry(tctx, tke, oracle):
     assert same_bits(out["tke_surf_corr_out"].cpu().numpy(), want[6])
 
 
+@pytest.mark.parametrize("off", [0, 1])
+def test_device_step_any_alignment_and_ragged_size(tctx, tke, oracle, off):
+    # the Adams-Bashforth update moves four cells per 16-byte access where the
+    # arrays allow it and one at a time otherwise: arrays 4 bytes past the
+    # 16-byte grid (off = 1) and a cell count that is not a multiple of 4 take
+    # the one-at-a-time path and its tail
+    import torch
+    X, Y, Z = 7, 6, 5
+    ins = dict(zip(tke.INPUT_NAMES, W.tke_inputs(X, Y, Z, seed=18, wet=True)))
+
+    def place(a):
+        a = np.ascontiguousarray(a, dtype=np.float32 if a.dtype.kind == "f" else a.dtype)
+        t = torch.zeros(a.size + off, dtype=torch.from_numpy(a).dtype, device="cuda")
+        t[off:] = torch.from_numpy(a.ravel()).cuda()
+        return t
+
+    dev = {k: place(v) for k, v in ins.items()}
+    out = {k: torch.zeros(n + off, dtype=torch.float32, device="cuda")
+           for k, n in (("tketaup1_out", X * Y * Z), ("dtketau_out", X * Y * Z), ("tke_surf_corr_out", X * Y))}
+    scratch = torch.empty(tctx.scratch_bytes(X, Y, Z), dtype=torch.uint8, device="cuda")
+    torch.cuda.synchronize()
+    ptrs = {k: dev[k][off:].data_ptr() for k in tke.STEP_INPUTS}
+    ptrs.update({k: v[off:].data_ptr() for k, v in out.items()})
+    ptrs["scratch"] = scratch.data_ptr()
+    tctx.step((X, Y, Z), ptrs)
+    tctx.check()
+    want = oracle.tke(*[ins[k] for k in tke.INPUT_NAMES])
+    assert same_bits(out["tketaup1_out"][off:].cpu().numpy().reshape(X, Y, Z), want[1])
+    assert same_bits(out["dtketau_out"][off:].cpu().numpy().reshape(X, Y, Z), want[3])
+    assert same_bits(out["tke_surf_corr_out"][off:].cpu().numpy().reshape(X, Y), want[6])
+
+
 def test_device_step_rejects_unaligned_scratch(tctx, tke, pkg):
     import torch
     X, Y, Z = 6, 6, 4

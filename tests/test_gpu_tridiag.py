@@ -91,6 +91,26 @@ def test_device_pointer_form_matches_entry_point(ctx, oracle):
         assert np.array_equal(out.cpu().numpy(), oracle.tridag(*host, form=oform))
 
 
+def test_device_pointer_form_reuses_arrays(ctx, oracle):
+    # the tensor maps of a batch are kept while its arrays and shape repeat:
+    # new contents in the same arrays, then a shorter batch and another inner
+    # size over the same memory, must all give the oracle's solutions
+    import torch
+    rows, m = 1024, 115
+    dev = [torch.empty(rows * m, dtype=torch.float32, device="cuda:0") for _ in range(4)]
+    out = torch.empty(rows * m, dtype=torch.float32, device="cuda:0")
+    for seed, r, mm in ((21, rows, m), (22, rows, m), (23, rows // 2, m), (24, 256, 111)):
+        host = wl.tridiag_inputs(r, mm, seed=seed)
+        for t, v in zip(dev, host):
+            t[:r * mm] = torch.from_numpy(v.ravel()).to("cuda:0")
+        for form, oform in (("seq", "seq"), ("par", "par4")):
+            torch.cuda.synchronize()
+            ctx.tridag_device(form, r, mm, *[t.data_ptr() for t in dev], out.data_ptr())
+            ctx.tridag_check()
+            got = out[:r * mm].cpu().numpy().reshape(r, mm)
+            assert np.array_equal(got, oracle.tridag(*host, form=oform)), (seed, form)
+
+
 @pytest.mark.parametrize("m", [115, 200, 300])
 def test_device_pointer_form_with_unaligned_arrays(ctx, oracle, m):
     # device arrays that start 4 bytes past a 16-byte boundary (the kernels'
